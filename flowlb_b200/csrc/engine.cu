@@ -1,0 +1,875 @@
+// engine.cu -- host side of the engine behind the C ABI of include/flowlb.h.
+//
+// Owns the device state of one case, issues the step passes on one stream and
+// replays steady runs of steps from captured CUDA graphs.  The reference's
+// counterpart is src/cuda/runCuda.cu (h_launchCudaCalculations2D and the
+// headless loops :460-528) plus src/cuda/cudaInitData.* (constants and
+// buffers).  Differences by design: parameters travel by value in the kernel
+// argument block instead of mutable __constant__ symbols, errors come back as
+// status codes instead of exit(), and there is no per-step host sync.
+#include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/flowlb.h"
+#include "kernels.cuh"
+
+using namespace flb;
+
+namespace {
+
+enum Variant { V_F64 = 0, V_F32 = 1, V_F16S = 2, V_F32M32 = 3 };
+
+constexpr int kGraphPairs = 16;  // steps per large graph = 2 * kGraphPairs
+
+struct GraphSlot {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t kernels = 0;
+};
+
+}  // namespace
+
+struct flb_engine {
+  flb_case_desc desc{};
+  Variant variant = V_F32;
+  uint32_t nx = 0, ny = 0, N = 0;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  size_t s_size = 4, c_size = 4, m_size = 8;
+  bool fs = false, hw = false, has_io = false;
+  uint64_t t = 0;
+  uint64_t launches = 0;
+  int cur = 0;  // index of the current flag buffer (free surface)
+  KParams kp{};
+  // device buffers
+  void* d_f = nullptr;
+  void* d_rho = nullptr;
+  void* d_u = nullptr;
+  uint8_t* d_flags[2] = {nullptr, nullptr};
+  uint8_t* d_geo = nullptr;
+  uint8_t* d_nbmask = nullptr;
+  void* d_mass = nullptr;
+  void* d_excess = nullptr;
+  void* d_phi = nullptr;
+  void* d_recon = nullptr;
+  uint8_t* d_recon_mask = nullptr;
+  void* d_rho_snap = nullptr;
+  void* d_u_snap = nullptr;
+  double* d_partial = nullptr;
+  double* d_scalar = nullptr;
+  unsigned long long* d_counts = nullptr;
+  GraphSlot g_pair, g_big;
+  std::string err;
+};
+
+namespace {
+
+const char* kStatusText[] = {"ok",          "invalid argument", "CUDA error", "out of memory",
+                             "unsupported", "I/O error",        "non-finite populations", "no CUDA device"};
+
+flb_status fail(flb_handle h, flb_status s, const std::string& msg) {
+  if (h) h->err = msg;
+  return s;
+}
+
+flb_status cuda_fail(flb_handle h, cudaError_t e, const char* what) {
+  const flb_status s = e == cudaErrorMemoryAllocation ? FLB_ERR_OUT_OF_MEMORY : FLB_ERR_CUDA;
+  return fail(h, s, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define FLB_CUDA(h, call)                                          \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) return cuda_fail((h), e_, #call);       \
+  } while (0)
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    cudaGetDevice(&prev);
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int now = -1;
+    cudaGetDevice(&now);
+    if (prev >= 0 && now != prev) cudaSetDevice(prev);
+  }
+};
+
+dim3 row_grid(uint32_t nx, uint32_t ny) { return dim3((nx + kBlock - 1) / kBlock, ny); }
+dim3 lin_grid(uint64_t n) { return dim3((unsigned)((n + kBlock - 1) / kBlock)); }
+
+// ---- per-variant launchers ------------------------------------------------
+template <class S, class C, class M>
+struct Ops {
+  static void sc(flb_engine* h, uint32_t odd, bool wm) {
+    const dim3 g = row_grid(h->nx, h->ny);
+    if (h->fs) {
+      if (h->hw) k_stream_collide<S, C, M, true, true, true><<<g, kBlock, 0, h->stream>>>(h->kp, odd);
+      else k_stream_collide<S, C, M, true, false, true><<<g, kBlock, 0, h->stream>>>(h->kp, odd);
+    } else if (wm) {
+      if (h->hw) k_stream_collide<S, C, M, false, true, true><<<g, kBlock, 0, h->stream>>>(h->kp, odd);
+      else k_stream_collide<S, C, M, false, false, true><<<g, kBlock, 0, h->stream>>>(h->kp, odd);
+    } else {
+      if (h->hw) k_stream_collide<S, C, M, false, true, false><<<g, kBlock, 0, h->stream>>>(h->kp, odd);
+      else k_stream_collide<S, C, M, false, false, false><<<g, kBlock, 0, h->stream>>>(h->kp, odd);
+    }
+  }
+  static void fs1(flb_engine* h, uint32_t odd) {
+    const dim3 g = row_grid(h->nx, h->ny);
+    if (h->hw) k_fs1<S, C, M, true><<<g, kBlock, 0, h->stream>>>(h->kp, odd);
+    else k_fs1<S, C, M, false><<<g, kBlock, 0, h->stream>>>(h->kp, odd);
+  }
+  static void fs234(flb_engine* h, uint32_t odd) {
+    const dim3 g((h->nx + kTX - 1) / kTX, (h->ny + kTY - 1) / kTY);
+    const dim3 b(kTX, kTY);
+    if (h->hw) k_fs234<S, C, M, true><<<g, b, 0, h->stream>>>(h->kp, odd);
+    else k_fs234<S, C, M, false><<<g, b, 0, h->stream>>>(h->kp, odd);
+  }
+  static void apply_recon(flb_engine* h, uint32_t odd) {
+    k_apply_recon<S, C><<<row_grid(h->nx, h->ny), kBlock, 0, h->stream>>>(h->kp, odd);
+  }
+  static void init_ddf(flb_engine* h) {
+    if (h->hw) k_init_ddf<S, C, true><<<row_grid(h->nx, h->ny), kBlock, 0, h->stream>>>(h->kp, h->d_geo);
+    else k_init_ddf<S, C, false><<<row_grid(h->nx, h->ny), kBlock, 0, h->stream>>>(h->kp, h->d_geo);
+  }
+  static void mass_partial(flb_engine* h, uint32_t odd) {
+    k_mass_partial<S, C, M><<<lin_grid(h->N), kBlock, 0, h->stream>>>(h->kp, odd, h->fs ? 1 : 0, h->d_partial);
+  }
+  static void census(flb_engine* h, uint32_t odd) {
+    k_census<S, C><<<lin_grid(h->N), kBlock, 0, h->stream>>>(h->kp, odd, h->d_counts);
+  }
+  static void decode(flb_engine* h, void* out) {
+    k_decode<S, C><<<lin_grid(9ull * h->N), kBlock, 0, h->stream>>>(static_cast<const S*>(h->d_f),
+                                                                     static_cast<C*>(out), h->N, h->kp.f16_inv);
+  }
+  static void encode(flb_engine* h, const void* in) {
+    k_encode<S, C><<<lin_grid(9ull * h->N), kBlock, 0, h->stream>>>(static_cast<S*>(h->d_f),
+                                                                     static_cast<const C*>(in), h->N,
+                                                                     h->kp.f16_scale);
+  }
+};
+
+template <class Fn>
+void dispatch(flb_engine* h, Fn&& fn) {
+  switch (h->variant) {
+    case V_F64: fn(Ops<double, double, double>{}); break;
+    case V_F32: fn(Ops<float, float, double>{}); break;
+    case V_F16S: fn(Ops<__half, float, double>{}); break;
+    case V_F32M32: fn(Ops<float, float, float>{}); break;
+  }
+}
+
+void refresh_params(flb_engine* h) {
+  KParams& k = h->kp;
+  k.nx = h->nx;
+  k.ny = h->ny;
+  k.N = h->N;
+  k.f = h->d_f;
+  k.rho = h->d_rho;
+  k.u = h->d_u;
+  k.flags = h->d_flags[h->cur];
+  k.flags_out = h->d_flags[h->cur ^ 1];
+  k.nbmask = h->d_nbmask;
+  k.mass = h->d_mass;
+  k.excess = h->d_excess;
+  k.phi = h->d_phi;
+  k.recon = h->d_recon;
+  k.recon_mask = h->d_recon_mask;
+  k.rho_snap = h->d_rho_snap;
+  k.u_snap = h->d_u_snap;
+}
+
+// Issues the passes of one time step at t on the stream.
+uint64_t issue_step(flb_engine* h, uint64_t t, bool write_macro) {
+  const uint32_t odd = (uint32_t)(t & 1u);
+  uint64_t k = 0;
+  refresh_params(h);
+  if (h->has_io) {
+    cudaMemcpyAsync(h->d_rho_snap, h->d_rho, (size_t)h->N * h->c_size, cudaMemcpyDeviceToDevice, h->stream);
+    cudaMemcpyAsync(h->d_u_snap, h->d_u, 2ull * h->N * h->c_size, cudaMemcpyDeviceToDevice, h->stream);
+  }
+  if (h->fs) {
+    dispatch(h, [&](auto ops) {
+      ops.fs1(h, odd);
+      ops.sc(h, odd, true);
+      ops.fs234(h, odd);
+    });
+    k = 3;
+    h->cur ^= 1;
+    refresh_params(h);
+  } else {
+    dispatch(h, [&](auto ops) { ops.sc(h, odd, write_macro || h->has_io); });
+    k = 1;
+  }
+  return k;
+}
+
+void destroy_graph(GraphSlot& g) {
+  if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (g.graph) cudaGraphDestroy(g.graph);
+  g = GraphSlot{};
+}
+
+// Captures 2*pairs steps starting at an even t with flag buffer 0 current.
+flb_status capture(flb_engine* h, GraphSlot& g, int pairs) {
+  if (g.exec) return FLB_OK;
+  const int saved_cur = h->cur;
+  FLB_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  uint64_t kernels = 0;
+  for (int s = 0; s < 2 * pairs; s++) kernels += issue_step(h, (uint64_t)s, false);
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+  h->cur = saved_cur;
+  refresh_params(h);
+  if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
+  cudaGraphExec_t exec = nullptr;
+  e = cudaGraphInstantiate(&exec, graph, 0);
+  if (e != cudaSuccess) {
+    cudaGraphDestroy(graph);
+    return cuda_fail(h, e, "cudaGraphInstantiate");
+  }
+  g.graph = graph;
+  g.exec = exec;
+  g.kernels = kernels;
+  return FLB_OK;
+}
+
+void free_all(flb_engine* h) {
+  destroy_graph(h->g_pair);
+  destroy_graph(h->g_big);
+  void* bufs[] = {h->d_f,      h->d_rho,    h->d_u,          h->d_flags[0],  h->d_flags[1], h->d_geo,
+                  h->d_nbmask, h->d_mass,   h->d_excess,     h->d_phi,       h->d_recon,    h->d_recon_mask,
+                  h->d_rho_snap, h->d_u_snap, h->d_partial,  h->d_scalar,    h->d_counts};
+  for (void* p : bufs)
+    if (p) cudaFree(p);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+}
+
+flb_status validate(const flb_case_desc* d, std::string& msg) {
+  if (!d) return msg = "null descriptor", FLB_ERR_INVALID_ARGUMENT;
+  if (!d->flags) return msg = "flags is null", FLB_ERR_INVALID_ARGUMENT;
+  if (d->nx < 3 || d->ny < 3) return msg = "nx and ny must be at least 3", FLB_ERR_INVALID_ARGUMENT;
+  const uint64_t N = (uint64_t)d->nx * d->ny;
+  if (9ull * N >= (1ull << 32)) return msg = "9*nx*ny must stay below 2^32", FLB_ERR_INVALID_ARGUMENT;
+  if (!(d->tau > 0.5f) || !std::isfinite(d->tau)) return msg = "tau must be finite and > 0.5", FLB_ERR_INVALID_ARGUMENT;
+  if (d->precision != 64 && d->precision != 32 && d->precision != 16)
+    return msg = "precision must be 64, 32 or 16", FLB_ERR_INVALID_ARGUMENT;
+  if (d->mass_precision != 64 && d->mass_precision != 32)
+    return msg = "mass_precision must be 64 or 32", FLB_ERR_INVALID_ARGUMENT;
+  if (d->mass_precision == 32 && d->precision != 32)
+    return msg = "mass_precision 32 requires precision 32", FLB_ERR_UNSUPPORTED;
+  if (d->collision != 0 && d->collision != 1) return msg = "collision must be SRT or TRT", FLB_ERR_INVALID_ARGUMENT;
+  if (d->bounce_back != FLB_BB_IMPLICIT && d->bounce_back != FLB_BB_HALFWAY)
+    return msg = "bounce_back must be IMPLICIT or HALFWAY", FLB_ERR_INVALID_ARGUMENT;
+  if (d->fs_mode != FLB_FS_REFERENCE && d->fs_mode != FLB_FS_CONSERVATIVE)
+    return msg = "fs_mode must be REFERENCE or CONSERVATIVE", FLB_ERR_INVALID_ARGUMENT;
+  if (d->precision == 16) {
+    const float s = d->f16_scale == 0.0f ? 4096.0f : d->f16_scale;
+    int e = 0;
+    if (!(s > 0.0f) || std::frexp(s, &e) != 0.5f) return msg = "f16_scale must be a power of two", FLB_ERR_INVALID_ARGUMENT;
+  }
+  return FLB_OK;
+}
+
+flb_status check_io(flb_engine* h, const uint8_t* flags) {
+  h->has_io = false;
+  for (uint64_t i = 0; i < h->N; i++) {
+    if (flags[i] & (kInlet | kOutlet)) h->has_io = true;
+    if ((flags[i] & kInlet) && i + 1 >= h->N) return fail(h, FLB_ERR_INVALID_ARGUMENT, "inlet in the last cell");
+    if ((flags[i] & kOutlet) && i == 0) return fail(h, FLB_ERR_INVALID_ARGUMENT, "outlet in the first cell");
+  }
+  return FLB_OK;
+}
+
+// Builds the initial state from the geometry flags in d_geo.
+flb_status initialise(flb_engine* h) {
+  FLB_CUDA(h, cudaMemsetAsync(h->d_f, 0, 9ull * h->N * h->s_size, h->stream));
+  const dim3 g = row_grid(h->nx, h->ny);
+  h->cur = 0;
+  h->t = 0;
+  if (h->fs) {
+    k_init_flags<<<g, kBlock, 0, h->stream>>>(h->d_geo, h->d_flags[0], h->nx, h->ny, 1, h->d_mass, h->d_excess,
+                                              h->d_phi, h->m_size == 8);
+  } else {
+    k_init_flags<<<g, kBlock, 0, h->stream>>>(h->d_geo, h->d_flags[0], h->nx, h->ny, 0, nullptr, nullptr, nullptr,
+                                              1);
+  }
+  h->launches++;
+  if (h->hw) {
+    k_nbmask<<<g, kBlock, 0, h->stream>>>(h->d_geo, h->d_nbmask, h->nx, h->ny);
+    h->launches++;
+  }
+  refresh_params(h);
+  dispatch(h, [&](auto ops) { ops.init_ddf(h); });
+  h->launches++;
+  if (h->fs) FLB_CUDA(h, cudaMemcpyAsync(h->d_flags[1], h->d_flags[0], h->N, cudaMemcpyDeviceToDevice, h->stream));
+  if (h->d_recon_mask) FLB_CUDA(h, cudaMemsetAsync(h->d_recon_mask, 0, h->N, h->stream));
+  FLB_CUDA(h, cudaGetLastError());
+  return FLB_OK;
+}
+
+}  // namespace
+
+// =============================================================================
+extern "C" {
+
+FLB_API void flb_case_desc_init(flb_case_desc* d) {
+  if (!d) return;
+  std::memset(d, 0, sizeof(*d));
+  d->precision = 32;
+  d->mass_precision = 64;
+  d->collision = FLB_COLLISION_SRT;
+  d->use_volumetric_force = 1;
+  d->tau = 0.6f;
+  d->bounce_back = FLB_BB_HALFWAY;
+  d->fs_mode = FLB_FS_CONSERVATIVE;
+  d->device = -1;
+}
+
+FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
+  if (!out) return FLB_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  std::string msg;
+  flb_status s = validate(desc, msg);
+  if (s != FLB_OK) {
+    std::fprintf(stderr, "flb_create: %s\n", msg.c_str());
+    return s;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return FLB_ERR_NO_DEVICE;
+  flb_engine* h = new flb_engine();
+  h->desc = *desc;
+  h->desc.flags = nullptr;
+  h->nx = desc->nx;
+  h->ny = desc->ny;
+  h->N = desc->nx * desc->ny;
+  h->fs = desc->free_surface != 0;
+  h->hw = desc->bounce_back == FLB_BB_HALFWAY;
+  if (desc->device >= 0) h->device = desc->device;
+  else cudaGetDevice(&h->device);
+  if (h->device >= ndev) {
+    delete h;
+    return FLB_ERR_INVALID_ARGUMENT;
+  }
+  DeviceGuard guard(h->device);
+  if (desc->precision == 64) {
+    h->variant = V_F64;
+    h->s_size = 8; h->c_size = 8; h->m_size = 8;
+  } else if (desc->precision == 16) {
+    h->variant = V_F16S;
+    h->s_size = 2; h->c_size = 4; h->m_size = 8;
+  } else if (desc->mass_precision == 32) {
+    h->variant = V_F32M32;
+    h->s_size = 4; h->c_size = 4; h->m_size = 4;
+  } else {
+    h->variant = V_F32;
+    h->s_size = 4; h->c_size = 4; h->m_size = 8;
+  }
+  s = check_io(h, desc->flags);
+  if (s != FLB_OK) {
+    std::fprintf(stderr, "flb_create: %s\n", h->err.c_str());
+    delete h;
+    return s;
+  }
+  auto bail = [&](flb_status st) {
+    std::fprintf(stderr, "flb_create: %s\n", h->err.c_str());
+    free_all(h);
+    delete h;
+    return st;
+  };
+  if (desc->stream) {
+    h->stream = static_cast<cudaStream_t>(desc->stream);
+  } else {
+    cudaError_t e = cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return bail(cuda_fail(h, e, "cudaStreamCreate"));
+    h->own_stream = true;
+  }
+  const uint64_t N = h->N;
+  struct Alloc { void** p; size_t bytes; bool need; };
+  const uint64_t blocks = (N + kBlock - 1) / kBlock;
+  Alloc allocs[] = {
+      {&h->d_f, 9 * N * h->s_size, true},
+      {&h->d_rho, N * h->c_size, true},
+      {&h->d_u, 2 * N * h->c_size, true},
+      {(void**)&h->d_flags[0], N, true},
+      {(void**)&h->d_flags[1], N, h->fs},
+      {(void**)&h->d_geo, N, true},
+      {(void**)&h->d_nbmask, N, h->hw},
+      {&h->d_mass, N * h->m_size, h->fs},
+      {&h->d_excess, N * h->m_size, h->fs},
+      {&h->d_phi, N * h->m_size, h->fs},
+      {&h->d_recon, 8 * N * h->c_size, h->fs && desc->fs_mode == FLB_FS_REFERENCE},
+      {(void**)&h->d_recon_mask, N, h->fs && desc->fs_mode == FLB_FS_REFERENCE},
+      {&h->d_rho_snap, N * h->c_size, h->has_io},
+      {&h->d_u_snap, 2 * N * h->c_size, h->has_io},
+      {(void**)&h->d_partial, blocks * sizeof(double), true},
+      {(void**)&h->d_scalar, sizeof(double), true},
+      {(void**)&h->d_counts, 8 * sizeof(unsigned long long), true},
+  };
+  for (Alloc& a : allocs) {
+    if (!a.need) continue;
+    cudaError_t e = cudaMalloc(a.p, a.bytes);
+    if (e != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc"));
+  }
+  KParams& k = h->kp;
+  std::memset(&k, 0, sizeof(k));
+  const float tau = desc->tau;  // float, as cudaInitData.cu:81-82
+  k.inv_tau = 1.0f / tau;
+  k.use_force = desc->use_volumetric_force ? 1 : 0;
+  k.fx = desc->use_volumetric_force ? desc->fx : 0.0f;
+  k.fy = desc->use_volumetric_force ? desc->fy : 0.0f;
+  k.subgrid = desc->subgrid ? 1 : 0;
+  k.collision = desc->collision;
+  k.f16_scale = desc->f16_scale == 0.0f ? 4096.0f : desc->f16_scale;
+  k.f16_inv = 1.0f / k.f16_scale;
+  k.inlet_ux = desc->inlet_ux;
+  k.inlet_uy = desc->inlet_uy;
+  k.fs_cons = desc->fs_mode == FLB_FS_CONSERVATIVE ? 1 : 0;
+  k.count_pre = 0;
+  cudaError_t e = cudaMemcpyAsync(h->d_geo, desc->flags, N, cudaMemcpyHostToDevice, h->stream);
+  if (e != cudaSuccess) return bail(cuda_fail(h, e, "cudaMemcpyAsync"));
+  s = initialise(h);
+  if (s != FLB_OK) return bail(s);
+  e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) return bail(cuda_fail(h, e, "cudaStreamSynchronize"));
+  *out = h;
+  return FLB_OK;
+}
+
+FLB_API flb_status flb_reset(flb_handle h, const uint8_t* host_flags) {
+  if (!h || !host_flags) return FLB_ERR_INVALID_ARGUMENT;
+  DeviceGuard guard(h->device);
+  const bool had_io = h->has_io;
+  flb_status s = check_io(h, host_flags);
+  if (s != FLB_OK) return s;
+  if (h->has_io && !had_io) {
+    h->has_io = false;
+    return fail(h, FLB_ERR_UNSUPPORTED, "reset adds inlet/outlet cells to a case created without them");
+  }
+  if (had_io != h->has_io) {
+    destroy_graph(h->g_pair);
+    destroy_graph(h->g_big);
+  }
+  FLB_CUDA(h, cudaMemcpyAsync(h->d_geo, host_flags, h->N, cudaMemcpyHostToDevice, h->stream));
+  return initialise(h);
+}
+
+FLB_API flb_status flb_destroy(flb_handle h) {
+  if (!h) return FLB_ERR_INVALID_ARGUMENT;
+  {
+    DeviceGuard guard(h->device);
+    cudaStreamSynchronize(h->stream);
+    free_all(h);
+  }
+  delete h;
+  return FLB_OK;
+}
+
+FLB_API flb_status flb_step(flb_handle h, uint64_t n) {
+  if (!h) return FLB_ERR_INVALID_ARGUMENT;
+  if (n == 0) return FLB_OK;
+  DeviceGuard guard(h->device);
+  nvtxRangePushA("flb_step");
+  uint64_t remaining = n;
+  flb_status s = FLB_OK;
+  while (remaining > 0 && s == FLB_OK) {
+    // graphs cover pairs of steps from an even t; the last step of the call
+    // runs on its own so that it writes density and velocity
+    const uint64_t big = 2ull * kGraphPairs;
+    if ((h->t & 1u) == 0 && remaining > big) {
+      s = capture(h, h->g_big, kGraphPairs);
+      if (s != FLB_OK) break;
+      cudaError_t e = cudaGraphLaunch(h->g_big.exec, h->stream);
+      if (e != cudaSuccess) { s = cuda_fail(h, e, "cudaGraphLaunch"); break; }
+      h->launches += h->g_big.kernels;
+      h->t += big;
+      remaining -= big;
+    } else if ((h->t & 1u) == 0 && remaining > 2) {
+      s = capture(h, h->g_pair, 1);
+      if (s != FLB_OK) break;
+      cudaError_t e = cudaGraphLaunch(h->g_pair.exec, h->stream);
+      if (e != cudaSuccess) { s = cuda_fail(h, e, "cudaGraphLaunch"); break; }
+      h->launches += h->g_pair.kernels;
+      h->t += 2;
+      remaining -= 2;
+    } else {
+      h->launches += issue_step(h, h->t, remaining == 1);
+      h->t += 1;
+      remaining -= 1;
+    }
+  }
+  nvtxRangePop();
+  if (s != FLB_OK) return s;
+  FLB_CUDA(h, cudaGetLastError());
+  return FLB_OK;
+}
+
+FLB_API flb_status flb_sync(flb_handle h) {
+  if (!h) return FLB_ERR_INVALID_ARGUMENT;
+  DeviceGuard guard(h->device);
+  FLB_CUDA(h, cudaStreamSynchronize(h->stream));
+  return FLB_OK;
+}
+
+FLB_API flb_status flb_get_time(flb_handle h, uint64_t* t) {
+  if (!h || !t) return FLB_ERR_INVALID_ARGUMENT;
+  *t = h->t;
+  return FLB_OK;
+}
+
+FLB_API flb_status flb_set_stream(flb_handle h, void* stream) {
+  if (!h) return FLB_ERR_INVALID_ARGUMENT;
+  DeviceGuard guard(h->device);
+  FLB_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (h->own_stream) cudaStreamDestroy(h->stream);
+  if (stream) {
+    h->stream = static_cast<cudaStream_t>(stream);
+    h->own_stream = false;
+  } else {
+    FLB_CUDA(h, cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+  }
+  return FLB_OK;
+}
+
+FLB_API flb_status flb_get_stream(flb_handle h, void** stream) {
+  if (!h || !stream) return FLB_ERR_INVALID_ARGUMENT;
+  *stream = h->stream;
+  return FLB_OK;
+}
+
+FLB_API flb_status flb_field_info(flb_handle h, int field, size_t* elem_size, size_t* count) {
+  if (!h) return FLB_ERR_INVALID_ARGUMENT;
+  size_t es = 0, n = 0;
+  switch (field) {
+    case FLB_FIELD_F: es = h->c_size; n = 9ull * h->N; break;
+    case FLB_FIELD_RHO: es = h->c_size; n = h->N; break;
+    case FLB_FIELD_U: es = h->c_size; n = 2ull * h->N; break;
+    case FLB_FIELD_FLAGS: es = 1; n = h->N; break;
+    case FLB_FIELD_MASS:
+    case FLB_FIELD_EXCESS:
+    case FLB_FIELD_PHI: es = h->m_size; n = h->fs ? h->N : 0; break;
+    default: return fail(h, FLB_ERR_INVALID_ARGUMENT, "unknown field");
+  }
+  if (elem_size) *elem_size = es;
+  if (count) *count = n;
+  return FLB_OK;
+}
+
+static flb_status field_ptr(flb_handle h, int field, void** ptr, size_t* bytes) {
+  size_t es = 0, n = 0;
+  flb_status s = flb_field_info(h, field, &es, &n);
+  if (s != FLB_OK) return s;
+  if (n == 0) return fail(h, FLB_ERR_UNSUPPORTED, "field not held in mono-fluid mode");
+  *bytes = es * n;
+  switch (field) {
+    case FLB_FIELD_F: *ptr = h->d_f; break;
+    case FLB_FIELD_RHO: *ptr = h->d_rho; break;
+    case FLB_FIELD_U: *ptr = h->d_u; break;
+    case FLB_FIELD_FLAGS: *ptr = h->d_flags[h->cur]; break;
+    case FLB_FIELD_MASS: *ptr = h->d_mass; break;
+    case FLB_FIELD_EXCESS: *ptr = h->d_excess; break;
+    case FLB_FIELD_PHI: *ptr = h->d_phi; break;
+  }
+  return FLB_OK;
+}
+
+FLB_API flb_status flb_read_field(flb_handle h, int field, void* dst, int on_device) {
+  if (!h || !dst) return FLB_ERR_INVALID_ARGUMENT;
+  DeviceGuard guard(h->device);
+  void* src = nullptr;
+  size_t bytes = 0;
+  flb_status s = field_ptr(h, field, &src, &bytes);
+  if (s != FLB_OK) return s;
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (field == FLB_FIELD_F && h->variant == V_F16S) {
+    void* tmp = nullptr;
+    FLB_CUDA(h, cudaMallocAsync(&tmp, bytes, h->stream));
+    refresh_params(h);
+    dispatch(h, [&](auto ops) { ops.decode(h, tmp); });
+    h->launches++;
+    cudaError_t e = cudaMemcpyAsync(dst, tmp, bytes, kind, h->stream);
+    cudaFreeAsync(tmp, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaMemcpyAsync");
+  } else {
+    FLB_CUDA(h, cudaMemcpyAsync(dst, src, bytes, kind, h->stream));
+  }
+  FLB_CUDA(h, cudaStreamSynchronize(h->stream));
+  return FLB_OK;
+}
+
+FLB_API flb_status flb_write_field(flb_handle h, int field, const void* src, int on_device) {
+  if (!h || !src) return FLB_ERR_INVALID_ARGUMENT;
+  DeviceGuard guard(h->device);
+  void* dst = nullptr;
+  size_t bytes = 0;
+  flb_status s = field_ptr(h, field, &dst, &bytes);
+  if (s != FLB_OK) return s;
+  const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  if (field == FLB_FIELD_F && h->variant == V_F16S) {
+    void* tmp = nullptr;
+    FLB_CUDA(h, cudaMallocAsync(&tmp, bytes, h->stream));
+    cudaError_t e = cudaMemcpyAsync(tmp, src, bytes, kind, h->stream);
+    if (e == cudaSuccess) {
+      refresh_params(h);
+      dispatch(h, [&](auto ops) { ops.encode(h, tmp); });
+      h->launches++;
+    }
+    cudaFreeAsync(tmp, h->stream);
+    if (e != cudaSuccess) return cuda_fail(h, e, "cudaMemcpyAsync");
+  } else {
+    FLB_CUDA(h, cudaMemcpyAsync(dst, src, bytes, kind, h->stream));
+  }
+  FLB_CUDA(h, cudaStreamSynchronize(h->stream));
+  return FLB_OK;
+}
+
+FLB_API flb_status flb_total_mass(flb_handle h, double* mass) {
+  if (!h || !mass) return FLB_ERR_INVALID_ARGUMENT;
+  DeviceGuard guard(h->device);
+  refresh_params(h);
+  const uint32_t odd = (uint32_t)(h->t & 1u);
+  dispatch(h, [&](auto ops) { ops.mass_partial(h, odd); });
+  const uint32_t blocks = (h->N + kBlock - 1) / kBlock;
+  k_sum_partials<<<1, kBlock, 0, h->stream>>>(h->d_partial, blocks, h->d_scalar);
+  h->launches += 2;
+  FLB_CUDA(h, cudaGetLastError());
+  FLB_CUDA(h, cudaMemcpyAsync(mass, h->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  FLB_CUDA(h, cudaStreamSynchronize(h->stream));
+  return FLB_OK;
+}
+
+static flb_status census(flb_handle h, unsigned long long out[5]) {
+  DeviceGuard guard(h->device);
+  refresh_params(h);
+  FLB_CUDA(h, cudaMemsetAsync(h->d_counts, 0, 8 * sizeof(unsigned long long), h->stream));
+  const uint32_t odd = (uint32_t)(h->t & 1u);
+  dispatch(h, [&](auto ops) { ops.census(h, odd); });
+  h->launches++;
+  FLB_CUDA(h, cudaGetLastError());
+  FLB_CUDA(h, cudaMemcpyAsync(out, h->d_counts, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->stream));
+  FLB_CUDA(h, cudaStreamSynchronize(h->stream));
+  return FLB_OK;
+}
+
+FLB_API flb_status flb_cell_counts(flb_handle h, uint64_t counts[4]) {
+  if (!h || !counts) return FLB_ERR_INVALID_ARGUMENT;
+  unsigned long long c[5];
+  flb_status s = census(h, c);
+  if (s != FLB_OK) return s;
+  for (int k = 0; k < 4; k++) counts[k] = c[k];
+  return FLB_OK;
+}
+
+FLB_API flb_status flb_check_finite(flb_handle h) {
+  if (!h) return FLB_ERR_INVALID_ARGUMENT;
+  unsigned long long c[5];
+  flb_status s = census(h, c);
+  if (s != FLB_OK) return s;
+  if (c[4]) return fail(h, FLB_ERR_NONFINITE, std::to_string(c[4]) + " cells hold non-finite populations");
+  return FLB_OK;
+}
+
+FLB_API flb_status flb_run_pass(flb_handle h, int pass) {
+  if (!h) return FLB_ERR_INVALID_ARGUMENT;
+  if (pass < 0 || pass > 2) return fail(h, FLB_ERR_INVALID_ARGUMENT, "pass must be 0, 1 or 2");
+  if (!h->fs && pass != 0) return fail(h, FLB_ERR_UNSUPPORTED, "free-surface pass on a mono-fluid case");
+  DeviceGuard guard(h->device);
+  refresh_params(h);
+  const uint32_t odd = (uint32_t)(h->t & 1u);
+  if (h->has_io && pass == 0) {
+    FLB_CUDA(h, cudaMemcpyAsync(h->d_rho_snap, h->d_rho, (size_t)h->N * h->c_size, cudaMemcpyDeviceToDevice,
+                                h->stream));
+    FLB_CUDA(h, cudaMemcpyAsync(h->d_u_snap, h->d_u, 2ull * h->N * h->c_size, cudaMemcpyDeviceToDevice, h->stream));
+  }
+  const bool recon = h->fs && h->d_recon_mask;
+  // alone, stream-collide sees no parked populations, and FS_1 writes its
+  // rebuilt populations into the population array like the reference kernel
+  if (pass == 0 && recon) FLB_CUDA(h, cudaMemsetAsync(h->d_recon_mask, 0, h->N, h->stream));
+  dispatch(h, [&](auto ops) {
+    if (pass == 0) ops.sc(h, odd, true);
+    else if (pass == 1) ops.fs1(h, odd);
+    else ops.fs234(h, odd);
+    if (pass == 1 && recon) ops.apply_recon(h, odd);
+  });
+  h->launches += (pass == 1 && recon) ? 2 : 1;
+  if (pass == 2)  // keep the current buffer index tied to t
+    FLB_CUDA(h, cudaMemcpyAsync(h->d_flags[h->cur], h->d_flags[h->cur ^ 1], h->N, cudaMemcpyDeviceToDevice,
+                                h->stream));
+  FLB_CUDA(h, cudaGetLastError());
+  FLB_CUDA(h, cudaStreamSynchronize(h->stream));
+  return FLB_OK;
+}
+
+FLB_API flb_status flb_profile_steps(flb_handle h, uint64_t n, double pass_ms[3]) {
+  if (!h || !pass_ms) return FLB_ERR_INVALID_ARGUMENT;
+  DeviceGuard guard(h->device);
+  pass_ms[0] = pass_ms[1] = pass_ms[2] = 0.0;
+  cudaEvent_t ev[4];
+  for (auto& e : ev) FLB_CUDA(h, cudaEventCreate(&e));
+  flb_status st = FLB_OK;
+  for (uint64_t k = 0; k < n && st == FLB_OK; k++) {
+    const uint32_t odd = (uint32_t)(h->t & 1u);
+    refresh_params(h);
+    if (h->has_io) {
+      cudaMemcpyAsync(h->d_rho_snap, h->d_rho, (size_t)h->N * h->c_size, cudaMemcpyDeviceToDevice, h->stream);
+      cudaMemcpyAsync(h->d_u_snap, h->d_u, 2ull * h->N * h->c_size, cudaMemcpyDeviceToDevice, h->stream);
+    }
+    cudaEventRecord(ev[0], h->stream);
+    if (h->fs) {
+      dispatch(h, [&](auto ops) { ops.fs1(h, odd); });
+      cudaEventRecord(ev[1], h->stream);
+      dispatch(h, [&](auto ops) { ops.sc(h, odd, true); });
+      cudaEventRecord(ev[2], h->stream);
+      dispatch(h, [&](auto ops) { ops.fs234(h, odd); });
+      cudaEventRecord(ev[3], h->stream);
+      h->launches += 3;
+      h->cur ^= 1;
+    } else {
+      cudaEventRecord(ev[1], h->stream);
+      dispatch(h, [&](auto ops) { ops.sc(h, odd, k + 1 == n || h->has_io); });
+      cudaEventRecord(ev[2], h->stream);
+      cudaEventRecord(ev[3], h->stream);
+      h->launches += 1;
+    }
+    h->t += 1;
+    cudaError_t e = cudaEventSynchronize(ev[3]);
+    if (e != cudaSuccess) {
+      st = cuda_fail(h, e, "cudaEventSynchronize");
+      break;
+    }
+    float a = 0, b = 0, c = 0;
+    cudaEventElapsedTime(&a, ev[0], ev[1]);
+    cudaEventElapsedTime(&b, ev[1], ev[2]);
+    cudaEventElapsedTime(&c, ev[2], ev[3]);
+    pass_ms[1] += a;
+    pass_ms[0] += b;
+    pass_ms[2] += c;
+  }
+  refresh_params(h);
+  for (auto& e : ev) cudaEventDestroy(e);
+  return st;
+}
+
+FLB_API flb_status flb_launch_count(flb_handle h, uint64_t* launches) {
+  if (!h || !launches) return FLB_ERR_INVALID_ARGUMENT;
+  *launches = h->launches;
+  return FLB_OK;
+}
+
+// ---- checkpoint ------------------------------------------------------------
+namespace {
+struct CkptHeader {
+  char magic[8];
+  uint32_t version, nx, ny, precision, mass_precision, free_surface, bounce_back, fs_mode;
+  uint64_t t;
+};
+}  // namespace
+
+FLB_API flb_status flb_save_checkpoint(flb_handle h, const char* path) {
+  if (!h || !path) return FLB_ERR_INVALID_ARGUMENT;
+  DeviceGuard guard(h->device);
+  CkptHeader hd{};
+  std::memcpy(hd.magic, "FLBCKPT1", 8);
+  hd.version = 1;
+  hd.nx = h->nx;
+  hd.ny = h->ny;
+  hd.precision = (uint32_t)h->desc.precision;
+  hd.mass_precision = (uint32_t)h->desc.mass_precision;
+  hd.free_surface = h->fs;
+  hd.bounce_back = (uint32_t)h->desc.bounce_back;
+  hd.fs_mode = (uint32_t)h->desc.fs_mode;
+  hd.t = h->t;
+  FILE* fp = std::fopen(path, "wb");
+  if (!fp) return fail(h, FLB_ERR_IO, std::string("cannot open ") + path);
+  std::fwrite(&hd, sizeof(hd), 1, fp);
+  struct Part { void* d; size_t bytes; };
+  std::vector<Part> parts = {{h->d_f, 9ull * h->N * h->s_size}, {h->d_rho, (size_t)h->N * h->c_size},
+                             {h->d_u, 2ull * h->N * h->c_size}, {h->d_flags[h->cur], h->N}};
+  if (h->fs) {
+    parts.push_back({h->d_mass, (size_t)h->N * h->m_size});
+    parts.push_back({h->d_excess, (size_t)h->N * h->m_size});
+    parts.push_back({h->d_phi, (size_t)h->N * h->m_size});
+  }
+  std::vector<char> buf;
+  for (const Part& p : parts) {
+    buf.resize(p.bytes);
+    cudaError_t e = cudaMemcpyAsync(buf.data(), p.d, p.bytes, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+      std::fclose(fp);
+      return cuda_fail(h, e, "checkpoint read-back");
+    }
+    if (std::fwrite(buf.data(), 1, p.bytes, fp) != p.bytes) {
+      std::fclose(fp);
+      return fail(h, FLB_ERR_IO, "short write");
+    }
+  }
+  std::fclose(fp);
+  return FLB_OK;
+}
+
+FLB_API flb_status flb_load_checkpoint(flb_handle h, const char* path) {
+  if (!h || !path) return FLB_ERR_INVALID_ARGUMENT;
+  DeviceGuard guard(h->device);
+  FILE* fp = std::fopen(path, "rb");
+  if (!fp) return fail(h, FLB_ERR_IO, std::string("cannot open ") + path);
+  CkptHeader hd{};
+  if (std::fread(&hd, sizeof(hd), 1, fp) != 1 || std::memcmp(hd.magic, "FLBCKPT1", 8) != 0) {
+    std::fclose(fp);
+    return fail(h, FLB_ERR_IO, "not a checkpoint file");
+  }
+  if (hd.nx != h->nx || hd.ny != h->ny || hd.precision != (uint32_t)h->desc.precision ||
+      hd.mass_precision != (uint32_t)h->desc.mass_precision || hd.free_surface != (uint32_t)h->fs ||
+      hd.bounce_back != (uint32_t)h->desc.bounce_back || hd.fs_mode != (uint32_t)h->desc.fs_mode) {
+    std::fclose(fp);
+    return fail(h, FLB_ERR_INVALID_ARGUMENT, "checkpoint was written by a different case configuration");
+  }
+  const int cur = (int)(hd.t & 1u) & (h->fs ? 1 : 0);
+  struct Part { void* d; size_t bytes; };
+  std::vector<Part> parts = {{h->d_f, 9ull * h->N * h->s_size}, {h->d_rho, (size_t)h->N * h->c_size},
+                             {h->d_u, 2ull * h->N * h->c_size}, {h->d_flags[cur], h->N}};
+  if (h->fs) {
+    parts.push_back({h->d_mass, (size_t)h->N * h->m_size});
+    parts.push_back({h->d_excess, (size_t)h->N * h->m_size});
+    parts.push_back({h->d_phi, (size_t)h->N * h->m_size});
+  }
+  std::vector<char> buf;
+  for (const Part& p : parts) {
+    buf.resize(p.bytes);
+    if (std::fread(buf.data(), 1, p.bytes, fp) != p.bytes) {
+      std::fclose(fp);
+      return fail(h, FLB_ERR_IO, "truncated checkpoint");
+    }
+    cudaError_t e = cudaMemcpyAsync(p.d, buf.data(), p.bytes, cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+      std::fclose(fp);
+      return cuda_fail(h, e, "checkpoint upload");
+    }
+  }
+  std::fclose(fp);
+  h->t = hd.t;
+  h->cur = cur;
+  refresh_params(h);
+  return FLB_OK;
+}
+
+FLB_API const char* flb_last_error(flb_handle h) { return h ? h->err.c_str() : "null handle"; }
+
+FLB_API const char* flb_status_string(flb_status s) {
+  const int i = (int)s;
+  return (i >= 0 && i < (int)(sizeof(kStatusText) / sizeof(kStatusText[0]))) ? kStatusText[i] : "unknown status";
+}
+
+FLB_API const char* flb_version(void) { return "flowlb-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

@@ -1,0 +1,138 @@
+// lattice.cuh -- D2Q9 constants and per-cell arithmetic of the engine.
+//
+// The formulas follow FlowLB src/cuda/cellCalculations.cuh with the same
+// operand order and literal types, so that with --fmad=false every float and
+// double operation rounds exactly as in the reference kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_fp16.h>
+
+namespace flb {
+
+// Cell-type bits, src/cuda/cudaInitData.cu:25-39 and src/utils.h:91-108.
+enum : uint8_t {
+  kFluid = 0x01,
+  kGas = 0x02,
+  kInterface = 0x04,
+  kWall = 0x08,
+  kMovingWall = 0x10,
+  kInlet = 0x20,
+  kOutlet = 0x40,
+  kGasInterface = 0x80,
+  kFGI = 0x07,
+  kIF = 0x05,
+  kIG = 0x06,
+  kInletFluid = 0x21
+};
+
+// Directions: 0 rest, 1 +x, 2 -x, 3 +y, 4 -y, 5 +x+y, 6 -x-y, 7 +x-y, 8 -x+y
+// (cudaInitData.cu:76,78); i and i+1 (odd i) are opposite.
+__host__ __device__ constexpr int cx(int i) {
+  return i == 1 || i == 5 || i == 7 ? 1 : (i == 2 || i == 6 || i == 8 ? -1 : 0);
+}
+__host__ __device__ constexpr int cy(int i) {
+  return i == 3 || i == 5 || i == 8 ? 1 : (i == 4 || i == 6 || i == 7 ? -1 : 0);
+}
+
+// Weights as the reference host builds them (src/ui/app.cpp:288 float, :304 double).
+template <class C>
+__host__ __device__ constexpr C wgt(int i) {
+  return i == 0 ? C(4) / C(9) : (i < 5 ? C(1) / C(9) : C(1) / C(36));
+}
+
+// ---- storage codecs -------------------------------------------------------
+// S is the storage type of the population array, C the arithmetic type.
+template <class S, class C>
+struct Codec {
+  __device__ __forceinline__ static C ld(const S* F, uint32_t a, int, float) { return (C)F[a]; }
+  __device__ __forceinline__ static void st(S* F, uint32_t a, int, C v, float) { F[a] = (S)v; }
+};
+
+// FP16S: binary16 holds (f_i - w_i) * scale; scale is a power of two.
+template <>
+struct Codec<__half, float> {
+  __device__ __forceinline__ static float ld(const __half* F, uint32_t a, int dir, float inv_scale) {
+    return __half2float(F[a]) * inv_scale + wgt<float>(dir);
+  }
+  __device__ __forceinline__ static void st(__half* F, uint32_t a, int dir, float v, float scale) {
+    F[a] = __float2half_rn((v - wgt<float>(dir)) * scale);
+  }
+};
+
+// ---- per-cell arithmetic, cellCalculations.cuh ----------------------------
+
+// calculateDensity, cellCalculations.cuh:16-22
+template <class C>
+__device__ __forceinline__ C density(const C* f) {
+  C rho = f[0];
+#pragma unroll
+  for (int i = 1; i < 9; i++) rho += f[i];
+  return rho;
+}
+
+// calculateVelocityD2Q9, cellCalculations.cuh:168-174
+template <class C>
+__device__ __forceinline__ void velocity(const C* f, C rho, C& ux, C& uy) {
+  ux = (f[1] - f[2] + f[5] - f[6] + f[7] - f[8]) / rho;
+  uy = (f[3] - f[4] + f[5] - f[6] + f[8] - f[7]) / rho;
+}
+
+// calculateEquilibriumDDF2Q9, cellCalculations.cuh:32-52
+template <class C>
+__device__ __forceinline__ void equilibrium(C rho, C ux, C uy, C* feq) {
+  const C u2 = 3.0f * (ux * ux + uy * uy);
+  const C rhow14 = wgt<C>(1) * rho;
+  const C rhow58 = wgt<C>(5) * rho;
+  ux *= 3.0f;
+  uy *= 3.0f;
+  const C u0 = ux - uy;
+  const C u1 = ux + uy;
+  feq[0] = wgt<C>(0) * rho * (1.0f - 0.5f * u2);
+  feq[1] = rhow14 * (1.0f + ux - 0.5f * u2 + 0.5f * ux * ux);
+  feq[2] = rhow14 * (1.0f - ux - 0.5f * u2 + 0.5f * ux * ux);
+  feq[3] = rhow14 * (1.0f + uy - 0.5f * u2 + 0.5f * uy * uy);
+  feq[4] = rhow14 * (1.0f - uy - 0.5f * u2 + 0.5f * uy * uy);
+  feq[5] = rhow58 * (1.0f + u1 - 0.5f * u2 + 0.5f * u1 * u1);
+  feq[6] = rhow58 * (1.0f - u1 - 0.5f * u2 + 0.5f * u1 * u1);
+  feq[7] = rhow58 * (1.0f + u0 - 0.5f * u2 + 0.5f * u0 * u0);
+  feq[8] = rhow58 * (1.0f - u0 - 0.5f * u2 + 0.5f * u0 * u0);
+}
+
+// calculateForcingTerms2D (Guo), cellCalculations.cuh:64-73
+template <class C>
+__device__ __forceinline__ void forcing(C* Fi, C ux, C uy, float Fx, float Fy) {
+  const C uF = -0.33333334f * (ux * Fx + uy * Fy);
+  Fi[0] = 9.0f * wgt<C>(0) * uF;
+#pragma unroll
+  for (int i = 1; i < 9; i++)
+    Fi[i] = 9.0f * wgt<C>(i) * ((cx(i) * Fx + cy(i) * Fy) * (cx(i) * ux + cy(i) * uy + 0.33333334f) + uF);
+}
+
+// calculatePhi, cellCalculations.cuh:153-158: the quotient is clamped in
+// float (__saturatef) whatever the precision.
+template <class M, class C>
+__device__ __forceinline__ M fill_level(M m, C rho) {
+  if (rho > 0.0f) return (M)__saturatef((float)(m / (M)rho));
+  return (M)0.5f;
+}
+
+// Neighbour cells with periodic wrap, cellCalculations.cuh:82-109.
+__device__ __forceinline__ void neighbours(uint32_t x, uint32_t y, uint32_t nx, uint32_t ny, uint32_t* nb) {
+  const uint32_t yc = y * nx;
+  const uint32_t yu = (y + 1u == ny ? 0u : y + 1u) * nx;
+  const uint32_t yd = (y == 0u ? ny - 1u : y - 1u) * nx;
+  const uint32_t xr = x + 1u == nx ? 0u : x + 1u;
+  const uint32_t xl = x == 0u ? nx - 1u : x - 1u;
+  nb[0] = x + yc;
+  nb[1] = xr + yc;
+  nb[2] = xl + yc;
+  nb[3] = x + yu;
+  nb[4] = x + yd;
+  nb[5] = xr + yu;
+  nb[6] = xl + yd;
+  nb[7] = xr + yd;
+  nb[8] = xl + yu;
+}
+
+}  // namespace flb

@@ -1,0 +1,265 @@
+"""Python binding of the engine's C ABI (``include/flowlb.h``).
+
+``Solver`` mirrors FlowLB's solver boundary (``src/cuda/runCuda.cuh:25-38``):
+construct from geometry flags and options, ``step(n)``, read back density,
+velocity, fill fraction and flags.  It is a thin ctypes layer over
+``libflowlb.so``; there is no CPU path: if the library cannot be loaded or no
+CUDA device is present, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libflowlb.so")
+
+FIELD_F, FIELD_RHO, FIELD_U, FIELD_FLAGS, FIELD_MASS, FIELD_EXCESS, FIELD_PHI = range(7)
+BB_IMPLICIT, BB_HALFWAY = 0, 1
+FS_REFERENCE, FS_CONSERVATIVE = 0, 1
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4: "unsupported",
+          5: "I/O error", 6: "non-finite populations", 7: "no CUDA device"}
+
+# Every symbol the header declares; tests check the library exports them all.
+EXPORTS = [
+    "flb_case_desc_init", "flb_create", "flb_reset", "flb_destroy", "flb_step", "flb_sync", "flb_get_time",
+    "flb_set_stream", "flb_get_stream", "flb_field_info", "flb_read_field", "flb_write_field", "flb_total_mass",
+    "flb_cell_counts", "flb_check_finite", "flb_run_pass", "flb_profile_steps", "flb_launch_count", "flb_save_checkpoint",
+    "flb_load_checkpoint", "flb_last_error", "flb_status_string", "flb_version",
+]
+
+
+class CaseDesc(C.Structure):
+    _fields_ = [
+        ("nx", C.c_uint32), ("ny", C.c_uint32), ("flags", C.c_void_p), ("free_surface", C.c_int32),
+        ("precision", C.c_int32), ("mass_precision", C.c_int32), ("collision", C.c_int32),
+        ("subgrid", C.c_int32), ("use_volumetric_force", C.c_int32), ("tau", C.c_float), ("fx", C.c_float),
+        ("fy", C.c_float), ("bounce_back", C.c_int32), ("fs_mode", C.c_int32), ("f16_scale", C.c_float),
+        ("device", C.c_int32), ("stream", C.c_void_p), ("inlet_ux", C.c_double), ("inlet_uy", C.c_double),
+    ]
+
+
+class FlowLBError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> C.CDLL:
+    """Loads libflowlb.so and declares the C signatures.  Raises if missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: build it with `python -c 'import __graft_entry__ as g; "
+                                f"g.build()'` or `make -C flowlb_b200/csrc`")
+    L = C.CDLL(path)
+    H = C.c_void_p
+    sig = {
+        "flb_case_desc_init": (None, [C.POINTER(CaseDesc)]),
+        "flb_create": (C.c_int, [C.POINTER(CaseDesc), C.POINTER(H)]),
+        "flb_reset": (C.c_int, [H, C.c_void_p]),
+        "flb_destroy": (C.c_int, [H]),
+        "flb_step": (C.c_int, [H, C.c_uint64]),
+        "flb_sync": (C.c_int, [H]),
+        "flb_get_time": (C.c_int, [H, C.POINTER(C.c_uint64)]),
+        "flb_set_stream": (C.c_int, [H, C.c_void_p]),
+        "flb_get_stream": (C.c_int, [H, C.POINTER(C.c_void_p)]),
+        "flb_field_info": (C.c_int, [H, C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+        "flb_read_field": (C.c_int, [H, C.c_int, C.c_void_p, C.c_int]),
+        "flb_write_field": (C.c_int, [H, C.c_int, C.c_void_p, C.c_int]),
+        "flb_total_mass": (C.c_int, [H, C.POINTER(C.c_double)]),
+        "flb_cell_counts": (C.c_int, [H, C.POINTER(C.c_uint64)]),
+        "flb_check_finite": (C.c_int, [H]),
+        "flb_run_pass": (C.c_int, [H, C.c_int]),
+        "flb_profile_steps": (C.c_int, [H, C.c_uint64, C.POINTER(C.c_double)]),
+        "flb_launch_count": (C.c_int, [H, C.POINTER(C.c_uint64)]),
+        "flb_save_checkpoint": (C.c_int, [H, C.c_char_p]),
+        "flb_load_checkpoint": (C.c_int, [H, C.c_char_p]),
+        "flb_last_error": (C.c_char_p, [H]),
+        "flb_status_string": (C.c_char_p, [C.c_int]),
+        "flb_version": (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _dtype(elem_size: int, field: int):
+    if field == FIELD_FLAGS:
+        return np.uint8
+    return {8: np.float64, 4: np.float32}[elem_size]
+
+
+class Solver:
+    """One case on one GPU.
+
+    Parameters mirror FlowLB's OptionsCalculation (``src/io/reader.h:98-127``):
+    ``free_surface`` (TYPE_PROBLEM), ``precision`` (PRECISION 64/32, plus 16 for
+    FP16 scaled-deviation storage), ``tau`` (RELAXATION_TIME), ``fx, fy``
+    (VOLUMETRIC_FORCE in lattice units), ``collision`` (0 SRT, 1 TRT),
+    ``subgrid`` (SUBGRID_TURBULENCE_MODEL).
+    """
+
+    def __init__(self, flags: np.ndarray, *, free_surface: bool = False, precision: int = 32,
+                 mass_precision: int = 64, tau: float = 0.6, fx: float = 0.0, fy: float = 0.0,
+                 use_force: bool = True, collision: int = 0, subgrid: bool = False,
+                 bounce_back: int = BB_HALFWAY, fs_mode: int = FS_CONSERVATIVE, inlet_ux: float = 0.0,
+                 inlet_uy: float = 0.0, f16_scale: float = 0.0, device: int = -1, stream: int | None = None):
+        L = load_library()
+        g = np.ascontiguousarray(flags, dtype=np.uint8)
+        if g.ndim != 2:
+            raise ValueError("flags must be a (ny, nx) array")
+        self.ny, self.nx = g.shape
+        self.N = self.nx * self.ny
+        d = CaseDesc()
+        L.flb_case_desc_init(C.byref(d))
+        d.nx, d.ny, d.flags = self.nx, self.ny, g.ctypes.data
+        d.free_surface = int(free_surface)
+        d.precision, d.mass_precision = int(precision), int(mass_precision)
+        d.collision, d.subgrid, d.use_volumetric_force = int(collision), int(subgrid), int(use_force)
+        d.tau, d.fx, d.fy = tau, fx, fy
+        d.inlet_ux, d.inlet_uy = inlet_ux, inlet_uy
+        d.bounce_back, d.fs_mode, d.f16_scale, d.device = int(bounce_back), int(fs_mode), f16_scale, int(device)
+        d.stream = stream or None
+        self._desc = d
+        self.free_surface = bool(free_surface)
+        self.precision = precision
+        h = C.c_void_p()
+        st = L.flb_create(C.byref(d), C.byref(h))
+        if st != 0:
+            raise FlowLBError(st, "flb_create failed")
+        self._h = h
+
+    # -- lifetime -------------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().flb_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _check(self, st: int):
+        if st != 0:
+            msg = load_library().flb_last_error(self._h)
+            raise FlowLBError(st, msg.decode() if msg else "")
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    # -- stepping -----------------------------------------------------------
+    def step(self, n: int = 1):
+        self._check(load_library().flb_step(self._h, int(n)))
+
+    def sync(self):
+        self._check(load_library().flb_sync(self._h))
+
+    def reset(self, flags: np.ndarray):
+        g = np.ascontiguousarray(flags, dtype=np.uint8)
+        assert g.shape == (self.ny, self.nx)
+        self._check(load_library().flb_reset(self._h, g.ctypes.data))
+
+    def run_pass(self, p: int):
+        self._check(load_library().flb_run_pass(self._h, int(p)))
+
+    @property
+    def t(self) -> int:
+        v = C.c_uint64()
+        self._check(load_library().flb_get_time(self._h, C.byref(v)))
+        return int(v.value)
+
+    @property
+    def stream(self) -> int:
+        v = C.c_void_p()
+        self._check(load_library().flb_get_stream(self._h, C.byref(v)))
+        return int(v.value or 0)
+
+    def set_stream(self, stream: int | None):
+        self._check(load_library().flb_set_stream(self._h, stream or None))
+
+    @property
+    def launches(self) -> int:
+        v = C.c_uint64()
+        self._check(load_library().flb_launch_count(self._h, C.byref(v)))
+        return int(v.value)
+
+    # -- fields ---------------------------------------------------------------
+    def field_info(self, field: int) -> tuple[int, int]:
+        es, n = C.c_size_t(), C.c_size_t()
+        self._check(load_library().flb_field_info(self._h, field, C.byref(es), C.byref(n)))
+        return int(es.value), int(n.value)
+
+    def read(self, field: int, out: np.ndarray | None = None) -> np.ndarray:
+        es, n = self.field_info(field)
+        dt = _dtype(es, field)
+        if out is None:
+            out = np.empty(n, dtype=dt)
+        assert out.dtype == dt and out.size == n and out.flags.c_contiguous
+        self._check(load_library().flb_read_field(self._h, field, out.ctypes.data, 0))
+        return out
+
+    def read_device(self, field: int, dst_ptr: int):
+        self._check(load_library().flb_read_field(self._h, field, C.c_void_p(dst_ptr), 1))
+
+    def write(self, field: int, values: np.ndarray):
+        es, n = self.field_info(field)
+        v = np.ascontiguousarray(values, dtype=_dtype(es, field))
+        assert v.size == n
+        self._check(load_library().flb_write_field(self._h, field, v.ctypes.data, 0))
+
+    f = property(lambda self: self.read(FIELD_F))
+    rho = property(lambda self: self.read(FIELD_RHO))
+    u = property(lambda self: self.read(FIELD_U))
+    flags = property(lambda self: self.read(FIELD_FLAGS))
+    mass = property(lambda self: self.read(FIELD_MASS))
+    excess = property(lambda self: self.read(FIELD_EXCESS))
+    phi = property(lambda self: self.read(FIELD_PHI))
+
+    def total_mass(self) -> float:
+        v = C.c_double()
+        self._check(load_library().flb_total_mass(self._h, C.byref(v)))
+        return float(v.value)
+
+    def cell_counts(self) -> dict:
+        arr = (C.c_uint64 * 4)()
+        self._check(load_library().flb_cell_counts(self._h, arr))
+        return dict(fluid=int(arr[0]), interface=int(arr[1]), gas=int(arr[2]), wall=int(arr[3]))
+
+    def check_finite(self) -> bool:
+        st = load_library().flb_check_finite(self._h)
+        if st == 6:
+            return False
+        self._check(st)
+        return True
+
+    def profile_steps(self, n: int) -> dict:
+        """Runs n steps with CUDA events around every pass; device ms per pass kind."""
+        arr = (C.c_double * 3)()
+        self._check(load_library().flb_profile_steps(self._h, int(n), arr))
+        return dict(stream_collide=arr[0], fs1=arr[1], fs234=arr[2])
+
+    def save_checkpoint(self, path: str):
+        self._check(load_library().flb_save_checkpoint(self._h, path.encode()))
+
+    def load_checkpoint(self, path: str):
+        self._check(load_library().flb_load_checkpoint(self._h, path.encode()))

@@ -1,0 +1,182 @@
+/*
+ * flowlb.h -- C ABI of the B200 D2Q9 lattice-Boltzmann engine.
+ *
+ * Drop-in for the solver path of FlowLB (a 2D culvert-flow LBM with a VOF
+ * free surface).  FlowLB's solver boundary is the C++ template set of
+ * src/cuda/runCuda.cuh:25-38 (h_launchCudaCalculations2D and the four run
+ * loops), called only from App::calculate (src/ui/app.cpp:293,310).  That
+ * boundary allocates every device buffer (runCuda.cu:85, cudaInitData.cuh:90-125),
+ * initialises the state on the host (initData.h:220-333), runs the time loop
+ * (runCuda.cu:460-528) and copies density, velocity, fill level and flags back
+ * to host vectors for the VTK writer (cudaUtils.cuh:42-53).  This header
+ * splits that into handle-based calls with plain pointers and status codes:
+ *
+ *   flb_create / flb_reset       <- h_initDataCuda2D + initData + h_initConstantDataCuda2D
+ *   flb_step                     <- the body of the run loops, n time steps
+ *   flb_read_field               <- CudaUtils::copyDataFromDevice
+ *   flb_destroy                  <- the cudaFree block, runCuda.cu:111-127
+ *
+ * Conventions.  Every function returns flb_status (never exits the process);
+ * flb_last_error() gives a message.  Calls on one handle must not overlap;
+ * different handles are independent.  All device work of a handle is issued
+ * on one CUDA stream (the caller's, if given).  Arrays are structure-of-arrays
+ * in the reference layout: cell c = x + y*nx; DDF slot s of cell c at
+ * f[c + s*N]; u[c] = u_x, u[c + N] = u_y.  Cell flags use the reference's
+ * uint8 encoding (src/utils.h:91-108): FLUID 0x01, GAS 0x02, INTERFACE 0x04,
+ * WALL 0x08, MOVING_WALL 0x10, INLET 0x20, OUTLET 0x40, GAS_INTERFACE 0x80.
+ */
+#ifndef FLOWLB_H
+#define FLOWLB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define FLB_API __attribute__((visibility("default")))
+#else
+#define FLB_API
+#endif
+
+typedef enum flb_status {
+  FLB_OK = 0,
+  FLB_ERR_INVALID_ARGUMENT = 1,
+  FLB_ERR_CUDA = 2,
+  FLB_ERR_OUT_OF_MEMORY = 3,
+  FLB_ERR_UNSUPPORTED = 4,
+  FLB_ERR_IO = 5,
+  FLB_ERR_NONFINITE = 6,
+  FLB_ERR_NO_DEVICE = 7
+} flb_status;
+
+/* Storage precision of the populations (OptionsCalc.txt PRECISION,
+ * src/io/reader.cpp:367).  16 stores (f_i - w_i) * f16_scale in binary16 and
+ * computes in float. */
+enum { FLB_PRECISION_F64 = 64, FLB_PRECISION_F32 = 32, FLB_PRECISION_F16S = 16 };
+
+/* Wall treatment.  IMPLICIT mirrors the reference: solid cells are skipped and
+ * a population sent into one returns two steps later.  HALFWAY reflects it
+ * into the opposite direction for the next step. */
+enum { FLB_BB_IMPLICIT = 0, FLB_BB_HALFWAY = 1 };
+
+/* Free-surface semantics.  REFERENCE mirrors lbmKernel2D.cu:14-303.
+ * CONSERVATIVE weights interface mass exchange symmetrically with the stored
+ * fill levels, reconstructs the populations that arrive from gas neighbours,
+ * and hands excess mass only to cells that collect it; with FP64 mass and
+ * HALFWAY walls it conserves total fluid mass to round-off. */
+enum { FLB_FS_REFERENCE = 0, FLB_FS_CONSERVATIVE = 1 };
+
+/* Collision operator (reference d_collisionOperator). */
+enum { FLB_COLLISION_SRT = 0, FLB_COLLISION_TRT = 1 };
+
+/* Field ids for flb_read_field / flb_write_field / flb_field_info. */
+enum {
+  FLB_FIELD_F = 0,       /* 9N populations, arithmetic type, reference slot layout */
+  FLB_FIELD_RHO = 1,     /* N, arithmetic type */
+  FLB_FIELD_U = 2,       /* 2N, arithmetic type */
+  FLB_FIELD_FLAGS = 3,   /* N, uint8 */
+  FLB_FIELD_MASS = 4,    /* N, mass type (free surface) */
+  FLB_FIELD_EXCESS = 5,  /* N, mass type (free surface) */
+  FLB_FIELD_PHI = 6      /* N, mass type (free surface): fill fraction */
+};
+
+/* Case description.  Fill with flb_case_desc_init() and override. */
+typedef struct flb_case_desc {
+  uint32_t nx, ny;            /* lattice size; N = nx*ny, 9N < 2^32 */
+  const uint8_t* flags;       /* host geometry flags, N bytes: FLUID/GAS/WALL/INLET/OUTLET cells as
+                                 the reference's geometry stage produces them (initData.h:256-317) */
+  int32_t free_surface;       /* TYPE_PROBLEM: 0 MONOFLUID, 1 FREE_SURFACE */
+  int32_t precision;          /* FLB_PRECISION_* */
+  int32_t mass_precision;     /* 64 or 32 (32 only with precision 32) */
+  int32_t collision;          /* FLB_COLLISION_* */
+  int32_t subgrid;            /* Smagorinsky subgrid model */
+  int32_t use_volumetric_force;
+  float tau;                  /* relaxation time (> 0.5) */
+  float fx, fy;               /* body force density in lattice units */
+  int32_t bounce_back;        /* FLB_BB_* */
+  int32_t fs_mode;            /* FLB_FS_* */
+  float f16_scale;            /* power of two; 0 selects 4096 */
+  int32_t device;             /* CUDA device ordinal; -1 = current */
+  void* stream;               /* cudaStream_t to issue on; NULL = a stream owned by the handle */
+  double inlet_ux, inlet_uy;  /* lattice velocity of INLET cells (double, as the reference's LBVelocity) */
+} flb_case_desc;
+
+typedef struct flb_engine* flb_handle;
+
+FLB_API void flb_case_desc_init(flb_case_desc* desc);
+
+/* Allocates the device state and builds the initial state on the device from
+ * desc->flags (host): f = feq(rho=1, u) stored with the t=1 esoteric pattern,
+ * and for free surface the interface layer, fill level and mass
+ * (initData.h:125-206, initData.cpp:13-37).  Replaces h_launchCudaCalculations2D's
+ * set-up half, runCuda.cu:34-85. */
+FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out);
+
+/* Rebuilds the initial state from new host geometry flags of the same size and
+ * sets t = 0, reusing the device buffers. */
+FLB_API flb_status flb_reset(flb_handle h, const uint8_t* host_flags);
+
+FLB_API flb_status flb_destroy(flb_handle h);
+
+/* Advances n time steps asynchronously on the handle's stream: per step
+ * FS_1, stream-collide, FS_2..4 (free surface) or stream-collide alone.
+ * Replaces the loop bodies of runCuda.cu:473-490 and :506-527. */
+FLB_API flb_status flb_step(flb_handle h, uint64_t n);
+
+FLB_API flb_status flb_sync(flb_handle h);
+FLB_API flb_status flb_get_time(flb_handle h, uint64_t* t);
+FLB_API flb_status flb_set_stream(flb_handle h, void* stream);
+FLB_API flb_status flb_get_stream(flb_handle h, void** stream);
+
+/* Element size and element count of a field (0 count: not held in this mode). */
+FLB_API flb_status flb_field_info(flb_handle h, int field, size_t* elem_size, size_t* count);
+
+/* Copies a field into dst (host memory when on_device = 0, device memory of the
+ * handle's GPU when 1) and waits for the copy.  Replaces copyDataFromDevice,
+ * cudaUtils.cuh:42-53; on_device = 1 is the headless stand-in for the OpenGL
+ * interop buffers of runCuda.cu:137-147. */
+FLB_API flb_status flb_read_field(flb_handle h, int field, void* dst, int on_device);
+
+/* Overwrites a field from src (same element type as flb_field_info). */
+FLB_API flb_status flb_write_field(flb_handle h, int field, const void* src, int on_device);
+
+/* Total fluid mass in FP64: free surface, the sum of cell masses plus the
+ * excess mass its neighbours will collect next step; mono-fluid, the sum of
+ * the populations the next step loads into non-solid cells. */
+FLB_API flb_status flb_total_mass(flb_handle h, double* mass);
+
+/* Cell-type census: counts[0..3] = fluid, interface, gas, solid(wall). */
+FLB_API flb_status flb_cell_counts(flb_handle h, uint64_t counts[4]);
+
+/* FLB_ERR_NONFINITE if any population of a non-solid cell is NaN or Inf. */
+FLB_API flb_status flb_check_finite(flb_handle h);
+
+/* Runs one pass of the step at the current t without advancing it (parity
+ * testing): 0 stream-collide, 1 FS_1 (mass exchange), 2 FS_2..4 (flag and
+ * mass finalisation). */
+FLB_API flb_status flb_run_pass(flb_handle h, int pass);
+
+/* Runs n time steps with a CUDA event around every pass on the handle's
+ * stream (no graphs) and returns the summed device time per pass kind in
+ * milliseconds: pass_ms[0] stream-collide, [1] FS_1, [2] FS_2..4.  Advances t. */
+FLB_API flb_status flb_profile_steps(flb_handle h, uint64_t n, double pass_ms[3]);
+
+/* Kernels this handle has launched so far (graph replays count each kernel). */
+FLB_API flb_status flb_launch_count(flb_handle h, uint64_t* launches);
+
+/* Binary checkpoint of the full state (populations, t, flags, mass, excess,
+ * fill level, density, velocity); the reference has none. */
+FLB_API flb_status flb_save_checkpoint(flb_handle h, const char* path);
+FLB_API flb_status flb_load_checkpoint(flb_handle h, const char* path);
+
+FLB_API const char* flb_last_error(flb_handle h);
+FLB_API const char* flb_status_string(flb_status s);
+FLB_API const char* flb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,120 @@
+// ref_cuda_harness.cu -- runs the reference's own CUDA kernels headless.
+//
+// TEST INFRASTRUCTURE ONLY.  Built by oracle/Makefile together with FlowLB's
+// src/cuda/lbmKernel2D.cu, src/cuda/cudaInitData.cu and src/utils.cpp
+// (compiled where they lie in the reference tree, with --fmad=false so that
+// every float operation rounds as written) into oracle/_ref/libflbref_cuda.so.
+//
+// The reference's headless loops (src/cuda/runCuda.cu:460-528) include the GUI
+// and OpenGL headers and cannot be built here, so this file re-states their
+// launch sequence: constants via FLB::h_initConstantDataCuda2D
+// (cudaInitData.cu:57-108), buffers via FLB::h_initDataCuda2D
+// (cudaInitData.cuh:90-125), 16x16 blocks and a ceil-divided grid
+// (cudaUtils.cu:89-105), and per step FS_1, StreamCollide, FS_2, FS_3, FS_4
+// (free surface) or StreamCollide alone (mono-fluid).
+#include <cstdint>
+#include <cstring>
+
+#include <cuda_runtime.h>
+
+#include "cudaInitData.cuh"
+#include "lbmKernel2D.cuh"
+
+namespace {
+
+template <typename P>
+int run_ref(int nx, int ny, int free_surface, int collision, int subgrid, int use_force, double tau, double fx,
+            double fy, uint64_t t0, uint64_t nsteps, int kernel_id, void* f, void* rho, void* u, uint8_t* flags,
+            void* mass, void* excess, void* phi) {
+  const unsigned int Nx = (unsigned)nx, Ny = (unsigned)ny, N = Nx * Ny;
+  static float wf[9] = {4.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f,
+                        1.0f / 36.0f, 1.0f / 36.0f, 1.0f / 36.0f, 1.0f / 36.0f};
+  static double wd[9] = {4.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0,
+                         1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0};
+  FLB::OptionsCalculation opts;
+  opts.graphicsAPI = FLB::API::NONE;
+  opts.typeProblem = free_surface ? FLB::TypeProblem::FREE_SURFACE : FLB::TypeProblem::MONOFLUID;
+  opts.collisionOperator = (uint8_t)collision;
+  opts.useSubgridModel = subgrid != 0;
+  opts.useVolumetricForce = use_force != 0;
+  opts.relaxationTime = tau;
+  opts.volumetricForce.x = fx;
+  opts.volumetricForce.y = fy;
+  opts.precision = sizeof(P) == 4 ? 32 : 64;
+  FLB::Units units;  // unit parameters 1: lattice units pass through
+  FLB::h_initConstantDataCuda2D<P>(opts, sizeof(P) == 4 ? (P*)(void*)wf : (P*)(void*)wd, Nx, Ny, N, units);
+
+  P *d_f = nullptr, *d_u = nullptr, *d_rho = nullptr, *d_mass = nullptr, *d_excess = nullptr, *d_phi = nullptr;
+  uint8_t* d_flags = nullptr;
+  FLB::h_initDataCuda2D<P>(opts, N, 2, 9, &d_f, (P*)f, &d_u, (P*)u, &d_flags, flags, &d_mass, (P*)mass, &d_rho,
+                           (P*)rho, &d_excess, (P*)excess, &d_phi, (P*)phi);
+  dim3 block(16, 16);
+  dim3 grid((Nx + block.x - 1) / block.x, (Ny + block.y - 1) / block.y);
+  if (kernel_id >= 0) {
+    const unsigned long t = (unsigned long)t0;
+    switch (kernel_id) {
+      case 0: FLB::d_StreamCollide2D<P, 9><<<grid, block>>>(d_f, d_rho, d_u, d_flags, d_mass, t); break;
+      case 1: FLB::d_FreeSurface2D_1<P, 9><<<grid, block>>>(d_f, d_rho, d_u, d_flags, d_mass, d_excess, d_phi, t); break;
+      case 2: FLB::d_FreeSurface2D_2<9><<<grid, block>>>(d_flags); break;
+      case 3: FLB::d_FreeSurface2D_3<P, 9><<<grid, block>>>(d_f, d_rho, d_u, d_flags, t); break;
+      case 4: FLB::d_FreeSurface2D_4<P, 9><<<grid, block>>>(d_rho, d_flags, d_mass, d_excess, d_phi); break;
+      default: break;
+    }
+  } else {
+    for (uint64_t k = 0; k < nsteps; k++) {
+      const unsigned long t = (unsigned long)(t0 + k);
+      if (free_surface) {
+        FLB::d_FreeSurface2D_1<P, 9><<<grid, block>>>(d_f, d_rho, d_u, d_flags, d_mass, d_excess, d_phi, t);
+        FLB::d_StreamCollide2D<P, 9><<<grid, block>>>(d_f, d_rho, d_u, d_flags, d_mass, t);
+        FLB::d_FreeSurface2D_2<9><<<grid, block>>>(d_flags);
+        FLB::d_FreeSurface2D_3<P, 9><<<grid, block>>>(d_f, d_rho, d_u, d_flags, t);
+        FLB::d_FreeSurface2D_4<P, 9><<<grid, block>>>(d_rho, d_flags, d_mass, d_excess, d_phi);
+      } else {
+        FLB::d_StreamCollide2D<P, 9><<<grid, block>>>(d_f, d_rho, d_u, d_flags, d_mass, t);
+      }
+    }
+  }
+  cudaError_t err = cudaDeviceSynchronize();
+  if (err == cudaSuccess) err = cudaGetLastError();
+  if (err == cudaSuccess) {
+    cudaMemcpy(f, d_f, 9ull * N * sizeof(P), cudaMemcpyDeviceToHost);
+    cudaMemcpy(rho, d_rho, (size_t)N * sizeof(P), cudaMemcpyDeviceToHost);
+    cudaMemcpy(u, d_u, 2ull * N * sizeof(P), cudaMemcpyDeviceToHost);
+    cudaMemcpy(flags, d_flags, N, cudaMemcpyDeviceToHost);
+    if (free_surface) {
+      cudaMemcpy(mass, d_mass, (size_t)N * sizeof(P), cudaMemcpyDeviceToHost);
+      cudaMemcpy(excess, d_excess, (size_t)N * sizeof(P), cudaMemcpyDeviceToHost);
+      cudaMemcpy(phi, d_phi, (size_t)N * sizeof(P), cudaMemcpyDeviceToHost);
+    }
+    err = cudaGetLastError();
+  }
+  cudaFree(d_f);
+  cudaFree(d_rho);
+  cudaFree(d_u);
+  cudaFree(d_flags);
+  if (free_surface) {
+    cudaFree(d_mass);
+    cudaFree(d_excess);
+    cudaFree(d_phi);
+  }
+  return err == cudaSuccess ? 0 : (int)err;
+}
+
+}  // namespace
+
+// kernel_id < 0: run nsteps full steps from t0; otherwise run that one kernel
+// (0 StreamCollide, 1..4 FreeSurface_1..4) once at t0.  All buffers are host
+// memory in the reference layout and are updated in place.
+extern "C" int ref_cuda_run(int precision, int nx, int ny, int free_surface, int collision, int subgrid,
+                            int use_force, double tau, double fx, double fy, uint64_t t0, uint64_t nsteps,
+                            int kernel_id, void* f, void* rho, void* u, uint8_t* flags, void* mass, void* excess,
+                            void* phi) {
+  if (nx < 3 || ny < 3) return -1;
+  if (precision == 32)
+    return run_ref<float>(nx, ny, free_surface, collision, subgrid, use_force, tau, fx, fy, t0, nsteps, kernel_id, f,
+                          rho, u, flags, mass, excess, phi);
+  if (precision == 64)
+    return run_ref<double>(nx, ny, free_surface, collision, subgrid, use_force, tau, fx, fy, t0, nsteps, kernel_id,
+                           f, rho, u, flags, mass, excess, phi);
+  return -1;
+}

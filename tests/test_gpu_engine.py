@@ -1,0 +1,301 @@
+"""GPU parity of the engine (through the C ABI) against the CPU oracle.
+
+The engine is built with --fmad=false and keeps the reference's operand
+order, so in every storage mode its fields must equal the oracle's exactly
+(value equality; only the sign of a zero may differ).
+"""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+from conftest import exact_equal, first_mismatch
+from flowlb_b200 import cases
+from flowlb_b200 import engine as E
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+# oracle variant -> (precision, mass_precision)
+PREC = {O.F64: (64, 64), O.F32: (32, 64), O.F32_M32: (32, 32), O.F16S: (16, 64)}
+VNAME = {O.F64: "f64", O.F32: "f32", O.F32_M32: "f32m32", O.F16S: "f16s"}
+
+
+def make_pair(flags, variant, *, free_surface=False, bb=O.BB_IMPLICIT, fs_mode=O.FS_REFERENCE, tau=0.6, fx=0.0,
+              fy=0.0, collision=0, subgrid=False, use_force=True, inlet=(0.0, 0.0)):
+    prec, mprec = PREC[variant]
+    s = E.Solver(flags, free_surface=free_surface, precision=prec, mass_precision=mprec, tau=tau, fx=fx, fy=fy,
+                 use_force=use_force, collision=collision, subgrid=subgrid, bounce_back=bb, fs_mode=fs_mode,
+                 inlet_ux=inlet[0], inlet_uy=inlet[1])
+    o = O.Oracle(flags, O.OracleConfig(variant=variant, free_surface=free_surface, bb=bb, fs_mode=fs_mode, tau=tau,
+                                       fx=fx, fy=fy, collision=collision, subgrid=subgrid, use_force=use_force,
+                                       inlet_ux=inlet[0], inlet_uy=inlet[1]))
+    return s, o
+
+
+def oracle_f(o, variant):
+    f = o.f64()
+    return f.astype(np.float32) if variant in (O.F32, O.F32_M32, O.F16S) else f
+
+
+def assert_same_state(s, o, variant, fs, what=""):
+    checks = [("f", s.f, oracle_f(o, variant)), ("rho", s.rho, o.rho), ("u", s.u, o.u), ("flags", s.flags, o.flags)]
+    if fs:
+        checks += [("mass", s.mass, o.mass), ("excess", s.excess, o.excess), ("phi", s.phi, o.phi)]
+    for name, a, b in checks:
+        assert exact_equal(a, b), f"{what} {name}: {first_mismatch(a, b)}"
+
+
+@pytest.fixture(scope="module")
+def channel():
+    return cases.plain_channel()
+
+
+@pytest.mark.parametrize("variant,bb", [(O.F32, O.BB_IMPLICIT), (O.F32, O.BB_HALFWAY), (O.F64, O.BB_IMPLICIT),
+                                        (O.F64, O.BB_HALFWAY), (O.F16S, O.BB_HALFWAY),
+                                        (O.F32_M32, O.BB_IMPLICIT)],
+                         ids=lambda v: str(v))
+def test_single_phase_steps_match_oracle(channel, variant, bb):
+    s, o = make_pair(channel.flags, variant, bb=bb, tau=channel.tau, fx=1e-5)
+    assert_same_state(s, o, variant, False, "init")
+    for n in (1, 2, 37, 80):  # single steps, a graph pair, graphs of 32 steps
+        s.step(n)
+        o.step(n)
+        assert s.t == o.t
+        assert_same_state(s, o, variant, False, f"t={o.t}")
+    s.close()
+
+
+@pytest.mark.parametrize("variant,bb,fs_mode", [
+    (O.F32_M32, O.BB_IMPLICIT, O.FS_REFERENCE),
+    (O.F64, O.BB_IMPLICIT, O.FS_REFERENCE),
+    (O.F32, O.BB_HALFWAY, O.FS_CONSERVATIVE),
+    (O.F64, O.BB_HALFWAY, O.FS_CONSERVATIVE),
+    (O.F16S, O.BB_HALFWAY, O.FS_CONSERVATIVE),
+    (O.F32, O.BB_IMPLICIT, O.FS_CONSERVATIVE),
+    (O.F32, O.BB_HALFWAY, O.FS_REFERENCE),
+], ids=lambda v: str(v))
+def test_free_surface_steps_match_oracle(variant, bb, fs_mode):
+    c = cases.small_dam_break(96, 64)
+    s, o = make_pair(c.flags, variant, free_surface=True, bb=bb, fs_mode=fs_mode, tau=c.tau, fy=c.fy)
+    assert_same_state(s, o, variant, True, "init")
+    for n in (1, 3, 40, 76):
+        s.step(n)
+        o.step(n)
+        assert_same_state(s, o, variant, True, f"t={o.t}")
+    s.close()
+
+
+def _random_state(flags, variant, fs, rng):
+    """Random but physical state: populations near equilibrium weights, a mix
+    of cell types, masses and fill levels in range."""
+    ny, nx = flags.shape
+    N = nx * ny
+    w = np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4)
+    f = (np.repeat(w, N) * (1 + 0.05 * rng.standard_normal(9 * N)))
+    st = dict(f=f)
+    if fs:
+        st["mass"] = rng.uniform(-0.05, 1.05, N)
+        st["excess"] = rng.uniform(-0.01, 0.01, N)
+        st["phi"] = rng.uniform(0, 1, N)
+        st["rho"] = 1 + 0.02 * rng.standard_normal(N)
+        st["u"] = 0.05 * rng.standard_normal(2 * N)
+    return st
+
+
+def _plant(s, o, st, flags_now, variant):
+    cdt = np.float64 if variant == O.F64 else np.float32
+    if variant == O.F16S:
+        # store through the engine's encoder, read the quantised values back
+        s.write(E.FIELD_F, st["f"].astype(np.float32))
+        o.f[:] = ((st["f"].astype(np.float32) - np.repeat(np.array(
+            [4 / 9] + [1 / 9] * 4 + [1 / 36] * 4, np.float32), o.N)) * np.float32(4096)).astype(np.float16)
+    else:
+        s.write(E.FIELD_F, st["f"].astype(cdt))
+        o.f[:] = st["f"].astype(cdt)
+    s.write(E.FIELD_FLAGS, flags_now)
+    o.flags[:] = flags_now
+    for k, fid in (("rho", E.FIELD_RHO), ("u", E.FIELD_U)):
+        if k in st:
+            s.write(fid, st[k].astype(cdt))
+            getattr(o, k)[:] = st[k].astype(cdt)
+    mdt = np.float32 if variant == O.F32_M32 else np.float64
+    for k, fid in (("mass", E.FIELD_MASS), ("excess", E.FIELD_EXCESS), ("phi", E.FIELD_PHI)):
+        if k in st:
+            s.write(fid, st[k].astype(mdt))
+            getattr(o, k)[:] = st[k].astype(mdt)
+
+
+@pytest.mark.parametrize("variant", [O.F32_M32, O.F64, O.F32, O.F16S], ids=lambda v: VNAME[v])
+@pytest.mark.parametrize("fs_mode,bb", [(O.FS_REFERENCE, O.BB_IMPLICIT), (O.FS_CONSERVATIVE, O.BB_HALFWAY)])
+@pytest.mark.parametrize("t_parity", [0, 1])
+def test_each_pass_matches_oracle_on_random_states(variant, fs_mode, bb, t_parity):
+    """Each pass from a random free-surface state with every cell type mixed
+    in: stream-collide (0), FS_1 (1), FS_2..4 fused (2)."""
+    rng = np.random.default_rng(1234 + variant + 10 * t_parity)
+    ny, nx = 40, 72
+    geo = np.full((ny, nx), cases.GAS, np.uint8)
+    geo[0, :] = geo[-1, :] = cases.WALL
+    geo[:, 0] = cases.WALL
+    for p, okr in ((0, None),):
+        pass
+    s, o = make_pair(geo, variant, free_surface=True, bb=bb, fs_mode=fs_mode, tau=0.57, fx=2e-5, fy=-3e-5)
+    choices = np.array([cases.FLUID, cases.GAS, cases.INTERFACE, cases.INTERFACE_FLUID, cases.INTERFACE_GAS,
+                        cases.GAS_INTERFACE], np.uint8)
+    for pass_id, oracle_kernels in ((0, [O.K_STREAM_COLLIDE]), (1, [O.K_FS1]), (2, [O.K_FS2, O.K_FS3, O.K_FS4])):
+        flags_now = choices[rng.integers(0, len(choices), nx * ny)].reshape(ny, nx)
+        if pass_id != 2:  # the stream-collide and FS_1 inputs hold settled types only
+            flags_now = np.where(np.isin(flags_now, [cases.INTERFACE_FLUID, cases.INTERFACE_GAS]), cases.INTERFACE,
+                                 flags_now)
+            flags_now = np.where(flags_now == cases.GAS_INTERFACE, cases.GAS, flags_now).astype(np.uint8)
+        flags_now[geo == cases.WALL] = cases.WALL
+        st = _random_state(geo, variant, True, rng)
+        _plant(s, o, st, flags_now.ravel(), variant)
+        o.t = t_parity
+        if s.t != t_parity:
+            s.step(1)  # advance the engine's clock to the parity
+            _plant(s, o, st, flags_now.ravel(), variant)
+        s.run_pass(pass_id)
+        for k in oracle_kernels:
+            o.kernel(k)
+        assert_same_state(s, o, variant, True, f"pass {pass_id}")
+    s.close()
+
+
+@pytest.mark.parametrize("variant", [O.F32, O.F64])
+def test_subgrid_and_trt_options_match_oracle(channel, variant):
+    for kw in (dict(subgrid=True), dict(collision=1, use_force=False), dict(collision=1, subgrid=True,
+                                                                           use_force=False)):
+        s, o = make_pair(channel.flags, variant, tau=0.52, fx=3e-5, **kw)
+        s.step(45)
+        o.step(45)
+        assert_same_state(s, o, variant, False, str(kw))
+        s.close()
+
+
+def test_inlet_outlet_match_oracle():
+    flags = cases.plain_channel(96, 32).flags.copy()
+    flags[1:-1, 0] = cases.INLET
+    flags[1:-1, -1] = cases.OUTLET
+    for variant in (O.F32, O.F64):
+        s, o = make_pair(flags, variant, tau=0.7, fx=0.0, inlet=(0.04, 0.0), use_force=False)
+        s.step(33)
+        o.step(33)
+        assert_same_state(s, o, variant, False, "inlet/outlet")
+        s.close()
+
+
+def test_total_mass_and_cell_counts():
+    c = cases.small_dam_break(96, 64)
+    s, o = make_pair(c.flags, O.F64, free_surface=True, bb=O.BB_HALFWAY, fs_mode=O.FS_CONSERVATIVE, tau=c.tau,
+                     fy=c.fy)
+    s.step(25)
+    o.step(25)
+    assert abs(s.total_mass() - o.total_mass()) <= 1e-12 * abs(o.total_mass())
+    fl = o.flags
+    cnt = s.cell_counts()
+    assert cnt["fluid"] == int(((fl & 7) == 1).sum() - ((fl & 0x08) & ((fl & 7) == 1)).sum())
+    assert cnt["interface"] == int(((fl & 7) == 4).sum())
+    assert cnt["wall"] == int(((fl & 8) != 0).sum())
+    assert s.check_finite()
+    ch = cases.plain_channel()
+    s2, o2 = make_pair(ch.flags, O.F32, bb=O.BB_HALFWAY, tau=ch.tau, fx=1e-5)
+    s2.step(11)
+    o2.step(11)
+    assert abs(s2.total_mass() - o2.total_mass()) <= 1e-12 * abs(o2.total_mass())
+    s.close()
+    s2.close()
+
+
+def test_checkpoint_roundtrip_continues_identically():
+    c = cases.small_dam_break(64, 48)
+    kw = dict(free_surface=True, precision=32, tau=c.tau, fy=c.fy)
+    a = E.Solver(c.flags, **kw)
+    b = E.Solver(c.flags, **kw)
+    a.step(17)
+    with tempfile.TemporaryDirectory() as d:
+        p = os.path.join(d, "ck.bin")
+        a.save_checkpoint(p)
+        b.load_checkpoint(p)
+    assert b.t == 17
+    a.step(40)
+    b.step(40)
+    for fid in (E.FIELD_F, E.FIELD_FLAGS, E.FIELD_MASS, E.FIELD_RHO):
+        assert exact_equal(a.read(fid), b.read(fid))
+    a.close()
+    b.close()
+
+
+def test_graph_replay_equals_single_steps():
+    c = cases.small_dam_break(64, 48)
+    kw = dict(free_surface=True, precision=32, tau=c.tau, fy=c.fy)
+    a = E.Solver(c.flags, **kw)
+    b = E.Solver(c.flags, **kw)
+    a.step(71)
+    for _ in range(71):
+        b.step(1)
+    for fid in (E.FIELD_F, E.FIELD_FLAGS, E.FIELD_MASS, E.FIELD_PHI):
+        assert exact_equal(a.read(fid), b.read(fid))
+    assert a.launches > 0 and b.launches > 0
+    a.close()
+    b.close()
+
+
+def test_reset_restarts_from_the_initial_state():
+    c = cases.small_dam_break(64, 48)
+    a = E.Solver(c.flags, free_surface=True, tau=c.tau, fy=c.fy)
+    f0 = a.f.copy()
+    a.step(20)
+    a.reset(c.flags)
+    assert a.t == 0 and exact_equal(a.f, f0)
+    a.close()
+
+
+def test_plain_channel_10000_steps_fp64_matches_oracle(channel):
+    """The 256x64 culvert channel for its full 10,000 steps: the FP64 engine
+    equals the FP64 oracle bit for bit, flags are unchanged, and the FP32
+    engine stays within 1e-5 (relative L2) of the FP64 velocity."""
+    s, o = make_pair(channel.flags, O.F64, bb=O.BB_IMPLICIT, tau=channel.tau, fx=channel.fx)
+    s.step(10_000)
+    o.step(10_000)
+    assert_same_state(s, o, O.F64, False, "t=10000")
+    s32 = E.Solver(channel.flags, precision=32, tau=channel.tau, fx=channel.fx, bounce_back=E.BB_IMPLICIT)
+    s32.step(10_000)
+    fluid = np.tile(channel.flags.ravel() == cases.FLUID, 2)
+    u64 = o.u[fluid]
+    u32 = s32.u.astype(np.float64)[fluid]
+    assert np.linalg.norm(u32 - u64) / np.linalg.norm(u64) < 1e-5
+    assert exact_equal(s32.flags, channel.flags.ravel())
+    s.close()
+    s32.close()
+
+
+def test_dam_break_2048x512_conserves_mass_20000_steps():
+    """The free-surface dam break at full size and length: FP32 populations,
+    FP64 mass, half-way walls, conservative mode; total mass conserved to 1e-6."""
+    c = cases.dam_break(1)
+    s = E.Solver(c.flags, free_surface=True, precision=32, mass_precision=64, tau=c.tau, fy=c.fy)
+    m0 = s.total_mass()
+    s.step(20_000)
+    m1 = s.total_mass()
+    assert abs(m1 - m0) / m0 < 1e-6, (m0, m1)
+    assert s.check_finite()
+    fl = s.flags
+    assert set(np.unique(fl)).issubset({cases.FLUID, cases.GAS, cases.INTERFACE, cases.WALL})
+    cnt = s.cell_counts()
+    assert cnt["fluid"] > 0 and cnt["interface"] > 0
+    s.close()
+
+
+def test_dam_break_8192x2048_conserves_mass():
+    """Precision-sweep size (8192x2048): mass conservation and flag sanity in
+    FP32 and FP16S storage over 300 steps."""
+    c = cases.dam_break(4)
+    for prec in (32, 16):
+        s = E.Solver(c.flags, free_surface=True, precision=prec, mass_precision=64, tau=c.tau, fy=c.fy)
+        m0 = s.total_mass()
+        s.step(300)
+        assert abs(s.total_mass() - m0) / m0 < 1e-6
+        assert s.check_finite()
+        s.close()
