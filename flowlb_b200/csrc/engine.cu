@@ -18,6 +18,7 @@
 
 #include "../../include/flowlb.h"
 #include "kernels.cuh"
+#include "sc_vec.cuh"
 
 using namespace flb;
 
@@ -44,9 +45,13 @@ struct flb_engine {
   bool own_stream = false;
   size_t s_size = 4, c_size = 4, m_size = 8;
   bool fs = false, hw = false, has_io = false;
+  bool use_vec = false;  // vectorised stream-collide
   uint64_t t = 0;
   uint64_t launches = 0;
   int cur = 0;  // index of the current flag buffer (free surface)
+  // the other flag buffer holds the previous step's post-stream-collide flags
+  // and the mass fields follow from full steps (enables write skipping)
+  bool trust = false;
   KParams kp{};
   // device buffers
   void* d_f = nullptr;
@@ -109,7 +114,28 @@ dim3 lin_grid(uint64_t n) { return dim3((unsigned)((n + kBlock - 1) / kBlock)); 
 // ---- per-variant launchers ------------------------------------------------
 template <class S, class C, class M>
 struct Ops {
+  template <bool FS, bool HW, bool WM>
+  static void sc_vec(flb_engine* h, uint32_t odd) {
+    constexpr int V = Lanes<S>::V;
+    const uint32_t per_row = h->nx / V;
+    const uint32_t block = per_row >= (uint32_t)kVecBlock ? (uint32_t)kVecBlock : ((per_row + 31u) / 32u) * 32u;
+    const dim3 g((per_row + block - 1) / block, h->ny);
+    k_sc_vec<S, C, M, FS, HW, WM><<<g, block, 0, h->stream>>>(h->kp, odd);
+  }
   static void sc(flb_engine* h, uint32_t odd, bool wm) {
+    if (h->use_vec) {
+      if (h->fs) {
+        if (h->hw) sc_vec<true, true, true>(h, odd);
+        else sc_vec<true, false, true>(h, odd);
+      } else if (wm) {
+        if (h->hw) sc_vec<false, true, true>(h, odd);
+        else sc_vec<false, false, true>(h, odd);
+      } else {
+        if (h->hw) sc_vec<false, true, false>(h, odd);
+        else sc_vec<false, false, false>(h, odd);
+      }
+      return;
+    }
     const dim3 g = row_grid(h->nx, h->ny);
     if (h->fs) {
       if (h->hw) k_stream_collide<S, C, M, true, true, true><<<g, kBlock, 0, h->stream>>>(h->kp, odd);
@@ -197,6 +223,7 @@ uint64_t issue_step(flb_engine* h, uint64_t t, bool write_macro) {
     cudaMemcpyAsync(h->d_u_snap, h->d_u, 2ull * h->N * h->c_size, cudaMemcpyDeviceToDevice, h->stream);
   }
   if (h->fs) {
+    h->kp.trust_prev = h->trust ? 1 : 0;
     dispatch(h, [&](auto ops) {
       ops.fs1(h, odd);
       ops.sc(h, odd, true);
@@ -204,6 +231,7 @@ uint64_t issue_step(flb_engine* h, uint64_t t, bool write_macro) {
     });
     k = 3;
     h->cur ^= 1;
+    h->trust = true;
     refresh_params(h);
   } else {
     dispatch(h, [&](auto ops) { ops.sc(h, odd, write_macro || h->has_io); });
@@ -271,6 +299,9 @@ flb_status validate(const flb_case_desc* d, std::string& msg) {
     return msg = "bounce_back must be IMPLICIT or HALFWAY", FLB_ERR_INVALID_ARGUMENT;
   if (d->fs_mode != FLB_FS_REFERENCE && d->fs_mode != FLB_FS_CONSERVATIVE)
     return msg = "fs_mode must be REFERENCE or CONSERVATIVE", FLB_ERR_INVALID_ARGUMENT;
+  if (d->kernel_variant < 0 || d->kernel_variant > 2) return msg = "kernel_variant must be 0, 1 or 2", FLB_ERR_INVALID_ARGUMENT;
+  if (d->kernel_variant == 2 && d->nx % (d->precision == 64 ? 2u : 4u) != 0)
+    return msg = "the vector stream-collide needs nx divisible by its vector width", FLB_ERR_UNSUPPORTED;
   if (d->precision == 16) {
     const float s = d->f16_scale == 0.0f ? 4096.0f : d->f16_scale;
     int e = 0;
@@ -312,6 +343,7 @@ flb_status initialise(flb_engine* h) {
   h->launches++;
   if (h->fs) FLB_CUDA(h, cudaMemcpyAsync(h->d_flags[1], h->d_flags[0], h->N, cudaMemcpyDeviceToDevice, h->stream));
   if (h->d_recon_mask) FLB_CUDA(h, cudaMemsetAsync(h->d_recon_mask, 0, h->N, h->stream));
+  h->trust = true;  // flags[1] = flags[0] and the initial fields satisfy the skip invariants
   FLB_CUDA(h, cudaGetLastError());
   return FLB_OK;
 }
@@ -372,6 +404,10 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
   } else {
     h->variant = V_F32;
     h->s_size = 4; h->c_size = 4; h->m_size = 8;
+  }
+  {
+    const uint32_t V = desc->precision == 64 ? 2u : 4u;
+    h->use_vec = desc->kernel_variant == 2 || (desc->kernel_variant == 0 && desc->nx % V == 0);
   }
   s = check_io(h, desc->flags);
   if (s != FLB_OK) {
@@ -484,7 +520,12 @@ FLB_API flb_status flb_step(flb_handle h, uint64_t n) {
     // graphs cover pairs of steps from an even t; the last step of the call
     // runs on its own so that it writes density and velocity
     const uint64_t big = 2ull * kGraphPairs;
-    if ((h->t & 1u) == 0 && remaining > big) {
+    if (h->fs && !h->trust) {
+      // first step after the state was written from outside: no write skipping
+      h->launches += issue_step(h, h->t, remaining == 1);
+      h->t += 1;
+      remaining -= 1;
+    } else if ((h->t & 1u) == 0 && remaining > big) {
       s = capture(h, h->g_big, kGraphPairs);
       if (s != FLB_OK) break;
       cudaError_t e = cudaGraphLaunch(h->g_big.exec, h->stream);
@@ -628,6 +669,7 @@ FLB_API flb_status flb_write_field(flb_handle h, int field, const void* src, int
   } else {
     FLB_CUDA(h, cudaMemcpyAsync(dst, src, bytes, kind, h->stream));
   }
+  h->trust = false;
   FLB_CUDA(h, cudaStreamSynchronize(h->stream));
   return FLB_OK;
 }
@@ -691,6 +733,8 @@ FLB_API flb_status flb_run_pass(flb_handle h, int pass) {
     FLB_CUDA(h, cudaMemcpyAsync(h->d_u_snap, h->d_u, 2ull * h->N * h->c_size, cudaMemcpyDeviceToDevice, h->stream));
   }
   const bool recon = h->fs && h->d_recon_mask;
+  h->trust = false;
+  h->kp.trust_prev = 0;
   // alone, stream-collide sees no parked populations, and FS_1 writes its
   // rebuilt populations into the population array like the reference kernel
   if (pass == 0 && recon) FLB_CUDA(h, cudaMemsetAsync(h->d_recon_mask, 0, h->N, h->stream));
@@ -725,6 +769,7 @@ FLB_API flb_status flb_profile_steps(flb_handle h, uint64_t n, double pass_ms[3]
     }
     cudaEventRecord(ev[0], h->stream);
     if (h->fs) {
+      h->kp.trust_prev = h->trust ? 1 : 0;
       dispatch(h, [&](auto ops) { ops.fs1(h, odd); });
       cudaEventRecord(ev[1], h->stream);
       dispatch(h, [&](auto ops) { ops.sc(h, odd, true); });
@@ -733,6 +778,7 @@ FLB_API flb_status flb_profile_steps(flb_handle h, uint64_t n, double pass_ms[3]
       cudaEventRecord(ev[3], h->stream);
       h->launches += 3;
       h->cur ^= 1;
+      h->trust = true;
     } else {
       cudaEventRecord(ev[1], h->stream);
       dispatch(h, [&](auto ops) { ops.sc(h, odd, k + 1 == n || h->has_io); });
@@ -859,6 +905,7 @@ FLB_API flb_status flb_load_checkpoint(flb_handle h, const char* path) {
   std::fclose(fp);
   h->t = hd.t;
   h->cur = cur;
+  h->trust = false;
   refresh_params(h);
   return FLB_OK;
 }

@@ -42,6 +42,9 @@ struct KParams {
   float f16_scale, f16_inv;
   double inlet_ux, inlet_uy;
   int use_force, subgrid, collision, fs_cons, count_pre;
+  // 1 when flags_out holds the previous step's post-stream-collide flags and
+  // the mass fields come from the previous full step (see k_fs234)
+  int trust_prev;
 };
 
 // ---- population access helpers -------------------------------------------
@@ -60,7 +63,9 @@ __device__ __forceinline__ void load_incoming(const S* F, uint32_t idx, const ui
   }
 }
 
-// storef plus the half-way redirect toward wall neighbours.
+// storef plus the half-way redirect: a population aimed at a wall neighbour is
+// also written where this cell loads the opposite direction at t+1 (its
+// regular slot belongs to the wall cell and is never read).
 template <class S, class C, bool HW>
 __device__ __forceinline__ void store_post(S* F, uint32_t idx, const uint32_t* nb, uint32_t N, uint32_t odd,
                                            uint32_t nbm, float scale, const C* f) {
@@ -68,10 +73,10 @@ __device__ __forceinline__ void store_post(S* F, uint32_t idx, const uint32_t* n
 #pragma unroll
   for (int i = 1; i < 9; i += 2) {
     const uint32_t a = odd ? i : i + 1, b = odd ? i + 1 : i;
+    Codec<S, C>::st(F, nb[i] + N * b, i, f[i], scale);
     if (HW && ((nbm >> (i - 1)) & 1u)) Codec<S, C>::st(F, nb[i] + N * a, i, f[i], scale);
-    else Codec<S, C>::st(F, nb[i] + N * b, i, f[i], scale);
+    Codec<S, C>::st(F, idx + N * a, i + 1, f[i + 1], scale);
     if (HW && ((nbm >> i) & 1u)) Codec<S, C>::st(F, idx + N * b, i + 1, f[i + 1], scale);
-    else Codec<S, C>::st(F, idx + N * a, i + 1, f[i + 1], scale);
   }
 }
 
@@ -561,7 +566,19 @@ __global__ void __launch_bounds__(kTX* kTY) k_fs234(const __grid_constant__ KPar
   const uint32_t N = p.N, idx = (uint32_t)gx + (uint32_t)gy * (uint32_t)nx;
   const uint8_t f1 = s1[ly][lx];
   const uint8_t f3 = s2[ly][lx];
-  p.flags_out[idx] = s3[ly][lx];
+  const uint8_t fin = s3[ly][lx];
+  // Write skipping.  flags_out still holds this cell's flag after the previous
+  // step's stream-collide ("old").  When the buffers come from consecutive
+  // full steps (trust_prev), a value already in memory is not rewritten:
+  //  * the flag, when old equals the new flag;
+  //  * all mass fields of a cell that was gas in the previous step and stays
+  //    gas: that step (or the initial state) left m = excess = phi = +0, and
+  //    FS_1 does not touch gas cells, so FS_4 would write the same zeros;
+  //  * the fill level of a cell that was fluid after the previous step and
+  //    stays fluid: it is already 1.
+  const bool trust = p.trust_prev != 0;
+  const uint8_t old = p.flags_out[idx];
+  if (!trust || old != fin) p.flags_out[idx] = fin;
   const C* R = static_cast<const C*>(p.rho);
   const C* U = static_cast<const C*>(p.u);
   uint32_t nb[9];
@@ -593,6 +610,9 @@ __global__ void __launch_bounds__(kTX* kTY) k_fs234(const __grid_constant__ KPar
   }
   // FS_4 fields
   if (f3 & (kWall | kMovingWall | kInlet)) return;
+  const uint8_t sw4 = f3 & (kFGI | kGasInterface);
+  if (trust && sw4 == kGas && (old & (kFGI | kGasInterface)) == kGas) return;
+  const bool keep_phi = trust && sw4 == kFluid && (s0[ly][lx] & (kFGI | kGasInterface)) == kFluid;
   M* Ms = static_cast<M*>(p.mass);
   const C rho = R[idx];
   M m = Ms[idx];
@@ -646,7 +666,7 @@ __global__ void __launch_bounds__(kTX* kTY) k_fs234(const __grid_constant__ KPar
   ex = cont > 0 ? ex / (float)cont : 0.0f;
   Ms[idx] = m;
   static_cast<M*>(p.excess)[idx] = ex;
-  static_cast<M*>(p.phi)[idx] = ph;
+  if (!keep_phi) static_cast<M*>(p.phi)[idx] = ph;
 }
 
 // ---- reductions and codecs --------------------------------------------------

@@ -39,6 +39,7 @@ class CaseDesc(C.Structure):
         ("subgrid", C.c_int32), ("use_volumetric_force", C.c_int32), ("tau", C.c_float), ("fx", C.c_float),
         ("fy", C.c_float), ("bounce_back", C.c_int32), ("fs_mode", C.c_int32), ("f16_scale", C.c_float),
         ("device", C.c_int32), ("stream", C.c_void_p), ("inlet_ux", C.c_double), ("inlet_uy", C.c_double),
+        ("kernel_variant", C.c_int32),
     ]
 
 
@@ -114,7 +115,8 @@ class Solver:
                  mass_precision: int = 64, tau: float = 0.6, fx: float = 0.0, fy: float = 0.0,
                  use_force: bool = True, collision: int = 0, subgrid: bool = False,
                  bounce_back: int = BB_HALFWAY, fs_mode: int = FS_CONSERVATIVE, inlet_ux: float = 0.0,
-                 inlet_uy: float = 0.0, f16_scale: float = 0.0, device: int = -1, stream: int | None = None):
+                 inlet_uy: float = 0.0, f16_scale: float = 0.0, device: int = -1, stream: int | None = None,
+                 kernel_variant: int = 0):
         L = load_library()
         g = np.ascontiguousarray(flags, dtype=np.uint8)
         if g.ndim != 2:
@@ -131,6 +133,7 @@ class Solver:
         d.inlet_ux, d.inlet_uy = inlet_ux, inlet_uy
         d.bounce_back, d.fs_mode, d.f16_scale, d.device = int(bounce_back), int(fs_mode), f16_scale, int(device)
         d.stream = stream or None
+        d.kernel_variant = int(kernel_variant)
         self._desc = d
         self.free_surface = bool(free_surface)
         self.precision = precision

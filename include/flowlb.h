@@ -102,6 +102,8 @@ typedef struct flb_case_desc {
   int32_t device;             /* CUDA device ordinal; -1 = current */
   void* stream;               /* cudaStream_t to issue on; NULL = a stream owned by the handle */
   double inlet_ux, inlet_uy;  /* lattice velocity of INLET cells (double, as the reference's LBVelocity) */
+  int32_t kernel_variant;     /* stream-collide data path: 0 auto, 1 one cell per thread, 2 vector
+                                 (V cells per thread; needs nx % V == 0, V = 4 for FP32/FP16S, 2 for FP64) */
 } flb_case_desc;
 
 typedef struct flb_engine* flb_handle;

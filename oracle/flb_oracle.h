@@ -65,6 +65,7 @@ typedef struct {
   int32_t subgrid;       /* Smagorinsky on/off */
   int32_t use_force;     /* Guo forcing on/off */
   int32_t fs_count_pre;  /* oracle-only: FS_4 counts IG neighbours as unconverted */
+  int32_t fs1_post;      /* oracle-only: FS_1 outgoing reads see neighbours' rebuilt populations */
   float tau;             /* relaxation time */
   float fx, fy;          /* body force, lattice units */
   float f16_scale;       /* power-of-two scale S of the F16S storage */

@@ -32,7 +32,8 @@ class OrcParams(C.Structure):
     _fields_ = [
         ("nx", C.c_int32), ("ny", C.c_int32), ("variant", C.c_int32), ("free_surface", C.c_int32),
         ("bb", C.c_int32), ("fs_mode", C.c_int32), ("collision", C.c_int32), ("subgrid", C.c_int32),
-        ("use_force", C.c_int32), ("fs_count_pre", C.c_int32), ("tau", C.c_float), ("fx", C.c_float),
+        ("use_force", C.c_int32), ("fs_count_pre", C.c_int32), ("fs1_post", C.c_int32), ("tau", C.c_float),
+        ("fx", C.c_float),
         ("fy", C.c_float), ("f16_scale", C.c_float), ("threads", C.c_int32), ("inlet_ux", C.c_double),
         ("inlet_uy", C.c_double),
     ]
@@ -87,6 +88,7 @@ class OracleConfig:
     subgrid: bool = False
     use_force: bool = True
     fs_count_pre: bool = False
+    fs1_post: bool = False
     tau: float = 0.6
     fx: float = 0.0
     fy: float = 0.0
@@ -106,7 +108,8 @@ class Oracle:
         self.N = self.nx * self.ny
         self.cfg = cfg
         p = OrcParams(self.nx, self.ny, cfg.variant, int(cfg.free_surface), cfg.bb, cfg.fs_mode, cfg.collision,
-                      int(cfg.subgrid), int(cfg.use_force), int(cfg.fs_count_pre), cfg.tau, cfg.fx, cfg.fy,
+                      int(cfg.subgrid), int(cfg.use_force), int(cfg.fs_count_pre), int(cfg.fs1_post), cfg.tau,
+                      cfg.fx, cfg.fy,
                       cfg.f16_scale, cfg.threads, cfg.inlet_ux, cfg.inlet_uy)
         self._h = lib().orc_create(C.byref(p), g.ctypes.data)
         if not self._h:

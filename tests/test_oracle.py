@@ -80,6 +80,38 @@ def test_oracle_steps_match_reference_cuda_fixture(path):
             assert exact_equal(getattr(o, k), g[k]), k
 
 
+def _kernel_fixtures():
+    return sorted(glob.glob(os.path.join(GOLDEN, "kernels_*.npz")))
+
+
+@pytest.mark.parametrize("path", _kernel_fixtures(), ids=lambda p: os.path.basename(p))
+def test_oracle_kernels_match_reference_cuda_fixture(path):
+    """Along the oracle's dam-break trajectory, each of FlowLB's five CUDA
+    kernels (recorded on a B200 by make_golden.py --cuda) and the oracle's
+    kernel give the same fields; for the two kernels that race in the
+    reference, each cell must match one of the two interleavings."""
+    from refcheck import check_kernel, snapshot
+    g = dict(np.load(path))
+    prec = 32 if "_p32" in path else 64
+    geo = g["geometry"]
+    cfg = O.OracleConfig(variant=VARIANT_OF_PREC[prec], free_surface=True, tau=float(g["tau"]),
+                         fx=float(g["fx"]), fy=float(g["fy"]))
+    o = O.Oracle(geo, cfg)
+    names = {O.K_FS1: "fs1", O.K_STREAM_COLLIDE: "sc", O.K_FS2: "fs2", O.K_FS3: "fs3", O.K_FS4: "fs4"}
+    samples = set(int(s) for s in g["sample_steps"])
+    checked = 0
+    for step in range(max(samples) + 1):
+        for kid in (O.K_FS1, O.K_STREAM_COLLIDE, O.K_FS2, O.K_FS3, O.K_FS4):
+            if step in samples:
+                prefix = f"s{step}_{names[kid]}_"
+                ref = {k[len(prefix):]: v for k, v in g.items() if k.startswith(prefix)}
+                check_kernel(geo, cfg, snapshot(o), o.t, kid, ref, f"step {step} {names[kid]}")
+                checked += 1
+            o.kernel(kid)
+        o.t = o.t + 1
+    assert checked == 5 * len(samples)
+
+
 def test_oracle_poiseuille_halfway_known_answer():
     """Body-force channel with half-way walls converges to the analytic
     parabola u(y) = F/(2 nu) (y - 1/2)(H + 1/2 - y), walls half a cell outside
