@@ -247,15 +247,19 @@ typedef struct {
   void (*init)(orc_state*);
   void (*read_f64)(const orc_state*, double*);
   double (*total_mass)(const orc_state*);
+  int (*fs1_options)(orc_state*, size_t, double*, double*, uint8_t*);
+  int (*fs4_options)(const orc_state*, size_t, double*);
 } orc_vtable;
 
 static const orc_vtable ORC_VT[4] = {
-    {stream_collide_f64, fs1_f64, fs3_fields_f64, fs4_fields_f64, init_f64, read_f64_f64, total_mass_f64},
-    {stream_collide_f32, fs1_f32, fs3_fields_f32, fs4_fields_f32, init_f32, read_f64_f32, total_mass_f32},
+    {stream_collide_f64, fs1_f64, fs3_fields_f64, fs4_fields_f64, init_f64, read_f64_f64, total_mass_f64,
+     fs1_options_f64, fs4_options_f64},
+    {stream_collide_f32, fs1_f32, fs3_fields_f32, fs4_fields_f32, init_f32, read_f64_f32, total_mass_f32,
+     fs1_options_f32, fs4_options_f32},
     {stream_collide_f16s, fs1_f16s, fs3_fields_f16s, fs4_fields_f16s, init_f16s, read_f64_f16s,
-     total_mass_f16s},
+     total_mass_f16s, fs1_options_f16s, fs4_options_f16s},
     {stream_collide_f32m32, fs1_f32m32, fs3_fields_f32m32, fs4_fields_f32m32, init_f32m32, read_f64_f32m32,
-     total_mass_f32m32},
+     total_mass_f32m32, fs1_options_f32m32, fs4_options_f32m32},
 };
 
 static void orc_free(orc_state* s) {
@@ -421,6 +425,16 @@ void* orc_field(orc_state* s, int field, size_t* elem_size) {
 
 void orc_read_f64(const orc_state* s, double* out) {
   if (s && out) ORC_VT[s->p.variant].read_f64(s, out);
+}
+
+int orc_fs1_options(orc_state* s, size_t idx, double* masses, double* recs, uint8_t* masks) {
+  if (!s || !s->p.free_surface || idx >= s->N) return -1;
+  return ORC_VT[s->p.variant].fs1_options(s, idx, masses, recs, masks);
+}
+
+int orc_fs4_options(const orc_state* s, size_t idx, double* out3) {
+  if (!s || !s->p.free_surface || idx >= s->N) return -1;
+  return ORC_VT[s->p.variant].fs4_options(s, idx, out3);
 }
 
 double orc_total_mass(const orc_state* s) { return s ? ORC_VT[s->p.variant].total_mass(s) : 0.0; }

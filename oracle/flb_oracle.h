@@ -106,6 +106,13 @@ void orc_read_f64(const orc_state* s, double* out);
  * the next step loads into non-solid cells. */
 double orc_total_mass(const orc_state* s);
 
+/* Race enumeration (test support), see flb_oracle_body.inc.  fs1: up to 256
+ * options of (mass, 8 rebuilt populations, rebuilt mask) for cell idx, state
+ * before FS_1.  fs4: up to 9 options of (mass, excess, fill level), state
+ * after FS_3.  Return the number of options (0: the kernel skips the cell). */
+int orc_fs1_options(orc_state* s, size_t idx, double* masses, double* recs, uint8_t* masks);
+int orc_fs4_options(const orc_state* s, size_t idx, double* out3);
+
 #ifdef __cplusplus
 }
 #endif

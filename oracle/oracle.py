@@ -64,6 +64,10 @@ def lib() -> C.CDLL:
         L.orc_read_f64.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_total_mass.restype = C.c_double
         L.orc_total_mass.argtypes = [C.c_void_p]
+        L.orc_fs1_options.restype = C.c_int
+        L.orc_fs1_options.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p]
+        L.orc_fs4_options.restype = C.c_int
+        L.orc_fs4_options.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p]
         _lib = L
     return _lib
 
@@ -162,6 +166,22 @@ class Oracle:
 
     def total_mass(self) -> float:
         return float(lib().orc_total_mass(self._h))
+
+    def fs1_options(self, idx: int):
+        """Every result the reference FS_1 kernel can give for cell idx (state
+        before FS_1): list of (mass, rebuilt[8], mask)."""
+        m = np.zeros(256)
+        r = np.zeros(256 * 8)
+        k = np.zeros(256, np.uint8)
+        n = lib().orc_fs1_options(self._h, int(idx), m.ctypes.data, r.ctypes.data, k.ctypes.data)
+        return [(m[c], r[8 * c:8 * c + 8], int(k[c])) for c in range(max(n, 0))]
+
+    def fs4_options(self, idx: int):
+        """Every (mass, excess, fill level) the reference FS_4 kernel can give
+        for cell idx (state after FS_3)."""
+        out = np.zeros(27)
+        n = lib().orc_fs4_options(self._h, int(idx), out.ctypes.data)
+        return [tuple(out[3 * c:3 * c + 3]) for c in range(max(n, 0))]
 
 
 # ---- the reference's own code ---------------------------------------------
