@@ -1,0 +1,116 @@
+// common.cuh -- kernel parameters and population access shared by all passes.
+//
+// Layout in HBM (structure of arrays, the reference layout, one population
+// buffer):
+//   f      9N  S   slot s of cell c at f[c + s*N] (slot[s] below points at
+//                  f + s*N); updated in place by the esoteric-pull pattern:
+//                  a cell loads and stores the same 9 addresses, so no second
+//                  buffer is needed
+//   rho     N  C   density of the incoming populations of the last step
+//   u      2N  C   force-shifted velocity, u_x then u_y
+//   flags  2xN u8  cell types; two buffers, the flag-stencil pass reads one
+//                  and writes the other
+//   nbmask  N  u8  bit k-1 set when neighbour k is a wall (half-way walls)
+//   mass, excess, phi  N  M   free-surface cell mass, excess share, fill level
+//   recon  8N  C   populations rebuilt by FS_1 toward gas (reference mode only)
+// S/C/M: storage / arithmetic / mass types.
+#pragma once
+
+#include <cstdint>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "lattice.cuh"
+
+namespace flb {
+
+constexpr int kBlock = 256;
+
+struct KParams {
+  uint32_t nx, ny, N;
+  void* f;
+  void* slot[9];  // f + s*N, typed by the kernel
+  void* rho;
+  void* u;
+  uint8_t* flags;      // current flags
+  uint8_t* flags_out;  // flag-stencil pass output
+  const uint8_t* nbmask;
+  void* mass;
+  void* excess;
+  void* phi;
+  void* recon;
+  uint8_t* recon_mask;
+  const void* rho_snap;
+  const void* u_snap;
+  float inv_tau, fx, fy;
+  float f16_scale, f16_inv;
+  double inlet_ux, inlet_uy;
+  int use_force, subgrid, collision, fs_cons;
+  // 1 when flags_out holds the previous step's post-stream-collide flags and
+  // the mass fields come from the previous full step (see k_fs234)
+  int trust_prev;
+  float u_max;  // velocity limiter, 0 = off
+};
+
+template <class S>
+__device__ __forceinline__ S* slotp(const KParams& p, int s) {
+  return static_cast<S*>(p.slot[s]);
+}
+
+// Slot holding incoming population i of a cell (i odd: own cell, slot a;
+// i+1: neighbour i's cell, slot b), cellCalculations.cuh:185-196.
+template <bool ODD>
+__device__ __forceinline__ constexpr int slot_a(int i) { return ODD ? i : i + 1; }
+template <bool ODD>
+__device__ __forceinline__ constexpr int slot_b(int i) { return ODD ? i + 1 : i; }
+
+// loadf plus the half-way wall: a population that would arrive from a wall
+// neighbour is read from where this cell stored the opposite population last
+// step, i.e. it comes back reflected after one step.  nbm bit k-1 = neighbour
+// k is a wall.
+template <class S, class C, bool HW, bool ODD>
+__device__ __forceinline__ void load_in(const KParams& p, uint32_t idx, const uint32_t* nb, uint32_t nbm, C* f) {
+  const float inv = p.f16_inv;
+  f[0] = Codec<S, C>::ld(slotp<S>(p, 0), idx, 0, inv);
+#pragma unroll
+  for (int i = 1; i < 9; i += 2) {
+    const int a = slot_a<ODD>(i), b = slot_b<ODD>(i);
+    if (HW && ((nbm >> i) & 1u)) f[i] = Codec<S, C>::ld(slotp<S>(p, b), idx, i, inv);
+    else f[i] = Codec<S, C>::ld(slotp<S>(p, a), idx, i, inv);
+    if (HW && ((nbm >> (i - 1)) & 1u)) f[i + 1] = Codec<S, C>::ld(slotp<S>(p, a), nb[i], i + 1, inv);
+    else f[i + 1] = Codec<S, C>::ld(slotp<S>(p, b), nb[i], i + 1, inv);
+  }
+}
+
+// loadOutgoingf, cellCalculations.cuh:207-217.
+template <class S, class C, bool ODD>
+__device__ __forceinline__ void load_out(const KParams& p, uint32_t idx, const uint32_t* nb, C* out) {
+  const float inv = p.f16_inv;
+#pragma unroll
+  for (int i = 1; i < 9; i += 2) {
+    out[i] = Codec<S, C>::ld(slotp<S>(p, slot_a<ODD>(i)), nb[i], i, inv);
+    out[i + 1] = Codec<S, C>::ld(slotp<S>(p, slot_b<ODD>(i)), idx, i + 1, inv);
+  }
+}
+
+// storef, cellCalculations.cuh:228-238.
+template <class S, class C, bool ODD>
+__device__ __forceinline__ void store_post(const KParams& p, uint32_t idx, const uint32_t* nb, const C* f) {
+  const float sc = p.f16_scale;
+  Codec<S, C>::st(slotp<S>(p, 0), idx, 0, f[0], sc);
+#pragma unroll
+  for (int i = 1; i < 9; i += 2) {
+    Codec<S, C>::st(slotp<S>(p, slot_b<ODD>(i)), nb[i], i, f[i], sc);
+    Codec<S, C>::st(slotp<S>(p, slot_a<ODD>(i)), idx, i + 1, f[i + 1], sc);
+  }
+}
+
+// Runtime-parity wrappers for passes that are not on the step's hot path.
+template <class S, class C, bool HW>
+__device__ __forceinline__ void load_in_rt(const KParams& p, uint32_t odd, uint32_t idx, const uint32_t* nb,
+                                           uint32_t nbm, C* f) {
+  if (odd) load_in<S, C, HW, true>(p, idx, nb, nbm, f);
+  else load_in<S, C, HW, false>(p, idx, nb, nbm, f);
+}
+
+}  // namespace flb

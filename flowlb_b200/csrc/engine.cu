@@ -17,8 +17,7 @@
 #include <vector>
 
 #include "../../include/flowlb.h"
-#include "kernels.cuh"
-#include "sc_vec.cuh"
+#include "launch.h"
 
 using namespace flb;
 
@@ -108,79 +107,25 @@ struct DeviceGuard {
   }
 };
 
-dim3 row_grid(uint32_t nx, uint32_t ny) { return dim3((nx + kBlock - 1) / kBlock, ny); }
-dim3 lin_grid(uint64_t n) { return dim3((unsigned)((n + kBlock - 1) / kBlock)); }
 
 // ---- per-variant launchers ------------------------------------------------
 template <class S, class C, class M>
 struct Ops {
-  template <bool FS, bool HW, bool WM>
-  static void sc_vec(flb_engine* h, uint32_t odd) {
-    constexpr int V = Lanes<S>::V;
-    const uint32_t per_row = h->nx / V;
-    const uint32_t block = per_row >= (uint32_t)kVecBlock ? (uint32_t)kVecBlock : ((per_row + 31u) / 32u) * 32u;
-    const dim3 g((per_row + block - 1) / block, h->ny);
-    k_sc_vec<S, C, M, FS, HW, WM><<<g, block, 0, h->stream>>>(h->kp, odd);
-  }
   static void sc(flb_engine* h, uint32_t odd, bool wm) {
-    if (h->use_vec) {
-      if (h->fs) {
-        if (h->hw) sc_vec<true, true, true>(h, odd);
-        else sc_vec<true, false, true>(h, odd);
-      } else if (wm) {
-        if (h->hw) sc_vec<false, true, true>(h, odd);
-        else sc_vec<false, false, true>(h, odd);
-      } else {
-        if (h->hw) sc_vec<false, true, false>(h, odd);
-        else sc_vec<false, false, false>(h, odd);
-      }
-      return;
-    }
-    const dim3 g = row_grid(h->nx, h->ny);
-    if (h->fs) {
-      if (h->hw) k_stream_collide<S, C, M, true, true, true><<<g, kBlock, 0, h->stream>>>(h->kp, odd);
-      else k_stream_collide<S, C, M, true, false, true><<<g, kBlock, 0, h->stream>>>(h->kp, odd);
-    } else if (wm) {
-      if (h->hw) k_stream_collide<S, C, M, false, true, true><<<g, kBlock, 0, h->stream>>>(h->kp, odd);
-      else k_stream_collide<S, C, M, false, false, true><<<g, kBlock, 0, h->stream>>>(h->kp, odd);
-    } else {
-      if (h->hw) k_stream_collide<S, C, M, false, true, false><<<g, kBlock, 0, h->stream>>>(h->kp, odd);
-      else k_stream_collide<S, C, M, false, false, false><<<g, kBlock, 0, h->stream>>>(h->kp, odd);
-    }
+    launch_sc<S, C, M>(h->kp, h->stream, odd, h->fs, h->hw, wm, h->use_vec);
   }
-  static void fs1(flb_engine* h, uint32_t odd) {
-    const dim3 g = row_grid(h->nx, h->ny);
-    if (h->hw) k_fs1<S, C, M, true><<<g, kBlock, 0, h->stream>>>(h->kp, odd);
-    else k_fs1<S, C, M, false><<<g, kBlock, 0, h->stream>>>(h->kp, odd);
-  }
-  static void fs234(flb_engine* h, uint32_t odd) {
-    const dim3 g((h->nx + kTX - 1) / kTX, (h->ny + kTY - 1) / kTY);
-    const dim3 b(kTX, kTY);
-    if (h->hw) k_fs234<S, C, M, true><<<g, b, 0, h->stream>>>(h->kp, odd);
-    else k_fs234<S, C, M, false><<<g, b, 0, h->stream>>>(h->kp, odd);
-  }
-  static void apply_recon(flb_engine* h, uint32_t odd) {
-    k_apply_recon<S, C><<<row_grid(h->nx, h->ny), kBlock, 0, h->stream>>>(h->kp, odd);
-  }
-  static void init_ddf(flb_engine* h) {
-    if (h->hw) k_init_ddf<S, C, true><<<row_grid(h->nx, h->ny), kBlock, 0, h->stream>>>(h->kp, h->d_geo);
-    else k_init_ddf<S, C, false><<<row_grid(h->nx, h->ny), kBlock, 0, h->stream>>>(h->kp, h->d_geo);
-  }
+  static void fs1(flb_engine* h, uint32_t odd) { launch_fs1<S, C, M>(h->kp, h->stream, odd, h->hw); }
+  static void fs234(flb_engine* h, uint32_t odd) { launch_fs234<S, C, M>(h->kp, h->stream, odd); }
+  static void apply_recon(flb_engine* h, uint32_t odd) { launch_apply_recon<S, C, M>(h->kp, h->stream, odd); }
+  static void init_ddf(flb_engine* h) { launch_init_ddf<S, C, M>(h->kp, h->stream, h->d_geo, h->hw); }
   static void mass_partial(flb_engine* h, uint32_t odd) {
-    k_mass_partial<S, C, M><<<lin_grid(h->N), kBlock, 0, h->stream>>>(h->kp, odd, h->fs ? 1 : 0, h->d_partial);
+    launch_mass_partial<S, C, M>(h->kp, h->stream, odd, h->fs ? 1 : 0, h->hw, h->d_partial);
   }
   static void census(flb_engine* h, uint32_t odd) {
-    k_census<S, C><<<lin_grid(h->N), kBlock, 0, h->stream>>>(h->kp, odd, h->d_counts);
+    launch_census<S, C, M>(h->kp, h->stream, odd, h->hw, h->d_counts);
   }
-  static void decode(flb_engine* h, void* out) {
-    k_decode<S, C><<<lin_grid(9ull * h->N), kBlock, 0, h->stream>>>(static_cast<const S*>(h->d_f),
-                                                                     static_cast<C*>(out), h->N, h->kp.f16_inv);
-  }
-  static void encode(flb_engine* h, const void* in) {
-    k_encode<S, C><<<lin_grid(9ull * h->N), kBlock, 0, h->stream>>>(static_cast<S*>(h->d_f),
-                                                                     static_cast<const C*>(in), h->N,
-                                                                     h->kp.f16_scale);
-  }
+  static void decode(flb_engine* h, void* out) { launch_decode<S, C, M>(h->kp, h->stream, out); }
+  static void encode(flb_engine* h, const void* in) { launch_encode<S, C, M>(h->kp, h->stream, in); }
 };
 
 template <class Fn>
@@ -199,6 +144,7 @@ void refresh_params(flb_engine* h) {
   k.ny = h->ny;
   k.N = h->N;
   k.f = h->d_f;
+  for (int q = 0; q < 9; q++) k.slot[q] = static_cast<char*>(h->d_f) + (size_t)q * h->N * h->s_size;
   k.rho = h->d_rho;
   k.u = h->d_u;
   k.flags = h->d_flags[h->cur];
@@ -299,6 +245,7 @@ flb_status validate(const flb_case_desc* d, std::string& msg) {
     return msg = "bounce_back must be IMPLICIT or HALFWAY", FLB_ERR_INVALID_ARGUMENT;
   if (d->fs_mode != FLB_FS_REFERENCE && d->fs_mode != FLB_FS_CONSERVATIVE)
     return msg = "fs_mode must be REFERENCE or CONSERVATIVE", FLB_ERR_INVALID_ARGUMENT;
+  if (!(d->u_max >= 0.0f) || !std::isfinite(d->u_max)) return msg = "u_max must be finite and >= 0", FLB_ERR_INVALID_ARGUMENT;
   if (d->kernel_variant < 0 || d->kernel_variant > 2) return msg = "kernel_variant must be 0, 1 or 2", FLB_ERR_INVALID_ARGUMENT;
   if (d->kernel_variant == 2 && d->nx % (d->precision == 64 ? 2u : 4u) != 0)
     return msg = "the vector stream-collide needs nx divisible by its vector width", FLB_ERR_UNSUPPORTED;
@@ -323,19 +270,16 @@ flb_status check_io(flb_engine* h, const uint8_t* flags) {
 // Builds the initial state from the geometry flags in d_geo.
 flb_status initialise(flb_engine* h) {
   FLB_CUDA(h, cudaMemsetAsync(h->d_f, 0, 9ull * h->N * h->s_size, h->stream));
-  const dim3 g = row_grid(h->nx, h->ny);
   h->cur = 0;
   h->t = 0;
-  if (h->fs) {
-    k_init_flags<<<g, kBlock, 0, h->stream>>>(h->d_geo, h->d_flags[0], h->nx, h->ny, 1, h->d_mass, h->d_excess,
-                                              h->d_phi, h->m_size == 8);
-  } else {
-    k_init_flags<<<g, kBlock, 0, h->stream>>>(h->d_geo, h->d_flags[0], h->nx, h->ny, 0, nullptr, nullptr, nullptr,
-                                              1);
-  }
+  if (h->fs)
+    launch_init_flags(h->d_geo, h->d_flags[0], h->nx, h->ny, 1, h->d_mass, h->d_excess, h->d_phi, h->m_size == 8,
+                      h->stream);
+  else
+    launch_init_flags(h->d_geo, h->d_flags[0], h->nx, h->ny, 0, nullptr, nullptr, nullptr, 1, h->stream);
   h->launches++;
   if (h->hw) {
-    k_nbmask<<<g, kBlock, 0, h->stream>>>(h->d_geo, h->d_nbmask, h->nx, h->ny);
+    launch_nbmask(h->d_geo, h->d_nbmask, h->nx, h->ny, h->stream);
     h->launches++;
   }
   refresh_params(h);
@@ -406,7 +350,7 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
     h->s_size = 4; h->c_size = 4; h->m_size = 8;
   }
   {
-    const uint32_t V = desc->precision == 64 ? 2u : 4u;
+    const uint32_t V = (uint32_t)vec_width(desc->precision);
     h->use_vec = desc->kernel_variant == 2 || (desc->kernel_variant == 0 && desc->nx % V == 0);
   }
   s = check_io(h, desc->flags);
@@ -469,7 +413,7 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
   k.inlet_ux = desc->inlet_ux;
   k.inlet_uy = desc->inlet_uy;
   k.fs_cons = desc->fs_mode == FLB_FS_CONSERVATIVE ? 1 : 0;
-  k.count_pre = 0;
+  k.u_max = desc->u_max > 0.0f ? desc->u_max : 0.0f;
   cudaError_t e = cudaMemcpyAsync(h->d_geo, desc->flags, N, cudaMemcpyHostToDevice, h->stream);
   if (e != cudaSuccess) return bail(cuda_fail(h, e, "cudaMemcpyAsync"));
   s = initialise(h);
@@ -681,7 +625,7 @@ FLB_API flb_status flb_total_mass(flb_handle h, double* mass) {
   const uint32_t odd = (uint32_t)(h->t & 1u);
   dispatch(h, [&](auto ops) { ops.mass_partial(h, odd); });
   const uint32_t blocks = (h->N + kBlock - 1) / kBlock;
-  k_sum_partials<<<1, kBlock, 0, h->stream>>>(h->d_partial, blocks, h->d_scalar);
+  launch_sum_partials(h->d_partial, blocks, h->d_scalar, h->stream);
   h->launches += 2;
   FLB_CUDA(h, cudaGetLastError());
   FLB_CUDA(h, cudaMemcpyAsync(mass, h->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, h->stream));

@@ -1,0 +1,354 @@
+// k_fs.cu -- the free-surface passes: FS_1 (lbmKernel2D.cu:14-121) and FS_2,
+// FS_3, FS_4 fused into one shared-memory flag-stencil kernel
+// (lbmKernel2D.cu:124-303).  Templated on the step parity.
+#include "launch.h"
+
+namespace flb {
+
+// ---- FS_1: mass exchange and gas reconstruction, lbmKernel2D.cu:14-121 -----
+template <class S, class C, class M, bool HW, bool ODD>
+__global__ void __launch_bounds__(kBlock) k_fs1(const __grid_constant__ KParams p) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t y = blockIdx.y;
+  if (x >= p.nx) return;
+  const uint32_t nx = p.nx, N = p.N;
+  const uint32_t idx = x + y * nx;
+  const uint8_t* flags = p.flags;
+  const uint8_t flag = flags[idx];
+  if (flag & (kGas | kWall | kInlet)) return;
+  const bool cons = p.fs_cons != 0;
+  const uint8_t e = flag & kFGI;
+  if (cons && (!(e == kFluid || e == kInterface) || (flag & kMovingWall))) return;
+  uint32_t nb[9];
+  neighbours(x, y, nx, p.ny, nb);
+  C in[9], out[9];
+  load_in<S, C, HW, ODD>(p, idx, nb, HW ? p.nbmask[idx] : 0u, in);
+  out[0] = in[0];
+  load_out<S, C, ODD>(p, idx, nb, out);
+  M* Ms = static_cast<M*>(p.mass);
+  const M* Ex = static_cast<const M*>(p.excess);
+  const M* Ph = static_cast<const M*>(p.phi);
+  M m = Ms[idx];
+#pragma unroll
+  for (int i = 1; i < 9; i++) m += Ex[nb[i]];
+  if (e == kFluid) {
+    if (!cons) {
+#pragma unroll
+      for (int i = 1; i < 9; i += 2) {
+        m += in[i + 1] - out[i];
+        m += in[i] - out[i + 1];
+      }
+    } else {
+#pragma unroll
+      for (int i = 1; i < 9; i += 2) {
+        const uint8_t na = flags[nb[i]] & kFGI, nbb = flags[nb[i + 1]] & kFGI;
+        if (na == kFluid || na == kInterface) m += in[i + 1] - out[i];
+        if (nbb == kFluid || nbb == kInterface) m += in[i] - out[i + 1];
+      }
+    }
+  } else if (e == kInterface) {
+    C rho, ux, uy, rhoYL = 0.0f;
+    if (flag & (kInlet | kOutlet)) {
+      rho = static_cast<const C*>(p.rho)[idx];
+      ux = static_cast<const C*>(p.u)[idx];
+      uy = static_cast<const C*>(p.u)[idx + N];
+    } else {
+      rho = density(out);
+      velocity(out, rho, ux, uy);
+    }
+    M phiN[9];
+#pragma unroll
+    for (int i = 1; i < 9; i++) phiN[i] = Ph[nb[i]];
+    phiN[0] = cons ? Ph[idx] : fill_level<M, C>(m, rho);
+    const C rho2 = 0.5f / rho;
+    ux = ux + rho2 * p.fx;
+    uy = uy + rho2 * p.fy;
+    limit_u(p.u_max, ux, uy);
+    C feq[9];
+    equilibrium<C>(1.0f - rhoYL, ux, uy, feq);
+    uint8_t nF[9];
+#pragma unroll
+    for (int i = 1; i < 9; i++) nF[i] = flags[nb[i]] & kFGI;
+#pragma unroll
+    for (int i = 1; i < 9; i += 2) {
+      uint8_t ne = nF[i];
+      if (ne == kFluid) m += in[i + 1] - out[i];
+      else if (ne == kInterface) m += (in[i + 1] - out[i]) * 0.5f * (phiN[i] + phiN[0]);
+      ne = nF[i + 1];
+      if (ne == kFluid) m += in[i] - out[i + 1];
+      else if (ne == kInterface) m += (in[i] - out[i + 1]) * 0.5f * (phiN[i + 1] + phiN[0]);
+    }
+#pragma unroll
+    for (int i = 1; i < 9; i += 2) {
+      in[i] = feq[i] - out[i + 1] + feq[i + 1];
+      in[i + 1] = feq[i + 1] - out[i] + feq[i];
+    }
+    if (!cons) {
+      // reference gate (storeReconstructedGasf, cellCalculations.cuh:250-259):
+      // tests the neighbour the population travels toward.  Parked in recon so
+      // that neighbours reading their outgoing slots see the pre-pass values.
+      C* rec = static_cast<C*>(p.recon);
+      uint32_t mask = 0;
+#pragma unroll
+      for (int i = 1; i < 9; i += 2) {
+        if (nF[i] == kGas) { mask |= 1u << (i - 1); rec[(uint32_t)(i - 1) * N + idx] = in[i]; }
+        if (nF[i + 1] == kGas) { mask |= 1u << i; rec[(uint32_t)i * N + idx] = in[i + 1]; }
+      }
+      p.recon_mask[idx] = (uint8_t)mask;
+    } else {
+      // population arriving from a gas neighbour: its slot is read by no other
+      // cell in this pass (the gas cell does not run), so store in place
+      const float scale = p.f16_scale;
+#pragma unroll
+      for (int i = 1; i < 9; i += 2) {
+        if (nF[i + 1] == kGas) Codec<S, C>::st(slotp<S>(p, slot_a<ODD>(i)), idx, i, in[i], scale);
+        if (nF[i] == kGas) Codec<S, C>::st(slotp<S>(p, slot_b<ODD>(i)), nb[i], i + 1, in[i + 1], scale);
+      }
+    }
+  }
+  Ms[idx] = m;
+}
+
+// Writes the populations FS_1 parked in recon (reference mode) into their
+// incoming slots, as the reference FS_1 kernel does itself.  Only the
+// isolated-pass path uses it; a full step hands them to stream-collide.
+template <class S, class C>
+__global__ void k_apply_recon(const __grid_constant__ KParams p, uint32_t odd) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t y = blockIdx.y;
+  if (x >= p.nx) return;
+  const uint32_t N = p.N, idx = x + y * p.nx;
+  const uint8_t flag = p.flags[idx];
+  if ((flag & (kFGI | kGas | kWall | kInlet)) != kInterface) return;
+  const uint32_t m = p.recon_mask[idx];
+  if (!m) return;
+  uint32_t nb[9];
+  neighbours(x, y, p.nx, p.ny, nb);
+  const C* rec = static_cast<const C*>(p.recon);
+#pragma unroll
+  for (int i = 1; i < 9; i += 2) {
+    const int a = odd ? i : i + 1, b = odd ? i + 1 : i;
+    if ((m >> (i - 1)) & 1u) Codec<S, C>::st(slotp<S>(p, a), idx, i, rec[(uint32_t)(i - 1) * N + idx], p.f16_scale);
+    if ((m >> i) & 1u) Codec<S, C>::st(slotp<S>(p, b), nb[i], i + 1, rec[(uint32_t)i * N + idx], p.f16_scale);
+  }
+  p.recon_mask[idx] = 0;
+}
+
+// ---- FS_2 + FS_3 + FS_4 fused: lbmKernel2D.cu:124-303 ----------------------
+// The three reference passes are flag stencils of radius one, chained; a tile
+// of 32x8 cells stages the flags of its 3-cell halo in shared memory and
+// evaluates the chain there, so neighbour flags are never read while another
+// block rewrites them.  Reads p.flags, writes p.flags_out.
+constexpr int kTX = 32, kTY = 8, kHalo = 3;
+constexpr int kSX = kTX + 2 * kHalo, kSY = kTY + 2 * kHalo;
+
+__device__ __forceinline__ int wrapi(int v, int n) {
+  v %= n;
+  return v < 0 ? v + n : v;
+}
+
+template <class S, class C, class M, bool ODD>
+__global__ void __launch_bounds__(kTX* kTY) k_fs234(const __grid_constant__ KParams p) {
+  __shared__ uint8_t s0[kSY][kSX];  // after stream-collide
+  __shared__ uint8_t s1[kSY][kSX];  // after FS_2
+  __shared__ uint8_t s2[kSY][kSX];  // after FS_3
+  __shared__ uint8_t s3[kSY][kSX];  // after FS_4 conversion
+  const int nx = (int)p.nx, ny = (int)p.ny;
+  const int x0 = (int)blockIdx.x * kTX - kHalo, y0 = (int)blockIdx.y * kTY - kHalo;
+  const int tid = threadIdx.x + threadIdx.y * kTX;
+  const uint8_t* flags = p.flags;
+  for (int k = tid; k < kSX * kSY; k += kTX * kTY) {
+    const int lx = k % kSX, ly = k / kSX;
+    s0[ly][lx] = flags[wrapi(x0 + lx, nx) + wrapi(y0 + ly, ny) * nx];
+  }
+  __syncthreads();
+  // FS_2: next to an IF cell, IG -> I and G -> GI
+  for (int k = tid; k < kSX * kSY; k += kTX * kTY) {
+    const int lx = k % kSX, ly = k / kSX;
+    if (lx < 1 || ly < 1 || lx >= kSX - 1 || ly >= kSY - 1) continue;
+    uint8_t f = s0[ly][lx];
+    bool any_if = false;
+#pragma unroll
+    for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+      for (int dx = -1; dx <= 1; dx++)
+        if (dx || dy) any_if |= (s0[ly + dy][lx + dx] & kIF) == kIF;
+    if (any_if) {
+      const uint8_t e = f & kIG;
+      if (e == kIG) f = (uint8_t)(f & ~kGas);
+      else if (e == kGas) f = (uint8_t)((f & ~kGas) | kGasInterface);
+    }
+    s1[ly][lx] = f;
+  }
+  __syncthreads();
+  // FS_3 flags: next to an IG cell, F / IF (not inlet) -> I
+  for (int k = tid; k < kSX * kSY; k += kTX * kTY) {
+    const int lx = k % kSX, ly = k / kSX;
+    if (lx < 2 || ly < 2 || lx >= kSX - 2 || ly >= kSY - 2) continue;
+    uint8_t f = s1[ly][lx];
+    const uint8_t e = f & (kInletFluid | kInterface);
+    if (e != kInletFluid && (e == kFluid || e == kIF)) {
+      bool any_ig = false;
+#pragma unroll
+      for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+        for (int dx = -1; dx <= 1; dx++)
+          if (dx || dy) any_ig |= (s1[ly + dy][lx + dx] & (kGasInterface | kIG)) == kIG;
+      if (any_ig) f = (uint8_t)((f & ~kIF) | kInterface);
+    }
+    s2[ly][lx] = f;
+    // FS_4 conversion
+    uint8_t g = f;
+    if (!(g & (kWall | kMovingWall | kInlet))) {
+      const uint8_t sw = g & (kFGI | kGasInterface);
+      if (sw == kIF || sw == kIG) g = (uint8_t)(g & ~kInterface);
+      else if (sw == kGasInterface) g = (uint8_t)((g & ~kGasInterface) | kInterface);
+    }
+    s3[ly][lx] = g;
+  }
+  __syncthreads();
+  const int lx = threadIdx.x + kHalo, ly = threadIdx.y + kHalo;
+  const int gx = (int)blockIdx.x * kTX + (int)threadIdx.x, gy = (int)blockIdx.y * kTY + (int)threadIdx.y;
+  if (gx >= nx || gy >= ny) return;
+  const uint32_t N = p.N, idx = (uint32_t)gx + (uint32_t)gy * (uint32_t)nx;
+  const uint8_t f1 = s1[ly][lx];
+  const uint8_t f3 = s2[ly][lx];
+  const uint8_t fin = s3[ly][lx];
+  // Write skipping.  flags_out still holds this cell's flag after the previous
+  // step's stream-collide ("old").  When the buffers come from consecutive
+  // full steps (trust_prev), a value already in memory is not rewritten:
+  //  * the flag, when old equals the new flag;
+  //  * all mass fields of a cell that was gas in the previous step and stays
+  //    gas: that step (or the initial state) left m = excess = phi = +0, and
+  //    FS_1 does not touch gas cells, so FS_4 would write the same zeros;
+  //  * the fill level of a cell that was fluid after the previous step and
+  //    stays fluid: it is already 1.
+  const bool trust = p.trust_prev != 0;
+  const uint8_t old = p.flags_out[idx];
+  if (!trust || old != fin) p.flags_out[idx] = fin;
+  const C* R = static_cast<const C*>(p.rho);
+  const C* U = static_cast<const C*>(p.u);
+  uint32_t nb[9];
+  neighbours((uint32_t)gx, (uint32_t)gy, (uint32_t)nx, (uint32_t)ny, nb);
+  // FS_3 fields: a gas->interface cell starts from feq of the neighbour
+  // average (calculateAverageValuesNeighbors2D, accumulating in float)
+  if ((f1 & (kGasInterface | kIG)) == kGasInterface) {
+    float count = 0.0f, lrho = 0.0f, lux = 0.0f, luy = 0.0f;
+    const int ddx[9] = {0, 1, -1, 0, 0, 1, -1, 1, -1};
+    const int ddy[9] = {0, 0, 0, 1, -1, 1, -1, -1, 1};
+#pragma unroll
+    for (int i = 1; i < 9; i++) {
+      if (s1[ly + ddy[i]][lx + ddx[i]] & kIF) {
+        count += 1.0f;
+        lrho += R[nb[i]];
+        lux += U[nb[i]];
+        luy += U[nb[i] + N];
+      }
+    }
+    C rho = count > 0.0f ? lrho / count : 0.0f;
+    C ux = count > 0.0f ? lux / count : 0.0f;
+    C uy = count > 0.0f ? luy / count : 0.0f;
+    C feq[9];
+    const C rho2 = 0.5f / rho;
+    ux = ux + rho2 * p.fx;
+    uy = uy + rho2 * p.fy;
+    limit_u(p.u_max, ux, uy);
+    equilibrium(rho, ux, uy, feq);
+    store_post<S, C, ODD>(p, idx, nb, feq);
+  }
+  // FS_4 fields
+  if (f3 & (kWall | kMovingWall | kInlet)) return;
+  const uint8_t sw4 = f3 & (kFGI | kGasInterface);
+  if (trust && sw4 == kGas && (old & (kFGI | kGasInterface)) == kGas) return;
+  const bool keep_phi = trust && sw4 == kFluid && (s0[ly][lx] & (kFGI | kGasInterface)) == kFluid;
+  M* Ms = static_cast<M*>(p.mass);
+  const C rho = R[idx];
+  M m = Ms[idx];
+  M ex = 0.0f, ph = 0.0f;
+  switch (f3 & (kFGI | kGasInterface)) {
+    case 1:
+    case 5:
+      ex = m - rho;
+      m = rho;
+      ph = 1.0f;
+      break;
+    case 2:
+    case 6:
+      ex = m;
+      m = 0.0f;
+      ph = 0.0f;
+      break;
+    case 4:
+    case 128:
+      if (m > rho) {
+        ex = m - rho;
+        m = rho;
+      } else if (m < 0.0f) {
+        ex = m;
+        m = 0.0f;
+      } else {
+        ex = 0.0f;
+      }
+      ph = fill_level<M, C>(m, rho);
+      break;
+    default:
+      break;
+  }
+  int cont = 0;
+  const bool cons = p.fs_cons != 0;
+#pragma unroll
+  for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+    for (int dx = -1; dx <= 1; dx++) {
+      if (!dx && !dy) continue;
+      const uint8_t v = s3[ly + dy][lx + dx];  // converted flags
+      if (cons) {
+        const uint8_t ev = v & kFGI;
+        cont += (ev == kFluid || ev == kInterface) && !(v & (kWall | kMovingWall | kInlet));
+      } else {
+        const uint8_t ev = v & (kIF | kGasInterface);
+        cont += ev == kFluid || ev == kInterface || ev == kIF || ev == kGasInterface;
+      }
+    }
+  m += cont > 0 ? 0.0f : ex;
+  ex = cont > 0 ? ex / (float)cont : 0.0f;
+  Ms[idx] = m;
+  static_cast<M*>(p.excess)[idx] = ex;
+  if (!keep_phi) static_cast<M*>(p.phi)[idx] = ph;
+}
+
+
+// ---- launchers -------------------------------------------------------------------
+template <class S, class C, class M>
+void launch_fs1(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw) {
+  const dim3 g((kp.nx + kBlock - 1) / kBlock, kp.ny);
+  if (hw) {
+    if (odd) k_fs1<S, C, M, true, true><<<g, kBlock, 0, st>>>(kp);
+    else k_fs1<S, C, M, true, false><<<g, kBlock, 0, st>>>(kp);
+  } else {
+    if (odd) k_fs1<S, C, M, false, true><<<g, kBlock, 0, st>>>(kp);
+    else k_fs1<S, C, M, false, false><<<g, kBlock, 0, st>>>(kp);
+  }
+}
+
+template <class S, class C, class M>
+void launch_apply_recon(const KParams& kp, cudaStream_t st, uint32_t odd) {
+  k_apply_recon<S, C><<<dim3((kp.nx + kBlock - 1) / kBlock, kp.ny), kBlock, 0, st>>>(kp, odd);
+}
+
+template <class S, class C, class M>
+void launch_fs234(const KParams& kp, cudaStream_t st, uint32_t odd) {
+  const dim3 g((kp.nx + kTX - 1) / kTX, (kp.ny + kTY - 1) / kTY);
+  const dim3 b(kTX, kTY);
+  if (odd) k_fs234<S, C, M, true><<<g, b, 0, st>>>(kp);
+  else k_fs234<S, C, M, false><<<g, b, 0, st>>>(kp);
+}
+
+#define FLB_INSTANTIATE(S, C, M)                                                      \
+  template void launch_fs1<S, C, M>(const KParams&, cudaStream_t, uint32_t, bool);    \
+  template void launch_apply_recon<S, C, M>(const KParams&, cudaStream_t, uint32_t); \
+  template void launch_fs234<S, C, M>(const KParams&, cudaStream_t, uint32_t);
+FLB_FOR_EACH_VARIANT(FLB_INSTANTIATE)
+#undef FLB_INSTANTIATE
+
+}  // namespace flb

@@ -1,0 +1,411 @@
+// k_sc.cu -- stream-collide: d_StreamCollide2D, lbmKernel2D.cu:306-519.
+//
+// Two data paths with the same per-cell arithmetic (collide_cell):
+//  * k_sc_scalar: one cell per thread;
+//  * k_sc_vec: V consecutive cells of a row per thread (V = 4 for FP32 and
+//    FP16S, 2 for FP64), every population slot moved with one aligned V-wide
+//    access (16 bytes for FP32/FP64, 8 for FP16S).  Own-cell slots and the
+//    (x, y+1) slot are aligned as they are; the three slots at the x+1
+//    neighbour ((x+1,y), (x+1,y+1), (x+1,y-1)) are loaded aligned at x0 and
+//    shifted one cell with a warp shuffle (the cell past the warp, or the
+//    row's periodic wrap, is a scalar), and stored the other way: an aligned
+//    store at x0 whose first element comes from the previous lane, lane 0
+//    writing its first V-1 elements as scalars and the warp's last lane the
+//    element past the warp.  A cell that is not updated (wall, gas) writes
+//    back the raw values it loaded: no other thread writes a slot that
+//    cell owns during this pass.
+// Both are templated on the step parity (slot indices become constants) and,
+// for the single-phase build, issue the population loads together with the
+// flag load instead of after it.
+#include "launch.h"
+
+namespace flb {
+
+// Everything between the load and the store of d_StreamCollide2D for one
+// updated cell: density and velocity (or the inlet/outlet values), interface
+// marking, Guo forcing, the optional velocity limiter, density/velocity
+// write-back, equilibrium, Smagorinsky, SRT/TRT.  f: incoming -> post.
+template <class C, class M, bool FS, bool WM>
+__device__ __forceinline__ void collide_cell(const KParams& p, uint32_t idx, uint32_t x, uint32_t y, uint8_t flag,
+                                             C* f) {
+  const uint32_t N = p.N;
+  if constexpr (FS) {
+    // reference mode: FS_1 left the populations it rebuilt toward gas here
+    if (!p.fs_cons && (flag & (kFGI | kInlet)) == kInterface) {
+      const uint32_t m = p.recon_mask[idx];
+      if (m) {
+        const C* rec = static_cast<const C*>(p.recon);
+#pragma unroll
+        for (int k = 0; k < 8; k++)
+          if ((m >> k) & 1u) f[k + 1] = rec[(uint32_t)k * N + idx];
+      }
+    }
+  }
+  C rho, ux, uy;
+  const uint8_t io = flag & (kInlet | kOutlet);
+  if (io & kInlet) {
+    const C* Rs = static_cast<const C*>(p.rho_snap);
+    const C* Us = static_cast<const C*>(p.u_snap);
+    rho = Rs[idx + 1];
+    ux = Us[idx];
+    uy = Us[idx + N];
+  } else if (flag & kOutlet) {
+    const C* Rs = static_cast<const C*>(p.rho_snap);
+    const C* Us = static_cast<const C*>(p.u_snap);
+    rho = Rs[idx];
+    ux = Us[idx - 1];
+    uy = Us[idx + N - 1];
+  } else {
+    rho = density(f);
+    velocity(f, rho, ux, uy);
+  }
+  if constexpr (FS) {
+    if ((flag & kInterface) == kInterface) {
+      uint32_t nb[9];
+      neighbours(x, y, p.nx, p.ny, nb);
+      const M m = static_cast<const M*>(p.mass)[idx];
+      bool notFluid = true, notGas = true;
+#pragma unroll
+      for (int i = 1; i < 9; i++) {
+        const uint8_t e = p.flags[nb[i]] & kFGI;
+        notFluid = notFluid && (e != kFluid);
+        notGas = notGas && (e != kGas);
+      }
+      // neighbours read these bytes concurrently; IF/IG compare unequal to
+      // FLUID and GAS either way, so the outcome does not depend on timing
+      if ((m > 1.001f * rho) || notGas) p.flags[idx] = (uint8_t)((flag & ~kFGI) | kIF);
+      else if ((m < -0.001f) || notFluid) p.flags[idx] = (uint8_t)((flag & ~kFGI) | kIG);
+    }
+  }
+  C Fi[9];
+  const bool use_force = p.use_force != 0;
+  if (use_force) {
+    const C rhol2 = 0.5f / rho;
+    ux = ux + rhol2 * p.fx;
+    uy = uy + rhol2 * p.fy;
+  }
+  limit_u(p.u_max, ux, uy);
+  if (use_force) forcing(Fi, ux, uy, p.fx, p.fy);
+  if (FS || WM) {
+    C* R = static_cast<C*>(p.rho);
+    C* U = static_cast<C*>(p.u);
+    if (!io || (flag & kOutlet)) {
+      U[idx] = ux;
+      U[idx + N] = uy;
+    }
+    R[idx] = rho;
+  }
+  C feq[9];
+  equilibrium(rho, ux, uy, feq);
+  float invTau = p.inv_tau;
+  if (p.subgrid) {
+    C Hxx = 0.0f, Hyy = 0.0f, Hxy = 0.0f;
+#pragma unroll
+    for (int i = 1; i < 9; i++) {
+      const C fne = f[i] - feq[i];
+      const C ccx = (C)cx(i), ccy = (C)cy(i);
+      Hxx += ccx * ccx * fne;
+      Hyy += ccy * ccy * fne;
+      Hxy += ccx * ccy * fne;
+    }
+    const C Q = Hxx * Hxx + Hyy * Hyy + 2.0f * Hxy * Hxy;
+    const float tau = 1.0f / invTau;
+    invTau = 2.0f / (tau + sqrtf(tau * tau + 0.54037965f * sqrtf(Q) / rho));
+  }
+  if (p.collision == 0) {
+    if (!io) {
+      if (use_force) {
+        const float taul = 1.0f - 0.5f * invTau;
+#pragma unroll
+        for (int i = 0; i < 9; i++) f[i] = (1.0f - invTau) * f[i] + invTau * feq[i] + taul * Fi[i];
+      } else {
+#pragma unroll
+        for (int i = 0; i < 9; i++) f[i] = (1.0f - invTau) * f[i] + invTau * feq[i];
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 9; i++) f[i] = feq[i];
+    }
+  } else {
+    const float invTauPos = invTau;
+    const float invTauNeg = 1.0f / (0.25f / (1.0f / invTau - 0.5f) + 0.5f);
+    if (!io) {
+      if (!use_force) {  // with forcing the reference leaves TRT empty (lbmKernel2D.cu:485-488)
+        f[0] = f[0] - invTauPos * (f[0] - feq[0]);
+#pragma unroll
+        for (int i = 1; i < 9; i += 2) {
+          const float fMinusFeq = f[i] - feq[i] + f[i + 1] - feq[i + 1];
+          const float fAnti = f[i] - f[i + 1];
+          const float feqAnti = feq[i] - feq[i + 1];
+          f[i] = f[i] - 0.5f * invTauPos * fMinusFeq - 0.5f * invTauNeg * (fAnti - feqAnti);
+          f[i + 1] = f[i + 1] - 0.5f * invTauPos * fMinusFeq - 0.5f * invTauNeg * (feqAnti - fAnti);
+        }
+      }
+    } else {
+#pragma unroll
+      for (int i = 0; i < 9; i++) f[i] = feq[i];
+    }
+  }
+}
+
+// ---- one cell per thread -----------------------------------------------------
+template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD>
+__global__ void __launch_bounds__(kBlock) k_sc_scalar(const __grid_constant__ KParams p) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t y = blockIdx.y;
+  if (x >= p.nx) return;
+  const uint32_t idx = x + y * p.nx;
+  uint32_t nb[9];
+  neighbours(x, y, p.nx, p.ny, nb);
+  C f[9];
+  uint8_t flag;
+  uint32_t nbm = 0;
+  if constexpr (!FS) {
+    // single phase: nearly every cell is updated, so load with the flag
+    flag = p.flags[idx];
+    if (HW) nbm = p.nbmask[idx];
+    load_in<S, C, HW, ODD>(p, idx, nb, nbm, f);
+    if (flag & (kGas | kWall)) return;
+  } else {
+    flag = p.flags[idx];
+    if (flag & (kGas | kWall)) return;
+    if (HW) nbm = p.nbmask[idx];
+    load_in<S, C, HW, ODD>(p, idx, nb, nbm, f);
+  }
+  collide_cell<C, M, FS, WM>(p, idx, x, y, flag, f);
+  store_post<S, C, ODD>(p, idx, nb, f);
+}
+
+// ---- V cells per thread ----------------------------------------------------------
+template <class S, int V>
+struct VecT;
+template <>
+struct VecT<float, 4> { using T = float4; };
+template <>
+struct VecT<double, 2> { using T = double2; };
+template <>
+struct VecT<__half, 4> { using T = uint2; };
+
+template <class S>
+struct Lanes;
+template <>
+struct Lanes<float> { static constexpr int V = 4; };
+template <>
+struct Lanes<double> { static constexpr int V = 2; };
+template <>
+struct Lanes<__half> { static constexpr int V = 4; };
+
+template <class S, int V>
+__device__ __forceinline__ void vload(const S* ptr, S (&r)[V]) {
+  using T = typename VecT<S, V>::T;
+  const T v = *reinterpret_cast<const T*>(ptr);
+  memcpy(r, &v, sizeof(T));
+}
+template <class S, int V>
+__device__ __forceinline__ void vstore(S* ptr, const S (&r)[V]) {
+  using T = typename VecT<S, V>::T;
+  T v;
+  memcpy(&v, r, sizeof(T));
+  *reinterpret_cast<T*>(ptr) = v;
+}
+
+__device__ __forceinline__ float shfl_dn(float v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+__device__ __forceinline__ double shfl_dn(double v) { return __shfl_down_sync(0xffffffffu, v, 1); }
+__device__ __forceinline__ __half shfl_dn(__half v) {
+  return __ushort_as_half((unsigned short)__shfl_down_sync(0xffffffffu, (int)__half_as_ushort(v), 1));
+}
+__device__ __forceinline__ float shfl_up1(float v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+__device__ __forceinline__ double shfl_up1(double v) { return __shfl_up_sync(0xffffffffu, v, 1); }
+__device__ __forceinline__ __half shfl_up1(__half v) {
+  return __ushort_as_half((unsigned short)__shfl_up_sync(0xffffffffu, (int)__half_as_ushort(v), 1));
+}
+
+template <int V>
+__device__ __forceinline__ void load_bytes(const uint8_t* ptr, uint8_t (&f)[V]) {
+  if constexpr (V == 4) {
+    const uchar4 v = *reinterpret_cast<const uchar4*>(ptr);
+    f[0] = v.x; f[1] = v.y; f[2] = v.z; f[3] = v.w;
+  } else {
+    const uchar2 v = *reinterpret_cast<const uchar2*>(ptr);
+    f[0] = v.x; f[1] = v.y;
+  }
+}
+
+constexpr int kVecBlock = 256;
+
+template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD>
+__global__ void __launch_bounds__(kVecBlock) k_sc_vec(const __grid_constant__ KParams p) {
+  constexpr int V = Lanes<S>::V;
+  using K = Codec<S, C>;
+  const uint32_t nx = p.nx, ny = p.ny;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t x0 = (blockIdx.x * blockDim.x + threadIdx.x) * V;
+  const uint32_t y = blockIdx.y;
+  const bool inrow = x0 < nx;
+  const uint32_t row = y * nx;
+  const uint32_t rowu = (y + 1u == ny ? 0u : y + 1u) * nx;
+  const uint32_t rowd = (y == 0u ? ny - 1u : y - 1u) * nx;
+  const bool tail = (lane == 31u) || (x0 + V >= nx);  // the cell past this lane is not the next lane's
+  const uint32_t xn = (x0 + V >= nx) ? 0u : x0 + V;   // position past this lane (periodic wrap)
+
+  uint8_t fl[V];
+  bool act[V];
+  bool any = false;
+  S raw0[V], own[4][V], nbr[4][V], tmp[4][V];
+  if (inrow) load_bytes<V>(p.flags + row + x0, fl);
+  if constexpr (!FS) {
+    // single phase: load the populations with the flags
+    if (inrow) {
+      vload<S, V>(slotp<S>(p, 0) + row + x0, raw0);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int i = 2 * q + 1;
+        const uint32_t r = (i == 1) ? row : (i == 7 ? rowd : rowu);
+        vload<S, V>(slotp<S>(p, slot_a<ODD>(i)) + row + x0, own[q]);
+        vload<S, V>(slotp<S>(p, slot_b<ODD>(i)) + r + x0, tmp[q]);
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < V; k++) {
+    act[k] = inrow && !(fl[k] & (kGas | kWall));
+    any |= act[k];
+  }
+  // a warp with no cell to update leaves memory untouched
+  if (!__any_sync(0xffffffffu, any)) return;
+  if constexpr (FS) {
+    if (inrow) {
+      vload<S, V>(slotp<S>(p, 0) + row + x0, raw0);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int i = 2 * q + 1;
+        const uint32_t r = (i == 1) ? row : (i == 7 ? rowd : rowu);
+        vload<S, V>(slotp<S>(p, slot_a<ODD>(i)) + row + x0, own[q]);
+        vload<S, V>(slotp<S>(p, slot_b<ODD>(i)) + r + x0, tmp[q]);
+      }
+    }
+  }
+  // realign the x+1 slots
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int i = 2 * q + 1;
+    if (i == 3) {
+#pragma unroll
+      for (int k = 0; k < V; k++) nbr[q][k] = tmp[q][k];
+    } else {
+      const uint32_t r = (i == 1) ? row : (i == 7 ? rowd : rowu);
+      const S from_next = shfl_dn(tmp[q][0]);
+#pragma unroll
+      for (int k = 0; k < V - 1; k++) nbr[q][k] = tmp[q][k + 1];
+      nbr[q][V - 1] = (tail && inrow) ? slotp<S>(p, slot_b<ODD>(i))[r + xn] : from_next;
+    }
+  }
+  uint8_t nbmv[V];
+#pragma unroll
+  for (int k = 0; k < V; k++) nbmv[k] = 0;
+  if (HW && inrow) load_bytes<V>(p.nbmask + row + x0, nbmv);
+
+  // ---- per-cell collision; cells not updated keep their raw values ---------
+#pragma unroll
+  for (int k = 0; k < V; k++) {
+    if (!act[k]) continue;
+    const uint32_t x = x0 + k;
+    const uint32_t idx = row + x;
+    C f[9];
+    f[0] = K::ld(raw0, k, 0, p.f16_inv);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int i = 2 * q + 1;
+      f[i] = K::ld(own[q], k, i, p.f16_inv);
+      f[i + 1] = K::ld(nbr[q], k, i + 1, p.f16_inv);
+    }
+    const uint32_t nbm = nbmv[k];
+    if (HW && nbm) {
+      // half-way walls: reflected populations, scalar (wall-adjacent cells only)
+      uint32_t nb[9];
+      neighbours(x, y, nx, ny, nb);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int i = 2 * q + 1;
+        if ((nbm >> i) & 1u) f[i] = K::ld(slotp<S>(p, slot_b<ODD>(i)), idx, i, p.f16_inv);
+        if ((nbm >> (i - 1)) & 1u) f[i + 1] = K::ld(slotp<S>(p, slot_a<ODD>(i)), nb[i], i + 1, p.f16_inv);
+      }
+    }
+    collide_cell<C, M, FS, WM>(p, idx, x, y, fl[k], f);
+    K::st(raw0, k, 0, f[0], p.f16_scale);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int i = 2 * q + 1;
+      K::st(nbr[q], k, i, f[i], p.f16_scale);      // post f_i -> neighbour slot b
+      K::st(own[q], k, i + 1, f[i + 1], p.f16_scale);  // post f_{i+1} -> own slot a
+    }
+  }
+
+  // ---- stores ------------------------------------------------------------------
+  if (inrow) vstore<S, V>(slotp<S>(p, 0) + row + x0, raw0);
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int i = 2 * q + 1;
+    if (inrow) vstore<S, V>(slotp<S>(p, slot_a<ODD>(i)) + row + x0, own[q]);
+    const uint32_t r = (i == 1) ? row : (i == 7 ? rowd : rowu);
+    S* dst = slotp<S>(p, slot_b<ODD>(i)) + r;
+    if (i == 3) {
+      if (inrow) vstore<S, V>(dst + x0, nbr[q]);
+    } else {
+      const S from_prev = shfl_up1(nbr[q][V - 1]);
+      if (inrow) {
+        if (lane != 0u) {
+          S v[V];
+          v[0] = from_prev;
+#pragma unroll
+          for (int k = 1; k < V; k++) v[k] = nbr[q][k - 1];
+          vstore<S, V>(dst + x0, v);
+        } else {
+#pragma unroll
+          for (int k = 0; k < V - 1; k++) dst[x0 + 1 + k] = nbr[q][k];
+        }
+        if (tail) dst[xn] = nbr[q][V - 1];
+      }
+    }
+  }
+}
+
+// ---- launchers -------------------------------------------------------------------
+template <class S, class C, class M, bool FS, bool HW, bool WM>
+static void launch_sc_t(const KParams& kp, cudaStream_t st, uint32_t odd, bool vec) {
+  if (vec) {
+    constexpr int V = Lanes<S>::V;
+    const uint32_t per_row = kp.nx / V;
+    const uint32_t block = per_row >= (uint32_t)kVecBlock ? (uint32_t)kVecBlock : ((per_row + 31u) / 32u) * 32u;
+    const dim3 g((per_row + block - 1) / block, kp.ny);
+    if (odd) k_sc_vec<S, C, M, FS, HW, WM, true><<<g, block, 0, st>>>(kp);
+    else k_sc_vec<S, C, M, FS, HW, WM, false><<<g, block, 0, st>>>(kp);
+  } else {
+    const dim3 g((kp.nx + kBlock - 1) / kBlock, kp.ny);
+    if (odd) k_sc_scalar<S, C, M, FS, HW, WM, true><<<g, kBlock, 0, st>>>(kp);
+    else k_sc_scalar<S, C, M, FS, HW, WM, false><<<g, kBlock, 0, st>>>(kp);
+  }
+}
+
+template <class S, class C, class M>
+void launch_sc(const KParams& kp, cudaStream_t st, uint32_t odd, bool fs, bool hw, bool wm, bool vec) {
+  if (fs) {
+    if (hw) launch_sc_t<S, C, M, true, true, true>(kp, st, odd, vec);
+    else launch_sc_t<S, C, M, true, false, true>(kp, st, odd, vec);
+  } else if (wm) {
+    if (hw) launch_sc_t<S, C, M, false, true, true>(kp, st, odd, vec);
+    else launch_sc_t<S, C, M, false, false, true>(kp, st, odd, vec);
+  } else {
+    if (hw) launch_sc_t<S, C, M, false, true, false>(kp, st, odd, vec);
+    else launch_sc_t<S, C, M, false, false, false>(kp, st, odd, vec);
+  }
+}
+
+int vec_width(int precision) { return precision == 64 ? Lanes<double>::V : Lanes<float>::V; }
+
+#define FLB_INSTANTIATE(S, C, M) \
+  template void launch_sc<S, C, M>(const KParams&, cudaStream_t, uint32_t, bool, bool, bool, bool);
+FLB_FOR_EACH_VARIANT(FLB_INSTANTIATE)
+#undef FLB_INSTANTIATE
+
+}  // namespace flb

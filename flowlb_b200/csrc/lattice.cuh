@@ -117,6 +117,19 @@ __device__ __forceinline__ M fill_level(M m, C rho) {
   return (M)0.5f;
 }
 
+// Optional velocity limiter (no reference counterpart; off unless u_max > 0):
+// scales u down to |u| = u_max.
+template <class C>
+__device__ __forceinline__ void limit_u(float umax, C& ux, C& uy) {
+  if (!(umax > 0.0f)) return;
+  const C uu = ux * ux + uy * uy;
+  if (uu > umax * umax) {
+    const C sc = umax / sqrt(uu);
+    ux = ux * sc;
+    uy = uy * sc;
+  }
+}
+
 // Neighbour cells with periodic wrap, cellCalculations.cuh:82-109.
 __device__ __forceinline__ void neighbours(uint32_t x, uint32_t y, uint32_t nx, uint32_t ny, uint32_t* nb) {
   const uint32_t yc = y * nx;

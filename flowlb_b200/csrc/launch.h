@@ -1,0 +1,52 @@
+// launch.h -- host launchers of the engine's kernels (one translation unit
+// per pass family: k_init.cu, k_sc.cu, k_fs.cu, k_reduce.cu).  Each is
+// instantiated for the four storage variants below.
+#pragma once
+
+#include <cstdint>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+// (storage, arithmetic, mass) type triples
+#define FLB_FOR_EACH_VARIANT(X) \
+  X(double, double, double)     \
+  X(float, float, double)       \
+  X(__half, float, double)      \
+  X(float, float, float)
+
+namespace flb {
+
+// stream-collide; vec selects the V-cells-per-thread data path
+template <class S, class C, class M>
+void launch_sc(const KParams& kp, cudaStream_t st, uint32_t odd, bool fs, bool hw, bool wm, bool vec);
+int vec_width(int precision);
+
+// FS_1, its reference-mode apply, and FS_2..4
+template <class S, class C, class M>
+void launch_fs1(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw);
+template <class S, class C, class M>
+void launch_apply_recon(const KParams& kp, cudaStream_t st, uint32_t odd);
+template <class S, class C, class M>
+void launch_fs234(const KParams& kp, cudaStream_t st, uint32_t odd);
+
+// initial state
+void launch_init_flags(const uint8_t* geo, uint8_t* flags, uint32_t nx, uint32_t ny, int free_surface, void* mass,
+                       void* excess, void* phi, int mass_f64, cudaStream_t st);
+void launch_nbmask(const uint8_t* geo, uint8_t* nbmask, uint32_t nx, uint32_t ny, cudaStream_t st);
+template <class S, class C, class M>
+void launch_init_ddf(const KParams& kp, cudaStream_t st, const uint8_t* geo, bool hw);
+
+// reductions and codecs
+template <class S, class C, class M>
+void launch_mass_partial(const KParams& kp, cudaStream_t st, uint32_t odd, int fs, bool hw, double* partial);
+void launch_sum_partials(const double* partial, uint32_t n, double* out, cudaStream_t st);
+template <class S, class C, class M>
+void launch_census(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, unsigned long long* counts);
+template <class S, class C, class M>
+void launch_decode(const KParams& kp, cudaStream_t st, void* out);
+template <class S, class C, class M>
+void launch_encode(const KParams& kp, cudaStream_t st, const void* in);
+
+}  // namespace flb

@@ -39,7 +39,7 @@ class CaseDesc(C.Structure):
         ("subgrid", C.c_int32), ("use_volumetric_force", C.c_int32), ("tau", C.c_float), ("fx", C.c_float),
         ("fy", C.c_float), ("bounce_back", C.c_int32), ("fs_mode", C.c_int32), ("f16_scale", C.c_float),
         ("device", C.c_int32), ("stream", C.c_void_p), ("inlet_ux", C.c_double), ("inlet_uy", C.c_double),
-        ("kernel_variant", C.c_int32),
+        ("kernel_variant", C.c_int32), ("u_max", C.c_float),
     ]
 
 
@@ -116,7 +116,7 @@ class Solver:
                  use_force: bool = True, collision: int = 0, subgrid: bool = False,
                  bounce_back: int = BB_HALFWAY, fs_mode: int = FS_CONSERVATIVE, inlet_ux: float = 0.0,
                  inlet_uy: float = 0.0, f16_scale: float = 0.0, device: int = -1, stream: int | None = None,
-                 kernel_variant: int = 0):
+                 kernel_variant: int = 0, u_max: float = 0.0):
         L = load_library()
         g = np.ascontiguousarray(flags, dtype=np.uint8)
         if g.ndim != 2:
@@ -134,6 +134,7 @@ class Solver:
         d.bounce_back, d.fs_mode, d.f16_scale, d.device = int(bounce_back), int(fs_mode), f16_scale, int(device)
         d.stream = stream or None
         d.kernel_variant = int(kernel_variant)
+        d.u_max = float(u_max)
         self._desc = d
         self.free_surface = bool(free_surface)
         self.precision = precision

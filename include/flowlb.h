@@ -104,6 +104,9 @@ typedef struct flb_case_desc {
   double inlet_ux, inlet_uy;  /* lattice velocity of INLET cells (double, as the reference's LBVelocity) */
   int32_t kernel_variant;     /* stream-collide data path: 0 auto, 1 one cell per thread, 2 vector
                                  (V cells per thread; needs nx % V == 0, V = 4 for FP32/FP16S, 2 for FP64) */
+  float u_max;                /* velocity limiter, lattice units (0 = off, the reference behaviour): the
+                                 force-shifted velocity used for feq and forcing is scaled down to |u| = u_max;
+                                 keeps high-Mach free-surface fronts stable; mass is still conserved */
 } flb_case_desc;
 
 typedef struct flb_engine* flb_handle;

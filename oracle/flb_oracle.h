@@ -71,6 +71,7 @@ typedef struct {
   float f16_scale;       /* power-of-two scale S of the F16S storage */
   int32_t threads;       /* OpenMP threads (<=0: default) */
   double inlet_ux, inlet_uy; /* inlet velocity, lattice units (double, as LBVelocity) */
+  float u_max;           /* velocity limiter (0: off), see flb_case_desc.u_max */
 } orc_params;
 
 typedef struct orc_state orc_state;

@@ -35,7 +35,7 @@ class OrcParams(C.Structure):
         ("use_force", C.c_int32), ("fs_count_pre", C.c_int32), ("fs1_post", C.c_int32), ("tau", C.c_float),
         ("fx", C.c_float),
         ("fy", C.c_float), ("f16_scale", C.c_float), ("threads", C.c_int32), ("inlet_ux", C.c_double),
-        ("inlet_uy", C.c_double),
+        ("inlet_uy", C.c_double), ("u_max", C.c_float),
     ]
 
 
@@ -100,6 +100,7 @@ class OracleConfig:
     inlet_uy: float = 0.0
     f16_scale: float = 4096.0
     threads: int = 0
+    u_max: float = 0.0
 
 
 class Oracle:
@@ -114,7 +115,7 @@ class Oracle:
         p = OrcParams(self.nx, self.ny, cfg.variant, int(cfg.free_surface), cfg.bb, cfg.fs_mode, cfg.collision,
                       int(cfg.subgrid), int(cfg.use_force), int(cfg.fs_count_pre), int(cfg.fs1_post), cfg.tau,
                       cfg.fx, cfg.fy,
-                      cfg.f16_scale, cfg.threads, cfg.inlet_ux, cfg.inlet_uy)
+                      cfg.f16_scale, cfg.threads, cfg.inlet_ux, cfg.inlet_uy, cfg.u_max)
         self._h = lib().orc_create(C.byref(p), g.ctypes.data)
         if not self._h:
             raise ValueError("orc_create rejected the case")
