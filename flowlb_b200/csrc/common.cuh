@@ -43,6 +43,7 @@ struct KParams {
   const void* rho_snap;
   const void* u_snap;
   float inv_tau, fx, fy;
+  float cF[9];  // cx[i]*Fx + cy[i]*Fy, computed on the host in float as the reference does per cell
   float f16_scale, f16_inv;
   double inlet_ux, inlet_uy;
   int use_force, subgrid, collision, fs_cons;

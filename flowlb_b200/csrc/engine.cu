@@ -414,6 +414,17 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
   k.inlet_uy = desc->inlet_uy;
   k.fs_cons = desc->fs_mode == FLB_FS_CONSERVATIVE ? 1 : 0;
   k.u_max = desc->u_max > 0.0f ? desc->u_max : 0.0f;
+  {
+    // cx[i]*Fx + cy[i]*Fy in float, the same IEEE operations the reference
+    // kernel evaluates per cell (cellCalculations.cuh:71); volatile keeps the
+    // host compiler from contracting or folding them
+    const int cxs[9] = {0, 1, -1, 0, 0, 1, -1, 1, -1}, cys[9] = {0, 0, 0, 1, -1, 1, -1, -1, 1};
+    for (int i = 0; i < 9; i++) {
+      volatile float a = (float)cxs[i] * k.fx;
+      volatile float b = (float)cys[i] * k.fy;
+      k.cF[i] = a + b;
+    }
+  }
   cudaError_t e = cudaMemcpyAsync(h->d_geo, desc->flags, N, cudaMemcpyHostToDevice, h->stream);
   if (e != cudaSuccess) return bail(cuda_fail(h, e, "cudaMemcpyAsync"));
   s = initialise(h);

@@ -19,6 +19,14 @@
 // flag load instead of after it.
 #include "launch.h"
 
+// occupancy targets (resident blocks per SM) of the two data paths
+#ifndef FLB_SC_MIN_BLOCKS
+#define FLB_SC_MIN_BLOCKS 1
+#endif
+#ifndef FLB_VEC_MIN_BLOCKS
+#define FLB_VEC_MIN_BLOCKS 1
+#endif
+
 namespace flb {
 
 // Everything between the load and the store of d_StreamCollide2D for one
@@ -27,12 +35,20 @@ namespace flb {
 // write-back, equilibrium, Smagorinsky, SRT/TRT.  f: incoming -> post.
 template <class C, class M, bool FS, bool WM>
 __device__ __forceinline__ void collide_cell(const KParams& p, uint32_t idx, uint32_t x, uint32_t y, uint8_t flag,
-                                             C* f) {
+                                             uint32_t nbm, C* f) {
   const uint32_t N = p.N;
   if constexpr (FS) {
-    // reference mode: FS_1 left the populations it rebuilt toward gas here
+    // reference mode: FS_1 left the populations it rebuilt toward gas here.
+    // FS_1 wrote them to their regular slots; where a half-way wall reflects
+    // the population instead (its source is a wall), that slot is not read.
     if (!p.fs_cons && (flag & (kFGI | kInlet)) == kInterface) {
-      const uint32_t m = p.recon_mask[idx];
+      uint32_t wallsrc = 0;  // bit k: the source of incoming population k+1 is a wall
+#pragma unroll
+      for (int i = 1; i < 9; i += 2) {
+        wallsrc |= ((nbm >> i) & 1u) << (i - 1);        // f_i comes from neighbour i+1
+        wallsrc |= ((nbm >> (i - 1)) & 1u) << i;        // f_{i+1} comes from neighbour i
+      }
+      const uint32_t m = p.recon_mask[idx] & ~wallsrc;
       if (m) {
         const C* rec = static_cast<const C*>(p.recon);
 #pragma unroll
@@ -85,7 +101,7 @@ __device__ __forceinline__ void collide_cell(const KParams& p, uint32_t idx, uin
     uy = uy + rhol2 * p.fy;
   }
   limit_u(p.u_max, ux, uy);
-  if (use_force) forcing(Fi, ux, uy, p.fx, p.fy);
+  if (use_force) forcing(Fi, ux, uy, p.fx, p.fy, p.cF);
   if (FS || WM) {
     C* R = static_cast<C*>(p.rho);
     C* U = static_cast<C*>(p.u);
@@ -150,7 +166,7 @@ __device__ __forceinline__ void collide_cell(const KParams& p, uint32_t idx, uin
 
 // ---- one cell per thread -----------------------------------------------------
 template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD>
-__global__ void __launch_bounds__(kBlock) k_sc_scalar(const __grid_constant__ KParams p) {
+__global__ void __launch_bounds__(kBlock, FLB_SC_MIN_BLOCKS) k_sc_scalar(const __grid_constant__ KParams p) {
   const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t y = blockIdx.y;
   if (x >= p.nx) return;
@@ -172,7 +188,7 @@ __global__ void __launch_bounds__(kBlock) k_sc_scalar(const __grid_constant__ KP
     if (HW) nbm = p.nbmask[idx];
     load_in<S, C, HW, ODD>(p, idx, nb, nbm, f);
   }
-  collide_cell<C, M, FS, WM>(p, idx, x, y, flag, f);
+  collide_cell<C, M, FS, WM>(p, idx, x, y, flag, nbm, f);
   store_post<S, C, ODD>(p, idx, nb, f);
 }
 
@@ -234,7 +250,7 @@ __device__ __forceinline__ void load_bytes(const uint8_t* ptr, uint8_t (&f)[V]) 
 constexpr int kVecBlock = 256;
 
 template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD>
-__global__ void __launch_bounds__(kVecBlock) k_sc_vec(const __grid_constant__ KParams p) {
+__global__ void __launch_bounds__(kVecBlock, FLB_VEC_MIN_BLOCKS) k_sc_vec(const __grid_constant__ KParams p) {
   constexpr int V = Lanes<S>::V;
   using K = Codec<S, C>;
   const uint32_t nx = p.nx, ny = p.ny;
@@ -331,7 +347,7 @@ __global__ void __launch_bounds__(kVecBlock) k_sc_vec(const __grid_constant__ KP
         if ((nbm >> (i - 1)) & 1u) f[i + 1] = K::ld(slotp<S>(p, slot_a<ODD>(i)), nb[i], i + 1, p.f16_inv);
       }
     }
-    collide_cell<C, M, FS, WM>(p, idx, x, y, fl[k], f);
+    collide_cell<C, M, FS, WM>(p, idx, x, y, fl[k], nbm, f);
     K::st(raw0, k, 0, f[0], p.f16_scale);
 #pragma unroll
     for (int q = 0; q < 4; q++) {

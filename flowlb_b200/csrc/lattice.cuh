@@ -99,14 +99,15 @@ __device__ __forceinline__ void equilibrium(C rho, C ux, C uy, C* feq) {
   feq[8] = rhow58 * (1.0f - u0 - 0.5f * u2 + 0.5f * u0 * u0);
 }
 
-// calculateForcingTerms2D (Guo), cellCalculations.cuh:64-73
+// calculateForcingTerms2D (Guo), cellCalculations.cuh:64-73.  cF[i] is the
+// cell-independent factor cx[i]*Fx + cy[i]*Fy, evaluated once in float with
+// the same operations (see flb_create).
 template <class C>
-__device__ __forceinline__ void forcing(C* Fi, C ux, C uy, float Fx, float Fy) {
+__device__ __forceinline__ void forcing(C* Fi, C ux, C uy, float Fx, float Fy, const float* cF) {
   const C uF = -0.33333334f * (ux * Fx + uy * Fy);
   Fi[0] = 9.0f * wgt<C>(0) * uF;
 #pragma unroll
-  for (int i = 1; i < 9; i++)
-    Fi[i] = 9.0f * wgt<C>(i) * ((cx(i) * Fx + cy(i) * Fy) * (cx(i) * ux + cy(i) * uy + 0.33333334f) + uF);
+  for (int i = 1; i < 9; i++) Fi[i] = 9.0f * wgt<C>(i) * (cF[i] * (cx(i) * ux + cy(i) * uy + 0.33333334f) + uF);
 }
 
 // calculatePhi, cellCalculations.cuh:153-158: the quotient is clamped in

@@ -14,7 +14,7 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libflowlb.so")
+LIB_PATH = os.environ.get("FLOWLB_LIB", os.path.join(HERE, "libflowlb.so"))
 
 FIELD_F, FIELD_RHO, FIELD_U, FIELD_FLAGS, FIELD_MASS, FIELD_EXCESS, FIELD_PHI = range(7)
 BB_IMPLICIT, BB_HALFWAY = 0, 1
