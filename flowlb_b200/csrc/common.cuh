@@ -53,6 +53,11 @@ struct KParams {
   float u_max;  // velocity limiter, 0 = off
 };
 
+__device__ __forceinline__ bool same_bits(double a, double b) {
+  return __double_as_longlong(a) == __double_as_longlong(b);
+}
+__device__ __forceinline__ bool same_bits(float a, float b) { return __float_as_uint(a) == __float_as_uint(b); }
+
 template <class S>
 __device__ __forceinline__ S* slotp(const KParams& p, int s) {
   return static_cast<S*>(p.slot[s]);

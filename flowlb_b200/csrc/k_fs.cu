@@ -216,13 +216,14 @@ __global__ void __launch_bounds__(kTX* kTY) k_fs234(const __grid_constant__ KPar
   const uint8_t fin = s3[ly][lx];
   // Write skipping.  flags_out still holds this cell's flag after the previous
   // step's stream-collide ("old").  When the buffers come from consecutive
-  // full steps (trust_prev), a value already in memory is not rewritten:
+  // full steps (trust_prev), values already in memory are not rewritten:
   //  * the flag, when old equals the new flag;
-  //  * all mass fields of a cell that was gas in the previous step and stays
-  //    gas: that step (or the initial state) left m = excess = phi = +0, and
-  //    FS_1 does not touch gas cells, so FS_4 would write the same zeros;
-  //  * the fill level of a cell that was fluid after the previous step and
-  //    stays fluid: it is already 1.
+  //  * the fill level of a cell that is fluid (gas) both before and after this
+  //    pass: it was fluid (gas) after the previous step too, whose FS_4 left
+  //    phi = 1 (0);
+  //  * mass and excess of a gas cell when they do not change (deep gas holds
+  //    zeros; a gas cell with no fluid or interface neighbour keeps its mass,
+  //    lbmKernel2D.cu:296, so nothing else is assumed about them).
   const bool trust = p.trust_prev != 0;
   const uint8_t old = p.flags_out[idx];
   if (!trust || old != fin) p.flags_out[idx] = fin;
@@ -259,11 +260,14 @@ __global__ void __launch_bounds__(kTX* kTY) k_fs234(const __grid_constant__ KPar
   // FS_4 fields
   if (f3 & (kWall | kMovingWall | kInlet)) return;
   const uint8_t sw4 = f3 & (kFGI | kGasInterface);
-  if (trust && sw4 == kGas && (old & (kFGI | kGasInterface)) == kGas) return;
-  const bool keep_phi = trust && sw4 == kFluid && (s0[ly][lx] & (kFGI | kGasInterface)) == kFluid;
+  const uint8_t sw0 = s0[ly][lx] & (kFGI | kGasInterface);
+  const bool gas_stays = trust && sw4 == kGas && sw0 == kGas;
+  const bool keep_phi = gas_stays || (trust && sw4 == kFluid && sw0 == kFluid);
   M* Ms = static_cast<M*>(p.mass);
-  const C rho = R[idx];
-  M m = Ms[idx];
+  M* Exs = static_cast<M*>(p.excess);
+  const C rho = sw4 == kGas ? C(0) : R[idx];  // the gas case does not use the density
+  const M m_old = Ms[idx];
+  M m = m_old;
   M ex = 0.0f, ph = 0.0f;
   switch (f3 & (kFGI | kGasInterface)) {
     case 1:
@@ -312,8 +316,13 @@ __global__ void __launch_bounds__(kTX* kTY) k_fs234(const __grid_constant__ KPar
     }
   m += cont > 0 ? 0.0f : ex;
   ex = cont > 0 ? ex / (float)cont : 0.0f;
-  Ms[idx] = m;
-  static_cast<M*>(p.excess)[idx] = ex;
+  if (gas_stays) {
+    if (!same_bits(m, m_old)) Ms[idx] = m;
+    if (!same_bits(ex, Exs[idx])) Exs[idx] = ex;
+  } else {
+    Ms[idx] = m;
+    Exs[idx] = ex;
+  }
   if (!keep_phi) static_cast<M*>(p.phi)[idx] = ph;
 }
 
