@@ -58,6 +58,24 @@ __device__ __forceinline__ bool same_bits(double a, double b) {
 }
 __device__ __forceinline__ bool same_bits(float a, float b) { return __float_as_uint(a) == __float_as_uint(b); }
 
+// Free-surface steps work on super-tiles of kSTW x kSTH cells.  Only the
+// super-tiles a pass can change are visited: the flag pass records which
+// super-tiles hold fluid or interface cells, a small kernel compacts them into
+// lists (k_build_lists), and the next step's passes loop over the lists in a
+// persistent grid.  all = 1 visits every super-tile (first step after the
+// state was set from outside).
+constexpr uint32_t kSTW = 128, kSTH = 8;
+
+struct TileList {
+  const uint32_t* list;
+  const uint32_t* count;
+  uint32_t ntiles, nsx;
+  int all;
+};
+
+__device__ __forceinline__ uint32_t tile_count(const TileList& tl) { return tl.all ? tl.ntiles : *tl.count; }
+__device__ __forceinline__ uint32_t tile_at(const TileList& tl, uint32_t i) { return tl.all ? i : tl.list[i]; }
+
 template <class S>
 __device__ __forceinline__ S* slotp(const KParams& p, int s) {
   return static_cast<S*>(p.slot[s]);

@@ -51,6 +51,14 @@ struct flb_engine {
   // the other flag buffer holds the previous step's post-stream-collide flags
   // and the mass fields follow from full steps (enables write skipping)
   bool trust = false;
+  // free surface: super-tile activity bitmaps and the lists of the next step
+  uint32_t nsx = 0, nsy = 0, ntiles = 0;
+  uint32_t* d_nz = nullptr;       // super-tile holds fluid/interface after the last flag pass
+  uint32_t* d_nz_prev = nullptr;  // the same one step earlier
+  uint32_t* d_list[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [step parity][0 FS_1/SC, 1 flag pass]
+  uint32_t* d_lcount = nullptr;   // [step parity][2] list lengths
+  bool lists_valid = false;       // lists of the current parity were built by the previous step
+  uint32_t grid_sc = 0, grid_fs1 = 0, grid_fs234 = 0;
   KParams kp{};
   // device buffers
   void* d_f = nullptr;
@@ -114,8 +122,20 @@ struct Ops {
   static void sc(flb_engine* h, uint32_t odd, bool wm) {
     launch_sc<S, C, M>(h->kp, h->stream, odd, h->fs, h->hw, wm, h->use_vec);
   }
-  static void fs1(flb_engine* h, uint32_t odd) { launch_fs1<S, C, M>(h->kp, h->stream, odd, h->hw); }
-  static void fs234(flb_engine* h, uint32_t odd) { launch_fs234<S, C, M>(h->kp, h->stream, odd); }
+  static void sc_list(flb_engine* h, uint32_t odd, const TileList& tl) {
+    launch_sc_list<S, C, M>(h->kp, h->stream, odd, h->hw, tl, h->grid_sc);
+  }
+  static void fs1(flb_engine* h, uint32_t odd, const TileList& tl) {
+    launch_fs1<S, C, M>(h->kp, h->stream, odd, h->hw, tl, h->grid_fs1);
+  }
+  static void fs234(flb_engine* h, uint32_t odd, const TileList& tl) {
+    launch_fs234<S, C, M>(h->kp, h->stream, odd, tl, h->grid_fs234, h->d_nz);
+  }
+  static void grids(flb_engine* h, int nsm) {
+    h->grid_sc = (uint32_t)(nsm * sc_list_blocks_per_sm<S, C, M>());
+    h->grid_fs1 = (uint32_t)(nsm * fs_blocks_per_sm<S, C, M>(0));
+    h->grid_fs234 = (uint32_t)(nsm * fs_blocks_per_sm<S, C, M>(1));
+  }
   static void apply_recon(flb_engine* h, uint32_t odd) { launch_apply_recon<S, C, M>(h->kp, h->stream, odd); }
   static void init_ddf(flb_engine* h) { launch_init_ddf<S, C, M>(h->kp, h->stream, h->d_geo, h->hw); }
   static void mass_partial(flb_engine* h, uint32_t odd) {
@@ -159,6 +179,30 @@ void refresh_params(flb_engine* h) {
   k.u_snap = h->d_u_snap;
 }
 
+// Super-tile lists consumed by the step at t (built by the step before) and the
+// buffers the step fills for t+1.  Without valid lists every super-tile is visited.
+struct FsLists {
+  TileList sc, fs;
+  uint32_t* next_count;
+  bool all;
+};
+
+FsLists fs_lists(flb_engine* h, uint64_t t) {
+  const int lp = (int)(t & 1u);
+  FsLists L;
+  L.all = !h->lists_valid;
+  L.sc = TileList{h->d_list[lp][0], h->d_lcount + 2 * lp, h->ntiles, h->nsx, L.all ? 1 : 0};
+  L.fs = TileList{h->d_list[lp][1], h->d_lcount + 2 * lp + 1, h->ntiles, h->nsx, L.all ? 1 : 0};
+  L.next_count = h->d_lcount + 2 * (lp ^ 1);
+  return L;
+}
+
+void build_lists(flb_engine* h, uint64_t t, const FsLists& L) {
+  const int np = (int)((t + 1) & 1u);
+  launch_build_lists(h->d_nz, h->d_nz_prev, h->nsx, h->nsy, L.all ? 1 : 0, h->d_list[np][0], h->d_list[np][1],
+                     L.next_count, h->stream);
+}
+
 // Issues the passes of one time step at t on the stream.
 uint64_t issue_step(flb_engine* h, uint64_t t, bool write_macro) {
   const uint32_t odd = (uint32_t)(t & 1u);
@@ -170,14 +214,18 @@ uint64_t issue_step(flb_engine* h, uint64_t t, bool write_macro) {
   }
   if (h->fs) {
     h->kp.trust_prev = h->trust ? 1 : 0;
+    const FsLists L = fs_lists(h, t);
+    cudaMemsetAsync(L.next_count, 0, 2 * sizeof(uint32_t), h->stream);
     dispatch(h, [&](auto ops) {
-      ops.fs1(h, odd);
-      ops.sc(h, odd, true);
-      ops.fs234(h, odd);
+      ops.fs1(h, odd, L.sc);
+      ops.sc_list(h, odd, L.sc);
+      ops.fs234(h, odd, L.fs);
     });
-    k = 3;
+    build_lists(h, t, L);
+    k = 4;
     h->cur ^= 1;
     h->trust = true;
+    h->lists_valid = true;
     refresh_params(h);
   } else {
     dispatch(h, [&](auto ops) { ops.sc(h, odd, write_macro || h->has_io); });
@@ -219,9 +267,11 @@ flb_status capture(flb_engine* h, GraphSlot& g, int pairs) {
 void free_all(flb_engine* h) {
   destroy_graph(h->g_pair);
   destroy_graph(h->g_big);
-  void* bufs[] = {h->d_f,      h->d_rho,    h->d_u,          h->d_flags[0],  h->d_flags[1], h->d_geo,
-                  h->d_nbmask, h->d_mass,   h->d_excess,     h->d_phi,       h->d_recon,    h->d_recon_mask,
-                  h->d_rho_snap, h->d_u_snap, h->d_partial,  h->d_scalar,    h->d_counts};
+  void* bufs[] = {h->d_f,          h->d_rho,         h->d_u,           h->d_flags[0],    h->d_flags[1],
+                  h->d_geo,        h->d_nbmask,      h->d_mass,        h->d_excess,      h->d_phi,
+                  h->d_recon,      h->d_recon_mask,  h->d_rho_snap,    h->d_u_snap,      h->d_partial,
+                  h->d_scalar,     h->d_counts,      h->d_nz,          h->d_nz_prev,     h->d_list[0][0],
+                  h->d_list[0][1], h->d_list[1][0],  h->d_list[1][1],  h->d_lcount};
   for (void* p : bufs)
     if (p) cudaFree(p);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -288,6 +338,7 @@ flb_status initialise(flb_engine* h) {
   if (h->fs) FLB_CUDA(h, cudaMemcpyAsync(h->d_flags[1], h->d_flags[0], h->N, cudaMemcpyDeviceToDevice, h->stream));
   if (h->d_recon_mask) FLB_CUDA(h, cudaMemsetAsync(h->d_recon_mask, 0, h->N, h->stream));
   h->trust = true;  // flags[1] = flags[0] and the initial fields satisfy the skip invariants
+  h->lists_valid = false;
   FLB_CUDA(h, cudaGetLastError());
   return FLB_OK;
 }
@@ -351,7 +402,10 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
   }
   {
     const uint32_t V = (uint32_t)vec_width(desc->precision);
-    h->use_vec = desc->kernel_variant == 2 || (desc->kernel_variant == 0 && desc->nx % V == 0);
+    // measured on a B200: one cell per thread is faster for FP32/FP64 (it runs
+    // at full occupancy), the vector path for FP16S (fewer instructions)
+    h->use_vec = desc->kernel_variant == 2 ||
+                 (desc->kernel_variant == 0 && desc->precision == 16 && desc->nx % V == 0);
   }
   s = check_io(h, desc->flags);
   if (s != FLB_OK) {
@@ -375,6 +429,10 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
   const uint64_t N = h->N;
   struct Alloc { void** p; size_t bytes; bool need; };
   const uint64_t blocks = (N + kBlock - 1) / kBlock;
+  h->nsx = (h->nx + kSTW - 1) / kSTW;
+  h->nsy = (h->ny + kSTH - 1) / kSTH;
+  h->ntiles = h->nsx * h->nsy;
+  const uint64_t tiles = h->ntiles;
   Alloc allocs[] = {
       {&h->d_f, 9 * N * h->s_size, true},
       {&h->d_rho, N * h->c_size, true},
@@ -393,11 +451,23 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
       {(void**)&h->d_partial, blocks * sizeof(double), true},
       {(void**)&h->d_scalar, sizeof(double), true},
       {(void**)&h->d_counts, 8 * sizeof(unsigned long long), true},
+      {(void**)&h->d_nz, tiles * sizeof(uint32_t), h->fs},
+      {(void**)&h->d_nz_prev, tiles * sizeof(uint32_t), h->fs},
+      {(void**)&h->d_list[0][0], tiles * sizeof(uint32_t), h->fs},
+      {(void**)&h->d_list[0][1], tiles * sizeof(uint32_t), h->fs},
+      {(void**)&h->d_list[1][0], tiles * sizeof(uint32_t), h->fs},
+      {(void**)&h->d_list[1][1], tiles * sizeof(uint32_t), h->fs},
+      {(void**)&h->d_lcount, 4 * sizeof(uint32_t), h->fs},
   };
   for (Alloc& a : allocs) {
     if (!a.need) continue;
     cudaError_t e = cudaMalloc(a.p, a.bytes);
     if (e != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc"));
+  }
+  if (h->fs) {
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
+    dispatch(h, [&](auto ops) { ops.grids(h, nsm > 0 ? nsm : 1); });
   }
   KParams& k = h->kp;
   std::memset(&k, 0, sizeof(k));
@@ -475,7 +545,7 @@ FLB_API flb_status flb_step(flb_handle h, uint64_t n) {
     // graphs cover pairs of steps from an even t; the last step of the call
     // runs on its own so that it writes density and velocity
     const uint64_t big = 2ull * kGraphPairs;
-    if (h->fs && !h->trust) {
+    if (h->fs && (!h->trust || !h->lists_valid)) {
       // first step after the state was written from outside: no write skipping
       h->launches += issue_step(h, h->t, remaining == 1);
       h->t += 1;
@@ -625,6 +695,7 @@ FLB_API flb_status flb_write_field(flb_handle h, int field, const void* src, int
     FLB_CUDA(h, cudaMemcpyAsync(dst, src, bytes, kind, h->stream));
   }
   h->trust = false;
+  h->lists_valid = false;
   FLB_CUDA(h, cudaStreamSynchronize(h->stream));
   return FLB_OK;
 }
@@ -689,14 +760,21 @@ FLB_API flb_status flb_run_pass(flb_handle h, int pass) {
   }
   const bool recon = h->fs && h->d_recon_mask;
   h->trust = false;
+  h->lists_valid = false;
   h->kp.trust_prev = 0;
+  const TileList all{nullptr, nullptr, h->ntiles, h->nsx, 1};
   // alone, stream-collide sees no parked populations, and FS_1 writes its
   // rebuilt populations into the population array like the reference kernel
   if (pass == 0 && recon) FLB_CUDA(h, cudaMemsetAsync(h->d_recon_mask, 0, h->N, h->stream));
   dispatch(h, [&](auto ops) {
-    if (pass == 0) ops.sc(h, odd, true);
-    else if (pass == 1) ops.fs1(h, odd);
-    else ops.fs234(h, odd);
+    if (pass == 0) {
+      if (h->fs) ops.sc_list(h, odd, all);
+      else ops.sc(h, odd, true);
+    } else if (pass == 1) {
+      ops.fs1(h, odd, all);
+    } else {
+      ops.fs234(h, odd, all);
+    }
     if (pass == 1 && recon) ops.apply_recon(h, odd);
   });
   h->launches += (pass == 1 && recon) ? 2 : 1;
@@ -725,15 +803,20 @@ FLB_API flb_status flb_profile_steps(flb_handle h, uint64_t n, double pass_ms[3]
     cudaEventRecord(ev[0], h->stream);
     if (h->fs) {
       h->kp.trust_prev = h->trust ? 1 : 0;
-      dispatch(h, [&](auto ops) { ops.fs1(h, odd); });
+      const FsLists L = fs_lists(h, h->t);
+      cudaMemsetAsync(L.next_count, 0, 2 * sizeof(uint32_t), h->stream);
+      cudaEventRecord(ev[0], h->stream);
+      dispatch(h, [&](auto ops) { ops.fs1(h, odd, L.sc); });
       cudaEventRecord(ev[1], h->stream);
-      dispatch(h, [&](auto ops) { ops.sc(h, odd, true); });
+      dispatch(h, [&](auto ops) { ops.sc_list(h, odd, L.sc); });
       cudaEventRecord(ev[2], h->stream);
-      dispatch(h, [&](auto ops) { ops.fs234(h, odd); });
+      dispatch(h, [&](auto ops) { ops.fs234(h, odd, L.fs); });
+      build_lists(h, h->t, L);
       cudaEventRecord(ev[3], h->stream);
-      h->launches += 3;
+      h->launches += 4;
       h->cur ^= 1;
       h->trust = true;
+      h->lists_valid = true;
     } else {
       cudaEventRecord(ev[1], h->stream);
       dispatch(h, [&](auto ops) { ops.sc(h, odd, k + 1 == n || h->has_io); });
@@ -861,6 +944,7 @@ FLB_API flb_status flb_load_checkpoint(flb_handle h, const char* path) {
   h->t = hd.t;
   h->cur = cur;
   h->trust = false;
+  h->lists_valid = false;
   refresh_params(h);
   return FLB_OK;
 }

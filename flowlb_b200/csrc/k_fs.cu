@@ -7,10 +7,7 @@ namespace flb {
 
 // ---- FS_1: mass exchange and gas reconstruction, lbmKernel2D.cu:14-121 -----
 template <class S, class C, class M, bool HW, bool ODD>
-__global__ void __launch_bounds__(kBlock) k_fs1(const __grid_constant__ KParams p) {
-  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t y = blockIdx.y;
-  if (x >= p.nx) return;
+__device__ __forceinline__ void fs1_cell(const KParams& p, uint32_t x, uint32_t y) {
   const uint32_t nx = p.nx, N = p.N;
   const uint32_t idx = x + y * nx;
   const uint8_t* flags = p.flags;
@@ -109,6 +106,22 @@ __global__ void __launch_bounds__(kBlock) k_fs1(const __grid_constant__ KParams 
   Ms[idx] = m;
 }
 
+// The listed super-tiles, one row of a super-tile per warp.
+template <class S, class C, class M, bool HW, bool ODD>
+__global__ void __launch_bounds__(kBlock) k_fs1(const __grid_constant__ KParams p, const TileList tl) {
+  const uint32_t n = tile_count(tl);
+  const uint32_t lane = threadIdx.x & 31u, row = threadIdx.x >> 5;
+  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+    const uint32_t t = tile_at(tl, i);
+    const uint32_t y = (t / tl.nsx) * kSTH + row;
+    if (y >= p.ny) continue;
+    const uint32_t xb = (t % tl.nsx) * kSTW + lane;
+#pragma unroll 1
+    for (uint32_t j = 0; j < kSTW; j += 32)
+      if (xb + j < p.nx) fs1_cell<S, C, M, HW, ODD>(p, xb + j, y);
+  }
+}
+
 // Writes the populations FS_1 parked in recon (reference mode) into their
 // incoming slots, as the reference FS_1 kernel does itself.  Only the
 // isolated-pass path uses it; a full step hands them to stream-collide.
@@ -147,15 +160,24 @@ __device__ __forceinline__ int wrapi(int v, int n) {
   return v < 0 ? v + n : v;
 }
 
+struct FlagTiles {
+  uint8_t s0[kSY][kSX];  // after stream-collide
+  uint8_t s1[kSY][kSX];  // after FS_2
+  uint8_t s2[kSY][kSX];  // after FS_3
+  uint8_t s3[kSY][kSX];  // after FS_4 conversion
+};
+
+// One 32x8 tile (tile coordinates tx, ty) with the 256 threads of the block;
+// every thread of the block must call it.  Returns whether this thread's cell
+// is fluid or interface after the pass.
 template <class S, class C, class M, bool ODD>
-__global__ void __launch_bounds__(kTX* kTY) k_fs234(const __grid_constant__ KParams p) {
-  __shared__ uint8_t s0[kSY][kSX];  // after stream-collide
-  __shared__ uint8_t s1[kSY][kSX];  // after FS_2
-  __shared__ uint8_t s2[kSY][kSX];  // after FS_3
-  __shared__ uint8_t s3[kSY][kSX];  // after FS_4 conversion
+__device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int tid, FlagTiles& sm) {
+  auto& s0 = sm.s0;
+  auto& s1 = sm.s1;
+  auto& s2 = sm.s2;
+  auto& s3 = sm.s3;
   const int nx = (int)p.nx, ny = (int)p.ny;
-  const int x0 = (int)blockIdx.x * kTX - kHalo, y0 = (int)blockIdx.y * kTY - kHalo;
-  const int tid = threadIdx.x + threadIdx.y * kTX;
+  const int x0 = tx * kTX - kHalo, y0 = ty * kTY - kHalo;
   const uint8_t* flags = p.flags;
   for (int k = tid; k < kSX * kSY; k += kTX * kTY) {
     const int lx = k % kSX, ly = k / kSX;
@@ -207,13 +229,14 @@ __global__ void __launch_bounds__(kTX* kTY) k_fs234(const __grid_constant__ KPar
     s3[ly][lx] = g;
   }
   __syncthreads();
-  const int lx = threadIdx.x + kHalo, ly = threadIdx.y + kHalo;
-  const int gx = (int)blockIdx.x * kTX + (int)threadIdx.x, gy = (int)blockIdx.y * kTY + (int)threadIdx.y;
-  if (gx >= nx || gy >= ny) return;
+  const int lx = tid % kTX + kHalo, ly = tid / kTX + kHalo;
+  const int gx = tx * kTX + tid % kTX, gy = ty * kTY + tid / kTX;
+  if (gx >= nx || gy >= ny) return false;
   const uint32_t N = p.N, idx = (uint32_t)gx + (uint32_t)gy * (uint32_t)nx;
   const uint8_t f1 = s1[ly][lx];
   const uint8_t f3 = s2[ly][lx];
   const uint8_t fin = s3[ly][lx];
+  const bool live = (fin & (kWall | kMovingWall)) == 0 && ((fin & kFGI) == kFluid || (fin & kFGI) == kInterface);
   // Write skipping.  flags_out still holds this cell's flag after the previous
   // step's stream-collide ("old").  When the buffers come from consecutive
   // full steps (trust_prev), values already in memory are not rewritten:
@@ -258,7 +281,7 @@ __global__ void __launch_bounds__(kTX* kTY) k_fs234(const __grid_constant__ KPar
     store_post<S, C, ODD>(p, idx, nb, feq);
   }
   // FS_4 fields
-  if (f3 & (kWall | kMovingWall | kInlet)) return;
+  if (f3 & (kWall | kMovingWall | kInlet)) return live;
   const uint8_t sw4 = f3 & (kFGI | kGasInterface);
   const uint8_t sw0 = s0[ly][lx] & (kFGI | kGasInterface);
   const bool gas_stays = trust && sw4 == kGas && sw0 == kGas;
@@ -324,19 +347,83 @@ __global__ void __launch_bounds__(kTX* kTY) k_fs234(const __grid_constant__ KPar
     Exs[idx] = ex;
   }
   if (!keep_phi) static_cast<M*>(p.phi)[idx] = ph;
+  return live;
+}
+
+// The listed super-tiles: each block runs the tile pass on the 4 tiles of a
+// super-tile and records in nz whether the super-tile holds fluid or
+// interface cells afterwards.
+template <class S, class C, class M, bool ODD>
+__global__ void __launch_bounds__(kTX* kTY) k_fs234(const __grid_constant__ KParams p, const TileList tl,
+                                                    uint32_t* __restrict__ nz) {
+  __shared__ FlagTiles sm;
+  const int tid = threadIdx.x;
+  const uint32_t n = tile_count(tl);
+  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+    const uint32_t t = tile_at(tl, i);
+    const int sx = (int)(t % tl.nsx), sy = (int)(t / tl.nsx);
+    bool live = false;
+#pragma unroll 1
+    for (int j = 0; j < (int)(kSTW / kTX); j++) {
+      const int tx = sx * (int)(kSTW / kTX) + j;
+      if (tx * kTX < (int)p.nx) live |= fs234_tile<S, C, M, ODD>(p, tx, sy, tid, sm);
+      __syncthreads();
+    }
+    live = __syncthreads_or(live);
+    if (tid == 0) nz[t] = live ? 1u : 0u;
+  }
 }
 
 
+// Compacts the super-tiles for the next step: FS_1 and stream-collide visit
+// super-tiles holding fluid or interface cells; the flag pass also visits
+// their neighbours (its stencil chain reaches 3 cells, less than a
+// super-tile) and, once more, super-tiles that held such cells a step earlier
+// (their converted gas cells still clear excess mass and the flag buffers
+// re-synchronise).  Appends with one atomic per warp; list order does not
+// affect results.
+__global__ void k_build_lists(const uint32_t* __restrict__ nz, uint32_t* __restrict__ nz_prev, uint32_t nsx,
+                              uint32_t nsy, int prev_unknown, uint32_t* __restrict__ list_sc,
+                              uint32_t* __restrict__ list_fs, uint32_t* __restrict__ counts) {
+  const uint32_t T = nsx * nsy;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  bool sc = false, fs = false;
+  if (t < T) {
+    const uint32_t sx = t % nsx, sy = t / nsx;
+    const uint32_t own = nz[t];
+    uint32_t near = 0;
+    for (int dy = -1; dy <= 1; dy++)
+      for (int dx = -1; dx <= 1; dx++) {
+        const uint32_t xx = (sx + nsx + dx) % nsx, yy = (sy + nsy + dy) % nsy;
+        near |= nz[xx + yy * nsx];
+      }
+    sc = own != 0;
+    fs = near != 0 || prev_unknown || nz_prev[t] != 0;
+    nz_prev[t] = own;
+  }
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t bsc = __ballot_sync(0xffffffffu, sc), bfs = __ballot_sync(0xffffffffu, fs);
+  uint32_t base_sc = 0, base_fs = 0;
+  if (lane == 0) {
+    if (bsc) base_sc = atomicAdd(&counts[0], (uint32_t)__popc(bsc));
+    if (bfs) base_fs = atomicAdd(&counts[1], (uint32_t)__popc(bfs));
+  }
+  base_sc = __shfl_sync(0xffffffffu, base_sc, 0);
+  base_fs = __shfl_sync(0xffffffffu, base_fs, 0);
+  const uint32_t below = (1u << lane) - 1u;
+  if (sc) list_sc[base_sc + __popc(bsc & below)] = t;
+  if (fs) list_fs[base_fs + __popc(bfs & below)] = t;
+}
+
 // ---- launchers -------------------------------------------------------------------
 template <class S, class C, class M>
-void launch_fs1(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw) {
-  const dim3 g((kp.nx + kBlock - 1) / kBlock, kp.ny);
+void launch_fs1(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl, uint32_t grid) {
   if (hw) {
-    if (odd) k_fs1<S, C, M, true, true><<<g, kBlock, 0, st>>>(kp);
-    else k_fs1<S, C, M, true, false><<<g, kBlock, 0, st>>>(kp);
+    if (odd) k_fs1<S, C, M, true, true><<<grid, kBlock, 0, st>>>(kp, tl);
+    else k_fs1<S, C, M, true, false><<<grid, kBlock, 0, st>>>(kp, tl);
   } else {
-    if (odd) k_fs1<S, C, M, false, true><<<g, kBlock, 0, st>>>(kp);
-    else k_fs1<S, C, M, false, false><<<g, kBlock, 0, st>>>(kp);
+    if (odd) k_fs1<S, C, M, false, true><<<grid, kBlock, 0, st>>>(kp, tl);
+    else k_fs1<S, C, M, false, false><<<grid, kBlock, 0, st>>>(kp, tl);
   }
 }
 
@@ -346,17 +433,31 @@ void launch_apply_recon(const KParams& kp, cudaStream_t st, uint32_t odd) {
 }
 
 template <class S, class C, class M>
-void launch_fs234(const KParams& kp, cudaStream_t st, uint32_t odd) {
-  const dim3 g((kp.nx + kTX - 1) / kTX, (kp.ny + kTY - 1) / kTY);
-  const dim3 b(kTX, kTY);
-  if (odd) k_fs234<S, C, M, true><<<g, b, 0, st>>>(kp);
-  else k_fs234<S, C, M, false><<<g, b, 0, st>>>(kp);
+void launch_fs234(const KParams& kp, cudaStream_t st, uint32_t odd, const TileList& tl, uint32_t grid, uint32_t* nz) {
+  if (odd) k_fs234<S, C, M, true><<<grid, kTX * kTY, 0, st>>>(kp, tl, nz);
+  else k_fs234<S, C, M, false><<<grid, kTX * kTY, 0, st>>>(kp, tl, nz);
 }
 
-#define FLB_INSTANTIATE(S, C, M)                                                      \
-  template void launch_fs1<S, C, M>(const KParams&, cudaStream_t, uint32_t, bool);    \
-  template void launch_apply_recon<S, C, M>(const KParams&, cudaStream_t, uint32_t); \
-  template void launch_fs234<S, C, M>(const KParams&, cudaStream_t, uint32_t);
+template <class S, class C, class M>
+int fs_blocks_per_sm(int which) {
+  int n = 0;
+  if (which == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fs1<S, C, M, true, false>, kBlock, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fs234<S, C, M, false>, kTX * kTY, 0);
+  return n > 0 ? n : 1;
+}
+
+void launch_build_lists(const uint32_t* nz, uint32_t* nz_prev, uint32_t nsx, uint32_t nsy, int prev_unknown,
+                        uint32_t* list_sc, uint32_t* list_fs, uint32_t* counts, cudaStream_t st) {
+  const uint32_t T = nsx * nsy;
+  k_build_lists<<<(T + kBlock - 1) / kBlock, kBlock, 0, st>>>(nz, nz_prev, nsx, nsy, prev_unknown, list_sc, list_fs,
+                                                              counts);
+}
+
+#define FLB_INSTANTIATE(S, C, M)                                                                                  \
+  template void launch_fs1<S, C, M>(const KParams&, cudaStream_t, uint32_t, bool, const TileList&, uint32_t);     \
+  template void launch_apply_recon<S, C, M>(const KParams&, cudaStream_t, uint32_t);                             \
+  template void launch_fs234<S, C, M>(const KParams&, cudaStream_t, uint32_t, const TileList&, uint32_t, uint32_t*); \
+  template int fs_blocks_per_sm<S, C, M>(int);
 FLB_FOR_EACH_VARIANT(FLB_INSTANTIATE)
 #undef FLB_INSTANTIATE
 

@@ -168,10 +168,7 @@ __device__ __forceinline__ void collide_cell(const KParams& p, uint32_t idx, uin
 
 // ---- one cell per thread -----------------------------------------------------
 template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD>
-__global__ void __launch_bounds__(kBlock, FLB_SC_MIN_BLOCKS) k_sc_scalar(const __grid_constant__ KParams p) {
-  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t y = blockIdx.y;
-  if (x >= p.nx) return;
+__device__ __forceinline__ void sc_cell(const KParams& p, uint32_t x, uint32_t y) {
   const uint32_t idx = x + y * p.nx;
   uint32_t nb[9];
   neighbours(x, y, p.nx, p.ny, nb);
@@ -192,6 +189,31 @@ __global__ void __launch_bounds__(kBlock, FLB_SC_MIN_BLOCKS) k_sc_scalar(const _
   }
   collide_cell<C, M, FS, WM>(p, idx, x, y, flag, nbm, f);
   store_post<S, C, ODD>(p, idx, nb, f);
+}
+
+template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD>
+__global__ void __launch_bounds__(kBlock, FLB_SC_MIN_BLOCKS) k_sc_scalar(const __grid_constant__ KParams p) {
+  const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t y = blockIdx.y;
+  if (x >= p.nx) return;
+  sc_cell<S, C, M, FS, HW, WM, ODD>(p, x, y);
+}
+
+// Free surface: the listed super-tiles, one row of a super-tile per warp.
+template <class S, class C, class M, bool HW, bool ODD>
+__global__ void __launch_bounds__(kBlock, FLB_SC_MIN_BLOCKS) k_sc_list(const __grid_constant__ KParams p,
+                                                                       const TileList tl) {
+  const uint32_t n = tile_count(tl);
+  const uint32_t lane = threadIdx.x & 31u, row = threadIdx.x >> 5;
+  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+    const uint32_t t = tile_at(tl, i);
+    const uint32_t y = (t / tl.nsx) * kSTH + row;
+    if (y >= p.ny) continue;
+    const uint32_t xb = (t % tl.nsx) * kSTW + lane;
+#pragma unroll 1
+    for (uint32_t j = 0; j < kSTW; j += 32)
+      if (xb + j < p.nx) sc_cell<S, C, M, true, HW, true, ODD>(p, xb + j, y);
+  }
 }
 
 // ---- V cells per thread ----------------------------------------------------------
@@ -421,8 +443,28 @@ void launch_sc(const KParams& kp, cudaStream_t st, uint32_t odd, bool fs, bool h
 
 int vec_width(int precision) { return precision == 64 ? Lanes<double>::V : Lanes<float>::V; }
 
-#define FLB_INSTANTIATE(S, C, M) \
-  template void launch_sc<S, C, M>(const KParams&, cudaStream_t, uint32_t, bool, bool, bool, bool);
+template <class S, class C, class M>
+void launch_sc_list(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl, uint32_t grid) {
+  if (hw) {
+    if (odd) k_sc_list<S, C, M, true, true><<<grid, kBlock, 0, st>>>(kp, tl);
+    else k_sc_list<S, C, M, true, false><<<grid, kBlock, 0, st>>>(kp, tl);
+  } else {
+    if (odd) k_sc_list<S, C, M, false, true><<<grid, kBlock, 0, st>>>(kp, tl);
+    else k_sc_list<S, C, M, false, false><<<grid, kBlock, 0, st>>>(kp, tl);
+  }
+}
+
+template <class S, class C, class M>
+int sc_list_blocks_per_sm() {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sc_list<S, C, M, true, false>, kBlock, 0);
+  return n > 0 ? n : 1;
+}
+
+#define FLB_INSTANTIATE(S, C, M)                                                                               \
+  template void launch_sc<S, C, M>(const KParams&, cudaStream_t, uint32_t, bool, bool, bool, bool);           \
+  template void launch_sc_list<S, C, M>(const KParams&, cudaStream_t, uint32_t, bool, const TileList&, uint32_t); \
+  template int sc_list_blocks_per_sm<S, C, M>();
 FLB_FOR_EACH_VARIANT(FLB_INSTANTIATE)
 #undef FLB_INSTANTIATE
 

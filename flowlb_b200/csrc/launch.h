@@ -22,14 +22,23 @@ namespace flb {
 template <class S, class C, class M>
 void launch_sc(const KParams& kp, cudaStream_t st, uint32_t odd, bool fs, bool hw, bool wm, bool vec);
 int vec_width(int precision);
-
-// FS_1, its reference-mode apply, and FS_2..4
+// free surface: the listed super-tiles in a persistent grid of `grid` blocks
 template <class S, class C, class M>
-void launch_fs1(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw);
+void launch_sc_list(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl, uint32_t grid);
+template <class S, class C, class M>
+int sc_list_blocks_per_sm();
+
+// FS_1, its reference-mode apply, FS_2..4 (listed super-tiles), and the list build
+template <class S, class C, class M>
+void launch_fs1(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl, uint32_t grid);
 template <class S, class C, class M>
 void launch_apply_recon(const KParams& kp, cudaStream_t st, uint32_t odd);
 template <class S, class C, class M>
-void launch_fs234(const KParams& kp, cudaStream_t st, uint32_t odd);
+void launch_fs234(const KParams& kp, cudaStream_t st, uint32_t odd, const TileList& tl, uint32_t grid, uint32_t* nz);
+template <class S, class C, class M>
+int fs_blocks_per_sm(int which);  // 0: FS_1, 1: FS_2..4
+void launch_build_lists(const uint32_t* nz, uint32_t* nz_prev, uint32_t nsx, uint32_t nsy, int prev_unknown,
+                        uint32_t* list_sc, uint32_t* list_fs, uint32_t* counts, cudaStream_t st);
 
 // initial state
 void launch_init_flags(const uint8_t* geo, uint8_t* flags, uint32_t nx, uint32_t ny, int free_surface, void* mass,
