@@ -27,7 +27,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4
 EXPORTS = [
     "flb_case_desc_init", "flb_create", "flb_reset", "flb_destroy", "flb_step", "flb_sync", "flb_get_time",
     "flb_set_stream", "flb_get_stream", "flb_field_info", "flb_read_field", "flb_write_field", "flb_total_mass",
-    "flb_cell_counts", "flb_check_finite", "flb_run_pass", "flb_profile_steps", "flb_launch_count", "flb_save_checkpoint",
+    "flb_total_mass_noalloc", "flb_cell_counts", "flb_check_finite", "flb_run_pass", "flb_profile_steps", "flb_launch_count", "flb_save_checkpoint",
     "flb_load_checkpoint", "flb_last_error", "flb_status_string", "flb_version",
 ]
 
@@ -76,6 +76,8 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "flb_read_field": (C.c_int, [H, C.c_int, C.c_void_p, C.c_int]),
         "flb_write_field": (C.c_int, [H, C.c_int, C.c_void_p, C.c_int]),
         "flb_total_mass": (C.c_int, [H, C.POINTER(C.c_double)]),
+        "flb_total_mass_noalloc": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_int,
+                                             C.c_void_p, C.c_void_p]),
         "flb_cell_counts": (C.c_int, [H, C.POINTER(C.c_uint64)]),
         "flb_check_finite": (C.c_int, [H]),
         "flb_run_pass": (C.c_int, [H, C.c_int]),
@@ -93,6 +95,17 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         fn.argtypes = args
     _lib = L
     return L
+
+
+def total_mass_noalloc(mass_ptr: int, excess_ptr: int, flags_ptr: int, nx: int, ny: int, fs_mode: int,
+                       out_ptr: int, stream: int = 0):
+    """flb_total_mass_noalloc on raw device pointers: enqueues the FP64 free-surface
+    mass sum into the device double at ``out_ptr`` on ``stream`` and returns at once."""
+    st = load_library().flb_total_mass_noalloc(C.c_void_p(mass_ptr), C.c_void_p(excess_ptr),
+                                               C.c_void_p(flags_ptr), int(nx), int(ny), int(fs_mode),
+                                               C.c_void_p(out_ptr), C.c_void_p(stream))
+    if st != 0:
+        raise FlowLBError(st, "flb_total_mass_noalloc")
 
 
 def _dtype(elem_size: int, field: int):

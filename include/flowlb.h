@@ -153,6 +153,23 @@ FLB_API flb_status flb_write_field(flb_handle h, int field, const void* src, int
  * the populations the next step loads into non-solid cells. */
 FLB_API flb_status flb_total_mass(flb_handle h, double* mass);
 
+/* Allocation-free free-surface total mass; no counterpart in the reference.
+ * For callers that may not allocate device memory when they need the check
+ * (inside their own stream capture, under a fixed audited memory budget, or
+ * holding only pointers to someone else's buffers): it takes the device
+ * fields directly (mass and excess in FP64, flags as the solver keeps them,
+ * nx*ny cells each), launches on `stream` and writes the same FP64 sum as
+ * flb_total_mass to the device pointer `out` without waiting.  Its scratch is
+ * a fixed array of FLB_NOALLOC_MAX_CELLS/256 doubles (512 KiB) that every GPU
+ * loading the library holds until exit; larger grids are rejected with
+ * FLB_ERR_INVALID_ARGUMENT.  Nothing needs zeroing beforehand.  Calls that
+ * overlap on the GPU (other streams or host threads) share that scratch and
+ * race; the first call on a device looks its address up, so make it before
+ * any capture. */
+#define FLB_NOALLOC_MAX_CELLS 16777216u
+FLB_API flb_status flb_total_mass_noalloc(const double* mass, const double* excess, const uint8_t* flags,
+                                          uint32_t nx, uint32_t ny, int fs_mode, double* out, void* stream);
+
 /* Cell-type census: counts[0..3] = fluid, interface, gas, solid(wall). */
 FLB_API flb_status flb_cell_counts(flb_handle h, uint64_t counts[4]);
 
