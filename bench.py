@@ -309,7 +309,7 @@ def cpu_baseline(case, args):
     threads = os.cpu_count() or 1
     o = O.Oracle(case.flags, O.OracleConfig(variant=O.F32, free_surface=True, bb=O.BB_HALFWAY,
                                             fs_mode=O.FS_CONSERVATIVE, tau=case.tau, fy=case.fy, threads=threads,
-                                            u_max=U_MAX))
+                                            u_max=U_MAX, arithmetic=O.ARITH_FUSED))
     o.step(1)
     n = args.cpu_steps
     t0 = time.perf_counter()

@@ -51,6 +51,11 @@ struct KParams {
   // the mass fields come from the previous full step (see k_fs234)
   int trust_prev;
   float u_max;  // velocity limiter, 0 = off
+  // fused SRT arithmetic (collide_fused), float constants computed on the host:
+  // 1-w, -3k, F/2, F (zero without forcing), and per direction pair q (odd
+  // direction 2q+1) 3k c.F and 9k c.F, with k = 1 - w/2
+  float fu_omc, fu_nk3, fu_hfx, fu_hfy, fu_fx, fu_fy;
+  float fu_g[4], fu_h[4];
 };
 
 __device__ __forceinline__ bool same_bits(double a, double b) {

@@ -45,6 +45,7 @@ struct flb_engine {
   size_t s_size = 4, c_size = 4, m_size = 8;
   bool fs = false, hw = false, has_io = false;
   bool use_vec = false;  // vectorised stream-collide
+  bool fused = false;    // fused SRT arithmetic in stream-collide
   uint64_t t = 0;
   uint64_t launches = 0;
   int cur = 0;  // index of the current flag buffer (free surface)
@@ -120,10 +121,10 @@ struct DeviceGuard {
 template <class S, class C, class M>
 struct Ops {
   static void sc(flb_engine* h, uint32_t odd, bool wm) {
-    launch_sc<S, C, M>(h->kp, h->stream, odd, h->fs, h->hw, wm, h->use_vec);
+    launch_sc<S, C, M>(h->kp, h->stream, odd, h->fs, h->hw, wm, h->use_vec, h->fused);
   }
   static void sc_list(flb_engine* h, uint32_t odd, const TileList& tl) {
-    launch_sc_list<S, C, M>(h->kp, h->stream, odd, h->hw, tl, h->grid_sc);
+    launch_sc_list<S, C, M>(h->kp, h->stream, odd, h->hw, tl, h->grid_sc, h->fused);
   }
   static void fs1(flb_engine* h, uint32_t odd, const TileList& tl) {
     launch_fs1<S, C, M>(h->kp, h->stream, odd, h->hw, tl, h->grid_fs1);
@@ -296,6 +297,8 @@ flb_status validate(const flb_case_desc* d, std::string& msg) {
   if (d->fs_mode != FLB_FS_REFERENCE && d->fs_mode != FLB_FS_CONSERVATIVE)
     return msg = "fs_mode must be REFERENCE or CONSERVATIVE", FLB_ERR_INVALID_ARGUMENT;
   if (!(d->u_max >= 0.0f) || !std::isfinite(d->u_max)) return msg = "u_max must be finite and >= 0", FLB_ERR_INVALID_ARGUMENT;
+  if (d->arithmetic != FLB_ARITH_REFERENCE && d->arithmetic != FLB_ARITH_FUSED)
+    return msg = "arithmetic must be REFERENCE or FUSED", FLB_ERR_INVALID_ARGUMENT;
   if (d->kernel_variant < 0 || d->kernel_variant > 2) return msg = "kernel_variant must be 0, 1 or 2", FLB_ERR_INVALID_ARGUMENT;
   if (d->kernel_variant == 2 && d->nx % (d->precision == 64 ? 2u : 4u) != 0)
     return msg = "the vector stream-collide needs nx divisible by its vector width", FLB_ERR_UNSUPPORTED;
@@ -359,6 +362,7 @@ FLB_API void flb_case_desc_init(flb_case_desc* d) {
   d->bounce_back = FLB_BB_HALFWAY;
   d->fs_mode = FLB_FS_CONSERVATIVE;
   d->device = -1;
+  d->arithmetic = FLB_ARITH_FUSED;
 }
 
 FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
@@ -380,6 +384,7 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
   h->N = desc->nx * desc->ny;
   h->fs = desc->free_surface != 0;
   h->hw = desc->bounce_back == FLB_BB_HALFWAY;
+  h->fused = desc->arithmetic == FLB_ARITH_FUSED && desc->collision == FLB_COLLISION_SRT && !desc->subgrid;
   if (desc->device >= 0) h->device = desc->device;
   else cudaGetDevice(&h->device);
   if (h->device >= ndev) {
@@ -402,10 +407,14 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
   }
   {
     const uint32_t V = (uint32_t)vec_width(desc->precision);
-    // measured on a B200: one cell per thread is faster for FP32/FP64 (it runs
-    // at full occupancy), the vector path for FP16S (fewer instructions)
+    // measured on a B200 (8192x2048 single phase): the vector path is faster
+    // for FP16S, and for FP32 with the fused arithmetic (89 vs 82 GLUPS); with
+    // the reference arithmetic FP32 runs faster one cell per thread (full
+    // occupancy), and so does FP64
+    const bool fused = desc->arithmetic == FLB_ARITH_FUSED && desc->collision == FLB_COLLISION_SRT && !desc->subgrid;
     h->use_vec = desc->kernel_variant == 2 ||
-                 (desc->kernel_variant == 0 && desc->precision == 16 && desc->nx % V == 0);
+                 (desc->kernel_variant == 0 && desc->nx % V == 0 &&
+                  (desc->precision == 16 || (desc->precision == 32 && fused)));
   }
   s = check_io(h, desc->flags);
   if (s != FLB_OK) {
@@ -493,6 +502,27 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
       volatile float a = (float)cxs[i] * k.fx;
       volatile float b = (float)cys[i] * k.fy;
       k.cF[i] = a + b;
+    }
+    // constants of the fused arithmetic, float, uncontracted (the oracle
+    // computes the same ones)
+    volatile float om = k.inv_tau;
+    volatile float omc = 1.0f - om;
+    volatile float half = 0.5f * om;
+    volatile float kk = 1.0f - half;
+    volatile float k3 = 3.0f * kk;
+    volatile float k9 = 9.0f * kk;
+    k.fu_omc = omc;
+    k.fu_nk3 = -k3;
+    k.fu_fx = k.fx;
+    k.fu_fy = k.fy;
+    volatile float hx = 0.5f * k.fx, hy = 0.5f * k.fy;
+    k.fu_hfx = hx;
+    k.fu_hfy = hy;
+    for (int q = 0; q < 4; q++) {
+      volatile float g = k3 * k.cF[2 * q + 1];
+      volatile float hh = k9 * k.cF[2 * q + 1];
+      k.fu_g[q] = g;
+      k.fu_h[q] = hh;
     }
   }
   cudaError_t e = cudaMemcpyAsync(h->d_geo, desc->flags, N, cudaMemcpyHostToDevice, h->stream);

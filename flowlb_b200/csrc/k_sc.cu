@@ -28,6 +28,9 @@
 #ifndef FLB_VEC_MIN_BLOCKS
 #define FLB_VEC_MIN_BLOCKS 3
 #endif
+#ifndef FLB_VEC_MIN_BLOCKS_FUSED
+#define FLB_VEC_MIN_BLOCKS_FUSED 4
+#endif
 
 namespace flb {
 
@@ -35,7 +38,9 @@ namespace flb {
 // updated cell: density and velocity (or the inlet/outlet values), interface
 // marking, Guo forcing, the optional velocity limiter, density/velocity
 // write-back, equilibrium, Smagorinsky, SRT/TRT.  f: incoming -> post.
-template <class C, class M, bool FS, bool WM>
+// FU: the fused SRT arithmetic (collide_fused) for cells that are neither inlet
+// nor outlet; the host selects it only for SRT without the subgrid model.
+template <class C, class M, bool FS, bool WM, bool FU>
 __device__ __forceinline__ void collide_cell(const KParams& p, uint32_t idx, uint32_t x, uint32_t y, uint8_t flag,
                                              uint32_t nbm, C* f) {
   const uint32_t N = p.N;
@@ -59,9 +64,14 @@ __device__ __forceinline__ void collide_cell(const KParams& p, uint32_t idx, uin
       }
     }
   }
-  C rho, ux, uy;
+  C rho, ux, uy, inv = C(0);
   const uint8_t io = flag & (kInlet | kOutlet);
-  if (io & kInlet) {
+  if (FU && !io) {
+    C jx, jy;
+    moments_fused(f, rho, jx, jy, inv);
+    ux = jx * inv;
+    uy = jy * inv;
+  } else if (io & kInlet) {
     const C* Rs = static_cast<const C*>(p.rho_snap);
     const C* Us = static_cast<const C*>(p.u_snap);
     rho = Rs[idx + 1];
@@ -94,6 +104,18 @@ __device__ __forceinline__ void collide_cell(const KParams& p, uint32_t idx, uin
       if ((m > 1.001f * rho) || notGas) p.flags[idx] = (uint8_t)((flag & ~kFGI) | kIF);
       else if ((m < -0.001f) || notFluid) p.flags[idx] = (uint8_t)((flag & ~kFGI) | kIG);
     }
+  }
+  if (FU && !io) {
+    ux = fmac((C)p.fu_hfx, inv, ux);
+    uy = fmac((C)p.fu_hfy, inv, uy);
+    limit_u(p.u_max, ux, uy);
+    if (FS || WM) {
+      static_cast<C*>(p.u)[idx] = ux;
+      static_cast<C*>(p.u)[idx + N] = uy;
+      static_cast<C*>(p.rho)[idx] = rho;
+    }
+    collide_fused(f, rho, ux, uy, p.inv_tau, p.fu_omc, p.fu_nk3, p.fu_fx, p.fu_fy, p.fu_g, p.fu_h);
+    return;
   }
   C Fi[9];
   const bool use_force = p.use_force != 0;
@@ -167,7 +189,7 @@ __device__ __forceinline__ void collide_cell(const KParams& p, uint32_t idx, uin
 }
 
 // ---- one cell per thread -----------------------------------------------------
-template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD>
+template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD, bool FU>
 __device__ __forceinline__ void sc_cell(const KParams& p, uint32_t x, uint32_t y) {
   const uint32_t idx = x + y * p.nx;
   uint32_t nb[9];
@@ -187,20 +209,20 @@ __device__ __forceinline__ void sc_cell(const KParams& p, uint32_t x, uint32_t y
     if (HW) nbm = p.nbmask[idx];
     load_in<S, C, HW, ODD>(p, idx, nb, nbm, f);
   }
-  collide_cell<C, M, FS, WM>(p, idx, x, y, flag, nbm, f);
+  collide_cell<C, M, FS, WM, FU>(p, idx, x, y, flag, nbm, f);
   store_post<S, C, ODD>(p, idx, nb, f);
 }
 
-template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD>
+template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD, bool FU>
 __global__ void __launch_bounds__(kBlock, FLB_SC_MIN_BLOCKS) k_sc_scalar(const __grid_constant__ KParams p) {
   const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t y = blockIdx.y;
   if (x >= p.nx) return;
-  sc_cell<S, C, M, FS, HW, WM, ODD>(p, x, y);
+  sc_cell<S, C, M, FS, HW, WM, ODD, FU>(p, x, y);
 }
 
 // Free surface: the listed super-tiles, one row of a super-tile per warp.
-template <class S, class C, class M, bool HW, bool ODD>
+template <class S, class C, class M, bool HW, bool ODD, bool FU>
 __global__ void __launch_bounds__(kBlock, FLB_SC_MIN_BLOCKS) k_sc_list(const __grid_constant__ KParams p,
                                                                        const TileList tl) {
   const uint32_t n = tile_count(tl);
@@ -212,7 +234,7 @@ __global__ void __launch_bounds__(kBlock, FLB_SC_MIN_BLOCKS) k_sc_list(const __g
     const uint32_t xb = (t % tl.nsx) * kSTW + lane;
 #pragma unroll 1
     for (uint32_t j = 0; j < kSTW; j += 32)
-      if (xb + j < p.nx) sc_cell<S, C, M, true, HW, true, ODD>(p, xb + j, y);
+      if (xb + j < p.nx) sc_cell<S, C, M, true, HW, true, ODD, FU>(p, xb + j, y);
   }
 }
 
@@ -273,8 +295,9 @@ __device__ __forceinline__ void load_bytes(const uint8_t* ptr, uint8_t (&f)[V]) 
 
 constexpr int kVecBlock = 256;
 
-template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD>
-__global__ void __launch_bounds__(kVecBlock, FLB_VEC_MIN_BLOCKS) k_sc_vec(const __grid_constant__ KParams p) {
+template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD, bool FU>
+__global__ void __launch_bounds__(kVecBlock, FU ? FLB_VEC_MIN_BLOCKS_FUSED : FLB_VEC_MIN_BLOCKS)
+    k_sc_vec(const __grid_constant__ KParams p) {
   constexpr int V = Lanes<S>::V;
   using K = Codec<S, C>;
   const uint32_t nx = p.nx, ny = p.ny;
@@ -371,7 +394,7 @@ __global__ void __launch_bounds__(kVecBlock, FLB_VEC_MIN_BLOCKS) k_sc_vec(const 
         if ((nbm >> (i - 1)) & 1u) f[i + 1] = K::ld(slotp<S>(p, slot_a<ODD>(i)), nb[i], i + 1, p.f16_inv);
       }
     }
-    collide_cell<C, M, FS, WM>(p, idx, x, y, fl[k], nbm, f);
+    collide_cell<C, M, FS, WM, FU>(p, idx, x, y, fl[k], nbm, f);
     K::st(raw0, k, 0, f[0], p.f16_scale);
 #pragma unroll
     for (int q = 0; q < 4; q++) {
@@ -411,59 +434,76 @@ __global__ void __launch_bounds__(kVecBlock, FLB_VEC_MIN_BLOCKS) k_sc_vec(const 
 }
 
 // ---- launchers -------------------------------------------------------------------
-template <class S, class C, class M, bool FS, bool HW, bool WM>
+template <class S, class C, class M, bool FS, bool HW, bool WM, bool FU>
 static void launch_sc_t(const KParams& kp, cudaStream_t st, uint32_t odd, bool vec) {
   if (vec) {
     constexpr int V = Lanes<S>::V;
     const uint32_t per_row = kp.nx / V;
     const uint32_t block = per_row >= (uint32_t)kVecBlock ? (uint32_t)kVecBlock : ((per_row + 31u) / 32u) * 32u;
     const dim3 g((per_row + block - 1) / block, kp.ny);
-    if (odd) k_sc_vec<S, C, M, FS, HW, WM, true><<<g, block, 0, st>>>(kp);
-    else k_sc_vec<S, C, M, FS, HW, WM, false><<<g, block, 0, st>>>(kp);
+    if (odd) k_sc_vec<S, C, M, FS, HW, WM, true, FU><<<g, block, 0, st>>>(kp);
+    else k_sc_vec<S, C, M, FS, HW, WM, false, FU><<<g, block, 0, st>>>(kp);
   } else {
     const dim3 g((kp.nx + kBlock - 1) / kBlock, kp.ny);
-    if (odd) k_sc_scalar<S, C, M, FS, HW, WM, true><<<g, kBlock, 0, st>>>(kp);
-    else k_sc_scalar<S, C, M, FS, HW, WM, false><<<g, kBlock, 0, st>>>(kp);
+    if (odd) k_sc_scalar<S, C, M, FS, HW, WM, true, FU><<<g, kBlock, 0, st>>>(kp);
+    else k_sc_scalar<S, C, M, FS, HW, WM, false, FU><<<g, kBlock, 0, st>>>(kp);
+  }
+}
+
+template <class S, class C, class M, bool FU>
+static void launch_sc_f(const KParams& kp, cudaStream_t st, uint32_t odd, bool fs, bool hw, bool wm, bool vec) {
+  if (fs) {
+    if (hw) launch_sc_t<S, C, M, true, true, true, FU>(kp, st, odd, vec);
+    else launch_sc_t<S, C, M, true, false, true, FU>(kp, st, odd, vec);
+  } else if (wm) {
+    if (hw) launch_sc_t<S, C, M, false, true, true, FU>(kp, st, odd, vec);
+    else launch_sc_t<S, C, M, false, false, true, FU>(kp, st, odd, vec);
+  } else {
+    if (hw) launch_sc_t<S, C, M, false, true, false, FU>(kp, st, odd, vec);
+    else launch_sc_t<S, C, M, false, false, false, FU>(kp, st, odd, vec);
   }
 }
 
 template <class S, class C, class M>
-void launch_sc(const KParams& kp, cudaStream_t st, uint32_t odd, bool fs, bool hw, bool wm, bool vec) {
-  if (fs) {
-    if (hw) launch_sc_t<S, C, M, true, true, true>(kp, st, odd, vec);
-    else launch_sc_t<S, C, M, true, false, true>(kp, st, odd, vec);
-  } else if (wm) {
-    if (hw) launch_sc_t<S, C, M, false, true, true>(kp, st, odd, vec);
-    else launch_sc_t<S, C, M, false, false, true>(kp, st, odd, vec);
-  } else {
-    if (hw) launch_sc_t<S, C, M, false, true, false>(kp, st, odd, vec);
-    else launch_sc_t<S, C, M, false, false, false>(kp, st, odd, vec);
-  }
+void launch_sc(const KParams& kp, cudaStream_t st, uint32_t odd, bool fs, bool hw, bool wm, bool vec, bool fu) {
+  if (fu) launch_sc_f<S, C, M, true>(kp, st, odd, fs, hw, wm, vec);
+  else launch_sc_f<S, C, M, false>(kp, st, odd, fs, hw, wm, vec);
 }
 
 int vec_width(int precision) { return precision == 64 ? Lanes<double>::V : Lanes<float>::V; }
 
-template <class S, class C, class M>
-void launch_sc_list(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl, uint32_t grid) {
+template <class S, class C, class M, bool FU>
+static void launch_sc_list_f(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl,
+                             uint32_t grid) {
   if (hw) {
-    if (odd) k_sc_list<S, C, M, true, true><<<grid, kBlock, 0, st>>>(kp, tl);
-    else k_sc_list<S, C, M, true, false><<<grid, kBlock, 0, st>>>(kp, tl);
+    if (odd) k_sc_list<S, C, M, true, true, FU><<<grid, kBlock, 0, st>>>(kp, tl);
+    else k_sc_list<S, C, M, true, false, FU><<<grid, kBlock, 0, st>>>(kp, tl);
   } else {
-    if (odd) k_sc_list<S, C, M, false, true><<<grid, kBlock, 0, st>>>(kp, tl);
-    else k_sc_list<S, C, M, false, false><<<grid, kBlock, 0, st>>>(kp, tl);
+    if (odd) k_sc_list<S, C, M, false, true, FU><<<grid, kBlock, 0, st>>>(kp, tl);
+    else k_sc_list<S, C, M, false, false, FU><<<grid, kBlock, 0, st>>>(kp, tl);
   }
 }
 
 template <class S, class C, class M>
+void launch_sc_list(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl, uint32_t grid,
+                    bool fu) {
+  if (fu) launch_sc_list_f<S, C, M, true>(kp, st, odd, hw, tl, grid);
+  else launch_sc_list_f<S, C, M, false>(kp, st, odd, hw, tl, grid);
+}
+
+template <class S, class C, class M>
 int sc_list_blocks_per_sm() {
-  int n = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sc_list<S, C, M, true, false>, kBlock, 0);
+  int n = 0, m = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sc_list<S, C, M, true, false, false>, kBlock, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_sc_list<S, C, M, true, false, true>, kBlock, 0);
+  n = n < m ? n : m;
   return n > 0 ? n : 1;
 }
 
 #define FLB_INSTANTIATE(S, C, M)                                                                               \
-  template void launch_sc<S, C, M>(const KParams&, cudaStream_t, uint32_t, bool, bool, bool, bool);           \
-  template void launch_sc_list<S, C, M>(const KParams&, cudaStream_t, uint32_t, bool, const TileList&, uint32_t); \
+  template void launch_sc<S, C, M>(const KParams&, cudaStream_t, uint32_t, bool, bool, bool, bool, bool);     \
+  template void launch_sc_list<S, C, M>(const KParams&, cudaStream_t, uint32_t, bool, const TileList&, uint32_t,  \
+                                        bool);                                                                  \
   template int sc_list_blocks_per_sm<S, C, M>();
 FLB_FOR_EACH_VARIANT(FLB_INSTANTIATE)
 #undef FLB_INSTANTIATE

@@ -18,13 +18,15 @@
 
 namespace flb {
 
-// stream-collide; vec selects the V-cells-per-thread data path
+// stream-collide; vec selects the V-cells-per-thread data path, fu the fused
+// SRT arithmetic
 template <class S, class C, class M>
-void launch_sc(const KParams& kp, cudaStream_t st, uint32_t odd, bool fs, bool hw, bool wm, bool vec);
+void launch_sc(const KParams& kp, cudaStream_t st, uint32_t odd, bool fs, bool hw, bool wm, bool vec, bool fu);
 int vec_width(int precision);
 // free surface: the listed super-tiles in a persistent grid of `grid` blocks
 template <class S, class C, class M>
-void launch_sc_list(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl, uint32_t grid);
+void launch_sc_list(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl, uint32_t grid,
+                    bool fu);
 template <class S, class C, class M>
 int sc_list_blocks_per_sm();
 

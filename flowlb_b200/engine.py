@@ -19,6 +19,7 @@ LIB_PATH = os.environ.get("FLOWLB_LIB", os.path.join(HERE, "libflowlb.so"))
 FIELD_F, FIELD_RHO, FIELD_U, FIELD_FLAGS, FIELD_MASS, FIELD_EXCESS, FIELD_PHI = range(7)
 BB_IMPLICIT, BB_HALFWAY = 0, 1
 FS_REFERENCE, FS_CONSERVATIVE = 0, 1
+ARITH_REFERENCE, ARITH_FUSED = 0, 1
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4: "unsupported",
           5: "I/O error", 6: "non-finite populations", 7: "no CUDA device"}
@@ -39,7 +40,7 @@ class CaseDesc(C.Structure):
         ("subgrid", C.c_int32), ("use_volumetric_force", C.c_int32), ("tau", C.c_float), ("fx", C.c_float),
         ("fy", C.c_float), ("bounce_back", C.c_int32), ("fs_mode", C.c_int32), ("f16_scale", C.c_float),
         ("device", C.c_int32), ("stream", C.c_void_p), ("inlet_ux", C.c_double), ("inlet_uy", C.c_double),
-        ("kernel_variant", C.c_int32), ("u_max", C.c_float),
+        ("kernel_variant", C.c_int32), ("u_max", C.c_float), ("arithmetic", C.c_int32),
     ]
 
 
@@ -129,7 +130,7 @@ class Solver:
                  use_force: bool = True, collision: int = 0, subgrid: bool = False,
                  bounce_back: int = BB_HALFWAY, fs_mode: int = FS_CONSERVATIVE, inlet_ux: float = 0.0,
                  inlet_uy: float = 0.0, f16_scale: float = 0.0, device: int = -1, stream: int | None = None,
-                 kernel_variant: int = 0, u_max: float = 0.0):
+                 kernel_variant: int = 0, u_max: float = 0.0, arithmetic: int = ARITH_FUSED):
         L = load_library()
         g = np.ascontiguousarray(flags, dtype=np.uint8)
         if g.ndim != 2:
@@ -148,6 +149,7 @@ class Solver:
         d.stream = stream or None
         d.kernel_variant = int(kernel_variant)
         d.u_max = float(u_max)
+        d.arithmetic = int(arithmetic)
         self._desc = d
         self.free_surface = bool(free_surface)
         self.precision = precision

@@ -40,13 +40,15 @@ def main(argv=None):
     ap.add_argument("--kernel-variant", type=int, default=0, choices=[0, 1, 2])
     ap.add_argument("--profile", action="store_true", help="per-pass CUDA-event times")
     ap.add_argument("--u-max", type=float, default=0.0, help="velocity limiter (0 = off)")
+    ap.add_argument("--arithmetic", default="fused", choices=["fused", "reference"])
     a = ap.parse_args(argv)
     case = CASES[a.case](a)
     s = E.Solver(case.flags, free_surface=case.free_surface, precision=a.precision,
                  mass_precision=a.mass_precision, tau=case.tau, fx=case.fx, fy=case.fy, subgrid=a.subgrid,
                  bounce_back=E.BB_HALFWAY if a.bounce_back == "halfway" else E.BB_IMPLICIT,
                  fs_mode=E.FS_CONSERVATIVE if a.fs_mode == "conservative" else E.FS_REFERENCE,
-                 kernel_variant=a.kernel_variant, u_max=a.u_max)
+                 kernel_variant=a.kernel_variant, u_max=a.u_max,
+                 arithmetic=E.ARITH_FUSED if a.arithmetic == "fused" else E.ARITH_REFERENCE)
     m0 = s.total_mass()
     s.step(a.warmup)
     s.sync()

@@ -69,6 +69,16 @@ enum { FLB_BB_IMPLICIT = 0, FLB_BB_HALFWAY = 1 };
  * HALFWAY walls it conserves total fluid mass to round-off. */
 enum { FLB_FS_REFERENCE = 0, FLB_FS_CONSERVATIVE = 1 };
 
+/* Arithmetic of the stream-collide step.  REFERENCE evaluates density,
+ * velocity, equilibrium, Guo forcing and the relaxation with the reference's
+ * expressions and operand order (bit-identical to FlowLB built without
+ * floating-point contraction).  FUSED computes the same second-order BGK + Guo
+ * update with explicit fused multiply-adds and shared subexpressions (about a
+ * third of the operations); it applies to SRT without the subgrid model, and
+ * TRT, the subgrid model and inlet/outlet cells keep the reference
+ * expressions. */
+enum { FLB_ARITH_REFERENCE = 0, FLB_ARITH_FUSED = 1 };
+
 /* Collision operator (reference d_collisionOperator). */
 enum { FLB_COLLISION_SRT = 0, FLB_COLLISION_TRT = 1 };
 
@@ -107,6 +117,7 @@ typedef struct flb_case_desc {
   float u_max;                /* velocity limiter, lattice units (0 = off, the reference behaviour): the
                                  force-shifted velocity used for feq and forcing is scaled down to |u| = u_max;
                                  keeps high-Mach free-surface fronts stable; mass is still conserved */
+  int32_t arithmetic;         /* FLB_ARITH_* (default FUSED; REFERENCE reproduces FlowLB's rounding) */
 } flb_case_desc;
 
 typedef struct flb_engine* flb_handle;

@@ -44,6 +44,9 @@ struct orc_state {
   uint64_t t;
   int nthreads;
   float inv_tau;
+  /* constants of the fused SRT arithmetic (see FN(collide_fused)) */
+  int fused;
+  float fu_omc, fu_nk3, fu_hfx, fu_hfy, fu_fx, fu_fy, fu_g[4], fu_h[4];
   float f16_scale, f16_inv_scale;
   size_t s_size, c_size, m_size;
   void* f;
@@ -299,6 +302,28 @@ orc_state* orc_create(const orc_params* p, const uint8_t* geometry_flags) {
   /* cudaInitData.cu:81-82: tau and its inverse are float */
   const float h_tau = p->tau;
   s->inv_tau = 1.0f / h_tau;
+  {
+    /* fused arithmetic: float constants, each operation rounded on its own */
+    s->fused = p->arithmetic == 1 && p->collision == 0 && !p->subgrid;
+    const float fx = p->use_force ? p->fx : 0.0f, fy = p->use_force ? p->fy : 0.0f;
+    const float om = s->inv_tau;
+    const float kk = 1.0f - 0.5f * om;
+    const float k3 = 3.0f * kk, k9 = 9.0f * kk;
+    s->fu_omc = 1.0f - om;
+    s->fu_nk3 = -k3;
+    s->fu_fx = fx;
+    s->fu_fy = fy;
+    s->fu_hfx = 0.5f * fx;
+    s->fu_hfy = 0.5f * fy;
+    for (int q = 0; q < 4; q++) {
+      const int i = 2 * q + 1;
+      const float a = (float)ORC_CX[i] * fx;
+      const float b = (float)ORC_CY[i] * fy;
+      const float cF = a + b;
+      s->fu_g[q] = k3 * cF;
+      s->fu_h[q] = k9 * cF;
+    }
+  }
   s->f16_scale = p->f16_scale > 0.0f ? p->f16_scale : 4096.0f;
   s->f16_inv_scale = 1.0f / s->f16_scale;
   switch (p->variant) {

@@ -72,6 +72,7 @@ typedef struct {
   int32_t threads;       /* OpenMP threads (<=0: default) */
   double inlet_ux, inlet_uy; /* inlet velocity, lattice units (double, as LBVelocity) */
   float u_max;           /* velocity limiter (0: off), see flb_case_desc.u_max */
+  int32_t arithmetic;    /* 0 the reference's expressions, 1 the engine's fused SRT form */
 } orc_params;
 
 typedef struct orc_state orc_state;

@@ -24,6 +24,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 F64, F32, F16S, F32_M32 = 0, 1, 2, 3
 BB_IMPLICIT, BB_HALFWAY = 0, 1
 FS_REFERENCE, FS_CONSERVATIVE = 0, 1
+ARITH_REFERENCE, ARITH_FUSED = 0, 1
 K_STREAM_COLLIDE, K_FS1, K_FS2, K_FS3, K_FS4 = 0, 1, 2, 3, 4
 FIELD_F, FIELD_RHO, FIELD_U, FIELD_FLAGS, FIELD_MASS, FIELD_EXCESS, FIELD_PHI = range(7)
 
@@ -35,7 +36,7 @@ class OrcParams(C.Structure):
         ("use_force", C.c_int32), ("fs_count_pre", C.c_int32), ("fs1_post", C.c_int32), ("tau", C.c_float),
         ("fx", C.c_float),
         ("fy", C.c_float), ("f16_scale", C.c_float), ("threads", C.c_int32), ("inlet_ux", C.c_double),
-        ("inlet_uy", C.c_double), ("u_max", C.c_float),
+        ("inlet_uy", C.c_double), ("u_max", C.c_float), ("arithmetic", C.c_int32),
     ]
 
 
@@ -101,6 +102,7 @@ class OracleConfig:
     f16_scale: float = 4096.0
     threads: int = 0
     u_max: float = 0.0
+    arithmetic: int = ARITH_REFERENCE
 
 
 class Oracle:
@@ -115,7 +117,7 @@ class Oracle:
         p = OrcParams(self.nx, self.ny, cfg.variant, int(cfg.free_surface), cfg.bb, cfg.fs_mode, cfg.collision,
                       int(cfg.subgrid), int(cfg.use_force), int(cfg.fs_count_pre), int(cfg.fs1_post), cfg.tau,
                       cfg.fx, cfg.fy,
-                      cfg.f16_scale, cfg.threads, cfg.inlet_ux, cfg.inlet_uy, cfg.u_max)
+                      cfg.f16_scale, cfg.threads, cfg.inlet_ux, cfg.inlet_uy, cfg.u_max, cfg.arithmetic)
         self._h = lib().orc_create(C.byref(p), g.ctypes.data)
         if not self._h:
             raise ValueError("orc_create rejected the case")

@@ -23,15 +23,19 @@ VNAME = {O.F64: "f64", O.F32: "f32", O.F32_M32: "f32m32", O.F16S: "f16s"}
 
 
 def make_pair(flags, variant, *, free_surface=False, bb=O.BB_IMPLICIT, fs_mode=O.FS_REFERENCE, tau=0.6, fx=0.0,
-              fy=0.0, collision=0, subgrid=False, use_force=True, inlet=(0.0, 0.0), kernel_variant=0, u_max=0.0):
+              fy=0.0, collision=0, subgrid=False, use_force=True, inlet=(0.0, 0.0), kernel_variant=0, u_max=0.0,
+              arith=O.ARITH_REFERENCE):
     prec, mprec = PREC[variant]
     s = E.Solver(flags, free_surface=free_surface, precision=prec, mass_precision=mprec, tau=tau, fx=fx, fy=fy,
                  use_force=use_force, collision=collision, subgrid=subgrid, bounce_back=bb, fs_mode=fs_mode,
-                 inlet_ux=inlet[0], inlet_uy=inlet[1], kernel_variant=kernel_variant, u_max=u_max)
+                 inlet_ux=inlet[0], inlet_uy=inlet[1], kernel_variant=kernel_variant, u_max=u_max, arithmetic=arith)
     o = O.Oracle(flags, O.OracleConfig(variant=variant, free_surface=free_surface, bb=bb, fs_mode=fs_mode, tau=tau,
                                        fx=fx, fy=fy, collision=collision, subgrid=subgrid, use_force=use_force,
-                                       inlet_ux=inlet[0], inlet_uy=inlet[1], u_max=u_max))
+                                       inlet_ux=inlet[0], inlet_uy=inlet[1], u_max=u_max, arithmetic=arith))
     return s, o
+
+
+ARITHS = pytest.mark.parametrize("arith", [O.ARITH_REFERENCE, O.ARITH_FUSED], ids=["ref-arith", "fused"])
 
 
 def oracle_f(o, variant):
@@ -57,8 +61,9 @@ def channel():
                                         (O.F32_M32, O.BB_IMPLICIT)],
                          ids=lambda v: str(v))
 @pytest.mark.parametrize("kv", [1, 2], ids=["scalar", "vector"])
-def test_single_phase_steps_match_oracle(channel, variant, bb, kv):
-    s, o = make_pair(channel.flags, variant, bb=bb, tau=channel.tau, fx=1e-5, kernel_variant=kv)
+@ARITHS
+def test_single_phase_steps_match_oracle(channel, variant, bb, kv, arith):
+    s, o = make_pair(channel.flags, variant, bb=bb, tau=channel.tau, fx=1e-5, kernel_variant=kv, arith=arith)
     assert_same_state(s, o, variant, False, "init")
     for n in (1, 2, 37, 80):  # single steps, a graph pair, graphs of 32 steps
         s.step(n)
@@ -78,10 +83,11 @@ def test_single_phase_steps_match_oracle(channel, variant, bb, kv):
     (O.F32, O.BB_HALFWAY, O.FS_REFERENCE),
 ], ids=lambda v: str(v))
 @pytest.mark.parametrize("kv", [1, 2], ids=["scalar", "vector"])
-def test_free_surface_steps_match_oracle(variant, bb, fs_mode, kv):
+@ARITHS
+def test_free_surface_steps_match_oracle(variant, bb, fs_mode, kv, arith):
     c = cases.small_dam_break(96, 64)
     s, o = make_pair(c.flags, variant, free_surface=True, bb=bb, fs_mode=fs_mode, tau=c.tau, fy=c.fy,
-                     kernel_variant=kv)
+                     kernel_variant=kv, arith=arith)
     assert_same_state(s, o, variant, True, "init")
     for n in (1, 3, 40, 76):
         s.step(n)
