@@ -56,6 +56,7 @@ struct KParams {
   // direction 2q+1) 3k c.F and 9k c.F, with k = 1 - w/2
   float fu_omc, fu_nk3, fu_hfx, fu_hfy, fu_fx, fu_fy;
   float fu_g[4], fu_h[4];
+  float fu_sw[3];  // FP16S deviation form: f16_scale * w for directions 0, 1..4, 5..8
 };
 
 __device__ __forceinline__ bool same_bits(double a, double b) {
@@ -97,17 +98,17 @@ __device__ __forceinline__ constexpr int slot_b(int i) { return ODD ? i + 1 : i;
 // neighbour is read from where this cell stored the opposite population last
 // step, i.e. it comes back reflected after one step.  nbm bit k-1 = neighbour
 // k is a wall.
-template <class S, class C, bool HW, bool ODD>
+template <class S, class C, bool HW, bool ODD, class K = Codec<S, C>>
 __device__ __forceinline__ void load_in(const KParams& p, uint32_t idx, const uint32_t* nb, uint32_t nbm, C* f) {
   const float inv = p.f16_inv;
-  f[0] = Codec<S, C>::ld(slotp<S>(p, 0), idx, 0, inv);
+  f[0] = K::ld(slotp<S>(p, 0), idx, 0, inv);
 #pragma unroll
   for (int i = 1; i < 9; i += 2) {
     const int a = slot_a<ODD>(i), b = slot_b<ODD>(i);
-    if (HW && ((nbm >> i) & 1u)) f[i] = Codec<S, C>::ld(slotp<S>(p, b), idx, i, inv);
-    else f[i] = Codec<S, C>::ld(slotp<S>(p, a), idx, i, inv);
-    if (HW && ((nbm >> (i - 1)) & 1u)) f[i + 1] = Codec<S, C>::ld(slotp<S>(p, a), nb[i], i + 1, inv);
-    else f[i + 1] = Codec<S, C>::ld(slotp<S>(p, b), nb[i], i + 1, inv);
+    if (HW && ((nbm >> i) & 1u)) f[i] = K::ld(slotp<S>(p, b), idx, i, inv);
+    else f[i] = K::ld(slotp<S>(p, a), idx, i, inv);
+    if (HW && ((nbm >> (i - 1)) & 1u)) f[i + 1] = K::ld(slotp<S>(p, a), nb[i], i + 1, inv);
+    else f[i + 1] = K::ld(slotp<S>(p, b), nb[i], i + 1, inv);
   }
 }
 
@@ -123,14 +124,14 @@ __device__ __forceinline__ void load_out(const KParams& p, uint32_t idx, const u
 }
 
 // storef, cellCalculations.cuh:228-238.
-template <class S, class C, bool ODD>
+template <class S, class C, bool ODD, class K = Codec<S, C>>
 __device__ __forceinline__ void store_post(const KParams& p, uint32_t idx, const uint32_t* nb, const C* f) {
   const float sc = p.f16_scale;
-  Codec<S, C>::st(slotp<S>(p, 0), idx, 0, f[0], sc);
+  K::st(slotp<S>(p, 0), idx, 0, f[0], sc);
 #pragma unroll
   for (int i = 1; i < 9; i += 2) {
-    Codec<S, C>::st(slotp<S>(p, slot_b<ODD>(i)), nb[i], i, f[i], sc);
-    Codec<S, C>::st(slotp<S>(p, slot_a<ODD>(i)), idx, i + 1, f[i + 1], sc);
+    K::st(slotp<S>(p, slot_b<ODD>(i)), nb[i], i, f[i], sc);
+    K::st(slotp<S>(p, slot_a<ODD>(i)), idx, i + 1, f[i + 1], sc);
   }
 }
 

@@ -518,6 +518,9 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
     volatile float hx = 0.5f * k.fx, hy = 0.5f * k.fy;
     k.fu_hfx = hx;
     k.fu_hfy = hy;
+    k.fu_sw[0] = k.f16_scale * wgt<float>(0);  // exact: power-of-two scale
+    k.fu_sw[1] = k.f16_scale * wgt<float>(1);
+    k.fu_sw[2] = k.f16_scale * wgt<float>(5);
     for (int q = 0; q < 4; q++) {
       volatile float g = k3 * k.cF[2 * q + 1];
       volatile float hh = k9 * k.cF[2 * q + 1];

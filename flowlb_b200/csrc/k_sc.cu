@@ -17,6 +17,8 @@
 // Both are templated on the step parity (slot indices become constants) and,
 // for the single-phase build, issue the population loads together with the
 // flag load instead of after it.
+#include <type_traits>
+
 #include "launch.h"
 
 // occupancy targets (resident blocks per SM) of the two data paths
@@ -40,10 +42,30 @@ namespace flb {
 // write-back, equilibrium, Smagorinsky, SRT/TRT.  f: incoming -> post.
 // FU: the fused SRT arithmetic (collide_fused) for cells that are neither inlet
 // nor outlet; the host selects it only for SRT without the subgrid model.
-template <class C, class M, bool FS, bool WM, bool FU>
+// DEV: f holds FP16S deviations h = (f - w) * scale (single phase with FU).
+template <class C, class M, bool FS, bool WM, bool FU, bool DEV = false>
 __device__ __forceinline__ void collide_cell(const KParams& p, uint32_t idx, uint32_t x, uint32_t y, uint8_t flag,
                                              uint32_t nbm, C* f) {
   const uint32_t N = p.N;
+  if constexpr (DEV) {
+    if (flag & (kInlet | kOutlet)) {
+      // inlet / outlet: the reference expressions on the decoded populations
+#pragma unroll
+      for (int i = 0; i < 9; i++) f[i] = fmac(f[i], p.f16_inv, wgt<C>(i));
+      collide_cell<C, M, FS, WM, false, false>(p, idx, x, y, flag, nbm, f);
+#pragma unroll
+      for (int i = 0; i < 9; i++) f[i] = (f[i] - wgt<C>(i)) * p.f16_scale;
+      return;
+    }
+    const DevOut o = collide_fused_dev(f, p.f16_inv, p.inv_tau, p.fu_omc, p.fu_nk3, p.fu_hfx, p.fu_hfy, p.fu_fx,
+                                       p.fu_fy, p.u_max, p.fu_g, p.fu_h, p.fu_sw);
+    if (WM) {
+      static_cast<C*>(p.u)[idx] = o.ux;
+      static_cast<C*>(p.u)[idx + N] = o.uy;
+      static_cast<C*>(p.rho)[idx] = o.rho;
+    }
+    return;
+  }
   if constexpr (FS) {
     // reference mode: FS_1 left the populations it rebuilt toward gas here.
     // FS_1 wrote them to their regular slots; where a half-way wall reflects
@@ -189,8 +211,14 @@ __device__ __forceinline__ void collide_cell(const KParams& p, uint32_t idx, uin
 }
 
 // ---- one cell per thread -----------------------------------------------------
+// FP16S single phase with the fused arithmetic works in deviation units
+template <class S, bool FS, bool FU>
+constexpr bool kDev = FU && !FS && std::is_same<S, __half>::value;
+
 template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD, bool FU>
 __device__ __forceinline__ void sc_cell(const KParams& p, uint32_t x, uint32_t y) {
+  constexpr bool DEV = kDev<S, FS, FU>;
+  using K = typename std::conditional<DEV, RawHalf, Codec<S, C>>::type;
   const uint32_t idx = x + y * p.nx;
   uint32_t nb[9];
   neighbours(x, y, p.nx, p.ny, nb);
@@ -201,16 +229,16 @@ __device__ __forceinline__ void sc_cell(const KParams& p, uint32_t x, uint32_t y
     // single phase: nearly every cell is updated, so load with the flag
     flag = p.flags[idx];
     if (HW) nbm = p.nbmask[idx];
-    load_in<S, C, HW, ODD>(p, idx, nb, nbm, f);
+    load_in<S, C, HW, ODD, K>(p, idx, nb, nbm, f);
     if (flag & (kGas | kWall)) return;
   } else {
     flag = p.flags[idx];
     if (flag & (kGas | kWall)) return;
     if (HW) nbm = p.nbmask[idx];
-    load_in<S, C, HW, ODD>(p, idx, nb, nbm, f);
+    load_in<S, C, HW, ODD, K>(p, idx, nb, nbm, f);
   }
-  collide_cell<C, M, FS, WM, FU>(p, idx, x, y, flag, nbm, f);
-  store_post<S, C, ODD>(p, idx, nb, f);
+  collide_cell<C, M, FS, WM, FU, DEV>(p, idx, x, y, flag, nbm, f);
+  store_post<S, C, ODD, K>(p, idx, nb, f);
 }
 
 template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD, bool FU>
@@ -299,7 +327,8 @@ template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD, bool F
 __global__ void __launch_bounds__(kVecBlock, FU ? FLB_VEC_MIN_BLOCKS_FUSED : FLB_VEC_MIN_BLOCKS)
     k_sc_vec(const __grid_constant__ KParams p) {
   constexpr int V = Lanes<S>::V;
-  using K = Codec<S, C>;
+  constexpr bool DEV = kDev<S, FS, FU>;
+  using K = typename std::conditional<DEV, RawHalf, Codec<S, C>>::type;
   const uint32_t nx = p.nx, ny = p.ny;
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t x0 = (blockIdx.x * blockDim.x + threadIdx.x) * V;
@@ -394,7 +423,7 @@ __global__ void __launch_bounds__(kVecBlock, FU ? FLB_VEC_MIN_BLOCKS_FUSED : FLB
         if ((nbm >> (i - 1)) & 1u) f[i + 1] = K::ld(slotp<S>(p, slot_a<ODD>(i)), nb[i], i + 1, p.f16_inv);
       }
     }
-    collide_cell<C, M, FS, WM, FU>(p, idx, x, y, fl[k], nbm, f);
+    collide_cell<C, M, FS, WM, FU, DEV>(p, idx, x, y, fl[k], nbm, f);
     K::st(raw0, k, 0, f[0], p.f16_scale);
 #pragma unroll
     for (int q = 0; q < 4; q++) {

@@ -62,6 +62,13 @@ struct Codec<__half, float> {
   }
 };
 
+// Raw FP16S access: the stored scaled deviation h = (f - w) * scale as a
+// float, for arithmetic done in deviation units (collide_fused_dev).
+struct RawHalf {
+  __device__ __forceinline__ static float ld(const __half* F, uint32_t a, int, float) { return __half2float(F[a]); }
+  __device__ __forceinline__ static void st(__half* F, uint32_t a, int, float v, float) { F[a] = __float2half_rn(v); }
+};
+
 // ---- per-cell arithmetic, cellCalculations.cuh ----------------------------
 
 // calculateDensity, cellCalculations.cuh:16-22
@@ -182,6 +189,50 @@ __device__ __forceinline__ void collide_fused(C* f, C rho, C ux, C uy, float om,
     f[i] = fmac(w, f[i], wi * (E + O));
     f[i + 1] = fmac(w, f[i + 1], wi * (E - O));
   }
+}
+
+// The fused update in FP16S deviation units (single phase): h_i = S (f_i - w_i)
+// goes in and out without conversion to f.  With rho = 1 + delta,
+//   h_i <- (1-w) h_i + S w_i (t_i - w),   t_i - w = Bd + g_i + cu (3A + h_i' + 4.5 A cu),
+//   Bd = w (delta t1 - 1.5 u.u) - 3k u.F,  t1 = 1 - 1.5 u.u,
+// the same update as collide_fused (the +-w_i of the codec cancel).
+// rho, ux, uy: out; h: in/out.
+struct DevOut {
+  float rho, ux, uy;
+};
+__device__ __forceinline__ DevOut collide_fused_dev(float* h, float invS, float om, float omc, float nk3, float hfx,
+                                                    float hfy, float fx, float fy, float umax, const float* g,
+                                                    const float* hh, const float* sw) {
+  const float s12 = h[1] + h[2], s34 = h[3] + h[4], s56 = h[5] + h[6], s78 = h[7] + h[8];
+  const float d12 = h[1] - h[2], d34 = h[3] - h[4], d56 = h[5] - h[6], d78 = h[7] - h[8];
+  const float dS = ((h[0] + s12) + (s34 + s56)) + s78;
+  const float jx = (d12 + d56) + d78, jy = (d34 + d56) - d78;
+  const float delta = dS * invS;
+  const float rho = fmac(dS, invS, 1.0f);
+  const float inv = 1.0f / rho;
+  const float invs = inv * invS;
+  float ux = fmac(hfx, inv, jx * invs);
+  float uy = fmac(hfy, inv, jy * invs);
+  limit_u(umax, ux, uy);
+  const float usq = fmac(ux, ux, uy * uy);
+  const float uF = fmac(ux, fx, uy * fy);
+  const float A = om * rho;
+  const float t1 = fmac(-1.5f, usq, 1.0f);
+  const float x = fmac(delta, t1, -1.5f * usq);
+  const float Bd = fmac(om, x, nk3 * uF);
+  const float A3 = 3.0f * A, A45 = 4.5f * A;
+  h[0] = fmac(omc, h[0], sw[0] * Bd);
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int i = 2 * q + 1;
+    const float cu = q == 0 ? ux : (q == 1 ? uy : (q == 2 ? ux + uy : ux - uy));
+    const float E = fmac(cu, fmac(A45, cu, hh[q]), Bd);
+    const float O = fmac(A3, cu, g[q]);
+    const float swi = sw[q < 2 ? 1 : 2];
+    h[i] = fmac(omc, h[i], swi * (E + O));
+    h[i + 1] = fmac(omc, h[i + 1], swi * (E - O));
+  }
+  return DevOut{rho, ux, uy};
 }
 
 // Neighbour cells with periodic wrap, cellCalculations.cuh:82-109.

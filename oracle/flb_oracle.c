@@ -46,7 +46,7 @@ struct orc_state {
   float inv_tau;
   /* constants of the fused SRT arithmetic (see FN(collide_fused)) */
   int fused;
-  float fu_omc, fu_nk3, fu_hfx, fu_hfy, fu_fx, fu_fy, fu_g[4], fu_h[4];
+  float fu_omc, fu_nk3, fu_hfx, fu_hfy, fu_fx, fu_fy, fu_g[4], fu_h[4], fu_sw[3];
   float f16_scale, f16_inv_scale;
   size_t s_size, c_size, m_size;
   void* f;
@@ -326,6 +326,9 @@ orc_state* orc_create(const orc_params* p, const uint8_t* geometry_flags) {
   }
   s->f16_scale = p->f16_scale > 0.0f ? p->f16_scale : 4096.0f;
   s->f16_inv_scale = 1.0f / s->f16_scale;
+  s->fu_sw[0] = s->f16_scale * (4.0f / 9.0f);
+  s->fu_sw[1] = s->f16_scale * (1.0f / 9.0f);
+  s->fu_sw[2] = s->f16_scale * (1.0f / 36.0f);
   switch (p->variant) {
     case ORC_F64: s->s_size = 8; s->c_size = 8; s->m_size = 8; break;
     case ORC_F32: s->s_size = 4; s->c_size = 4; s->m_size = 8; break;
