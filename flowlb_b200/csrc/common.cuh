@@ -57,6 +57,7 @@ struct KParams {
   float fu_omc, fu_nk3, fu_hfx, fu_hfy, fu_fx, fu_fy;
   float fu_g[4], fu_h[4];
   float fu_sw[3];  // FP16S deviation form: f16_scale * w for directions 0, 1..4, 5..8
+  int has_io;      // the case has inlet or outlet cells
 };
 
 __device__ __forceinline__ bool same_bits(double a, double b) {

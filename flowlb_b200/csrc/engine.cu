@@ -178,6 +178,7 @@ void refresh_params(flb_engine* h) {
   k.recon_mask = h->d_recon_mask;
   k.rho_snap = h->d_rho_snap;
   k.u_snap = h->d_u_snap;
+  k.has_io = h->has_io ? 1 : 0;
 }
 
 // Super-tile lists consumed by the step at t (built by the step before) and the
@@ -300,7 +301,7 @@ flb_status validate(const flb_case_desc* d, std::string& msg) {
   if (d->arithmetic != FLB_ARITH_REFERENCE && d->arithmetic != FLB_ARITH_FUSED)
     return msg = "arithmetic must be REFERENCE or FUSED", FLB_ERR_INVALID_ARGUMENT;
   if (d->kernel_variant < 0 || d->kernel_variant > 2) return msg = "kernel_variant must be 0, 1 or 2", FLB_ERR_INVALID_ARGUMENT;
-  if (d->kernel_variant == 2 && d->nx % (d->precision == 64 ? 2u : 4u) != 0)
+  if (d->kernel_variant == 2 && d->nx % (uint32_t)vec_width(d->precision) != 0)
     return msg = "the vector stream-collide needs nx divisible by its vector width", FLB_ERR_UNSUPPORTED;
   if (d->precision == 16) {
     const float s = d->f16_scale == 0.0f ? 4096.0f : d->f16_scale;

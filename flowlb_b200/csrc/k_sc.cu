@@ -30,8 +30,14 @@
 #ifndef FLB_VEC_MIN_BLOCKS
 #define FLB_VEC_MIN_BLOCKS 3
 #endif
+#ifndef FLB_F16_V
+#define FLB_F16_V 4  // FP16S cells per thread of the vector path (4 or 2)
+#endif
 #ifndef FLB_VEC_MIN_BLOCKS_FUSED
 #define FLB_VEC_MIN_BLOCKS_FUSED 4
+#endif
+#ifndef FLB_F16_MIN_BLOCKS
+#define FLB_F16_MIN_BLOCKS 4
 #endif
 
 namespace flb {
@@ -275,6 +281,8 @@ template <>
 struct VecT<double, 2> { using T = double2; };
 template <>
 struct VecT<__half, 4> { using T = uint2; };
+template <>
+struct VecT<__half, 2> { using T = unsigned int; };
 
 template <class S>
 struct Lanes;
@@ -283,7 +291,7 @@ struct Lanes<float> { static constexpr int V = 4; };
 template <>
 struct Lanes<double> { static constexpr int V = 2; };
 template <>
-struct Lanes<__half> { static constexpr int V = 4; };
+struct Lanes<__half> { static constexpr int V = FLB_F16_V; };
 
 template <class S, int V>
 __device__ __forceinline__ void vload(const S* ptr, S (&r)[V]) {
@@ -324,7 +332,9 @@ __device__ __forceinline__ void load_bytes(const uint8_t* ptr, uint8_t (&f)[V]) 
 constexpr int kVecBlock = 256;
 
 template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD, bool FU>
-__global__ void __launch_bounds__(kVecBlock, FU ? FLB_VEC_MIN_BLOCKS_FUSED : FLB_VEC_MIN_BLOCKS)
+__global__ void __launch_bounds__(kVecBlock, FU ? (std::is_same<S, __half>::value ? FLB_F16_MIN_BLOCKS
+                                                                                     : FLB_VEC_MIN_BLOCKS_FUSED)
+                                                    : FLB_VEC_MIN_BLOCKS)
     k_sc_vec(const __grid_constant__ KParams p) {
   constexpr int V = Lanes<S>::V;
   constexpr bool DEV = kDev<S, FS, FU>;
@@ -462,9 +472,201 @@ __global__ void __launch_bounds__(kVecBlock, FU ? FLB_VEC_MIN_BLOCKS_FUSED : FLB
   }
 }
 
+// ---- FP16S single phase, fused deviation arithmetic, binary16 pairs --------
+// The vector data path of k_sc_vec (4 cells per thread, one 8-byte access per
+// population slot) specialised for FP16S storage with collide_fused_dev: the
+// four halves of a slot stay packed in two 32-bit words, two cells are
+// converted per instruction pair (__half22float2) and packed back with one
+// conversion per two values, and the one-cell shift of the x+1 slots is a byte
+// permutation of the packed words.  Cells that are not updated (wall, gas)
+// keep their loaded halves through a per-half mask.  Used when the case has
+// no inlet or outlet cells (those need the reference expressions).
+__device__ __forceinline__ float2 h2f(uint32_t w) {
+  __half2 h;
+  memcpy(&h, &w, 4);
+  return __half22float2(h);
+}
+__device__ __forceinline__ uint32_t f2h(float lo, float hi) {
+  const __half2 h = __floats2half2_rn(lo, hi);
+  uint32_t w;
+  memcpy(&w, &h, 4);
+  return w;
+}
+// words (a, b) = halves [a0 a1 b0 b1] -> [a1 b0]
+__device__ __forceinline__ uint32_t mid(uint32_t a, uint32_t b) { return __byte_perm(a, b, 0x5432); }
+__device__ __forceinline__ uint2 ldw(const __half* base, uint32_t at) {
+  return *reinterpret_cast<const uint2*>(base + at);
+}
+__device__ __forceinline__ void stw(__half* base, uint32_t at, uint2 v) { *reinterpret_cast<uint2*>(base + at) = v; }
+
+template <bool HW, bool WM, bool ODD>
+__global__ void __launch_bounds__(kVecBlock, FLB_F16_MIN_BLOCKS) k_sc_h16(const __grid_constant__ KParams p) {
+  const uint32_t nx = p.nx, ny = p.ny;
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t x0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4u;
+  const uint32_t y = blockIdx.y;
+  const bool inrow = x0 < nx;
+  const uint32_t row = y * nx;
+  const uint32_t rowu = (y + 1u == ny ? 0u : y + 1u) * nx;
+  const uint32_t rowd = (y == 0u ? ny - 1u : y - 1u) * nx;
+  const bool tail = (lane == 31u) || (x0 + 4u >= nx);
+  const uint32_t xn = (x0 + 4u >= nx) ? 0u : x0 + 4u;
+
+  uint32_t fl = 0, nbw = 0;
+  uint2 w0 = make_uint2(0u, 0u), own[4], tmp[4], nbr[4];
+#pragma unroll
+  for (int q = 0; q < 4; q++) own[q] = tmp[q] = make_uint2(0u, 0u);
+  if (inrow) {
+    fl = *reinterpret_cast<const uint32_t*>(p.flags + row + x0);
+    w0 = ldw(slotp<__half>(p, 0), row + x0);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int i = 2 * q + 1;
+      const uint32_t r = (i == 1) ? row : (i == 7 ? rowd : rowu);
+      own[q] = ldw(slotp<__half>(p, slot_a<ODD>(i)), row + x0);
+      tmp[q] = ldw(slotp<__half>(p, slot_b<ODD>(i)), r + x0);
+    }
+    if (HW) nbw = *reinterpret_cast<const uint32_t*>(p.nbmask + row + x0);
+  }
+  bool act[4];
+  bool any = false;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    act[k] = inrow && !((fl >> (8 * k)) & (kGas | kWall));
+    any |= act[k];
+  }
+  if (!__any_sync(0xffffffffu, any)) return;
+  // realign the x+1 slots: element k of nbr is cell x0+k+1
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int i = 2 * q + 1;
+    if (i == 3) {
+      nbr[q] = tmp[q];
+    } else {
+      const uint32_t r = (i == 1) ? row : (i == 7 ? rowd : rowu);
+      uint32_t nxt = __shfl_down_sync(0xffffffffu, tmp[q].x, 1);
+      if (tail && inrow) nxt = (uint32_t)__half_as_ushort(slotp<__half>(p, slot_b<ODD>(i))[r + xn]);
+      nbr[q].x = mid(tmp[q].x, tmp[q].y);
+      nbr[q].y = mid(tmp[q].y, nxt);
+    }
+  }
+  const float invS = p.f16_inv;
+  // two cells (2P, 2P+1) per pass: the low and high halves of word P
+#pragma unroll
+  for (int P = 0; P < 2; P++) {
+    float ha[9], hb[9];
+    {
+      const float2 v = h2f(P ? w0.y : w0.x);
+      ha[0] = v.x;
+      hb[0] = v.y;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int i = 2 * q + 1;
+      const float2 vo = h2f(P ? own[q].y : own[q].x);
+      const float2 vn = h2f(P ? nbr[q].y : nbr[q].x);
+      ha[i] = vo.x;
+      hb[i] = vo.y;
+      ha[i + 1] = vn.x;
+      hb[i + 1] = vn.y;
+    }
+    if (HW) {
+      // half-way walls: reflected populations, scalar (wall-adjacent cells only)
+#pragma unroll
+      for (int c = 0; c < 2; c++) {
+        const int k = 2 * P + c;
+        const uint32_t nbm = (nbw >> (8 * k)) & 0xffu;
+        if (act[k] && nbm) {
+          float* h = c ? hb : ha;
+          const uint32_t x = x0 + k, idx = row + x;
+          uint32_t nb[9];
+          neighbours(x, y, nx, ny, nb);
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const int i = 2 * q + 1;
+            if ((nbm >> i) & 1u) h[i] = RawHalf::ld(slotp<__half>(p, slot_b<ODD>(i)), idx, i, invS);
+            if ((nbm >> (i - 1)) & 1u) h[i + 1] = RawHalf::ld(slotp<__half>(p, slot_a<ODD>(i)), nb[i], i + 1, invS);
+          }
+        }
+      }
+    }
+    const DevOut oa = collide_fused_dev(ha, invS, p.inv_tau, p.fu_omc, p.fu_nk3, p.fu_hfx, p.fu_hfy, p.fu_fx, p.fu_fy,
+                                        p.u_max, p.fu_g, p.fu_h, p.fu_sw);
+    const DevOut ob = collide_fused_dev(hb, invS, p.inv_tau, p.fu_omc, p.fu_nk3, p.fu_hfx, p.fu_hfy, p.fu_fx, p.fu_fy,
+                                        p.u_max, p.fu_g, p.fu_h, p.fu_sw);
+    if (WM) {
+      float* R = static_cast<float*>(p.rho);
+      float* U = static_cast<float*>(p.u);
+      const uint32_t idx = row + x0 + 2 * P;
+      if (act[2 * P]) {
+        R[idx] = oa.rho;
+        U[idx] = oa.ux;
+        U[idx + p.N] = oa.uy;
+      }
+      if (act[2 * P + 1]) {
+        R[idx + 1] = ob.rho;
+        U[idx + 1] = ob.ux;
+        U[idx + 1 + p.N] = ob.uy;
+      }
+    }
+    // computed halves where the cell is updated, loaded ones elsewhere
+    const uint32_t m = (act[2 * P] ? 0x0000ffffu : 0u) | (act[2 * P + 1] ? 0xffff0000u : 0u);
+    auto put = [m](uint32_t& w, uint32_t v) { w = (v & m) | (w & ~m); };
+    if (P) put(w0.y, f2h(ha[0], hb[0]));
+    else put(w0.x, f2h(ha[0], hb[0]));
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int i = 2 * q + 1;
+      // post f_i -> neighbour slot b (nbr), post f_{i+1} -> own slot a (own)
+      if (P) {
+        put(nbr[q].y, f2h(ha[i], hb[i]));
+        put(own[q].y, f2h(ha[i + 1], hb[i + 1]));
+      } else {
+        put(nbr[q].x, f2h(ha[i], hb[i]));
+        put(own[q].x, f2h(ha[i + 1], hb[i + 1]));
+      }
+    }
+  }
+
+  // ---- stores ------------------------------------------------------------------
+  if (inrow) stw(slotp<__half>(p, 0), row + x0, w0);
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int i = 2 * q + 1;
+    if (inrow) stw(slotp<__half>(p, slot_a<ODD>(i)), row + x0, own[q]);
+    const uint32_t r = (i == 1) ? row : (i == 7 ? rowd : rowu);
+    __half* dst = slotp<__half>(p, slot_b<ODD>(i)) + r;
+    if (i == 3) {
+      if (inrow) stw(dst, x0, nbr[q]);
+    } else {
+      const uint32_t prev = __shfl_up_sync(0xffffffffu, nbr[q].y, 1);
+      if (inrow) {
+        if (lane != 0u) {
+          stw(dst, x0, make_uint2(mid(prev, nbr[q].x), mid(nbr[q].x, nbr[q].y)));
+        } else {
+          // x0 belongs to the previous warp's last lane
+          dst[x0 + 1] = __ushort_as_half((unsigned short)(nbr[q].x & 0xffffu));
+          *reinterpret_cast<uint32_t*>(dst + x0 + 2) = mid(nbr[q].x, nbr[q].y);
+        }
+        if (tail) dst[xn] = __ushort_as_half((unsigned short)(nbr[q].y >> 16));
+      }
+    }
+  }
+}
+
 // ---- launchers -------------------------------------------------------------------
 template <class S, class C, class M, bool FS, bool HW, bool WM, bool FU>
 static void launch_sc_t(const KParams& kp, cudaStream_t st, uint32_t odd, bool vec) {
+  if constexpr (kDev<S, FS, FU>) {
+    if (vec && !kp.has_io) {
+      const uint32_t per_row = kp.nx / 4u;
+      const uint32_t block = per_row >= (uint32_t)kVecBlock ? (uint32_t)kVecBlock : ((per_row + 31u) / 32u) * 32u;
+      const dim3 g((per_row + block - 1) / block, kp.ny);
+      if (odd) k_sc_h16<HW, WM, true><<<g, block, 0, st>>>(kp);
+      else k_sc_h16<HW, WM, false><<<g, block, 0, st>>>(kp);
+      return;
+    }
+  }
   if (vec) {
     constexpr int V = Lanes<S>::V;
     const uint32_t per_row = kp.nx / V;
@@ -499,7 +701,9 @@ void launch_sc(const KParams& kp, cudaStream_t st, uint32_t odd, bool fs, bool h
   else launch_sc_f<S, C, M, false>(kp, st, odd, fs, hw, wm, vec);
 }
 
-int vec_width(int precision) { return precision == 64 ? Lanes<double>::V : Lanes<float>::V; }
+int vec_width(int precision) {
+  return precision == 64 ? Lanes<double>::V : (precision == 16 ? Lanes<__half>::V : Lanes<float>::V);
+}
 
 template <class S, class C, class M, bool FU>
 static void launch_sc_list_f(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl,

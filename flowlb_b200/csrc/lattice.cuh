@@ -155,6 +155,9 @@ __device__ __forceinline__ void limit_u(float umax, C& ux, C& uy) {
 // restatement with fma()/fmaf() matches bit for bit.
 __device__ __forceinline__ float fmac(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double fmac(double a, double b, double c) { return __fma_rn(a, b, c); }
+// correctly rounded 1/x (the same value as 1/x with IEEE division)
+__device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+__device__ __forceinline__ double rcp(double x) { return __drcp_rn(x); }
 
 // Density, momentum and 1/rho in the fused form (pairwise sums).
 template <class C>
@@ -164,7 +167,7 @@ __device__ __forceinline__ void moments_fused(const C* f, C& rho, C& jx, C& jy, 
   rho = ((f[0] + s12) + (s34 + s56)) + s78;
   jx = (d12 + d56) + d78;
   jy = (d34 + d56) - d78;
-  inv = C(1) / rho;
+  inv = rcp(rho);
 }
 
 // The relaxation with forcing, from the force-shifted (and limited) velocity.
@@ -209,7 +212,7 @@ __device__ __forceinline__ DevOut collide_fused_dev(float* h, float invS, float 
   const float jx = (d12 + d56) + d78, jy = (d34 + d56) - d78;
   const float delta = dS * invS;
   const float rho = fmac(dS, invS, 1.0f);
-  const float inv = 1.0f / rho;
+  const float inv = rcp(rho);
   const float invs = inv * invS;
   float ux = fmac(hfx, inv, jx * invs);
   float uy = fmac(hfy, inv, jy * invs);
