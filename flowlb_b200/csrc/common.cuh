@@ -58,7 +58,21 @@ struct KParams {
   float fu_g[4], fu_h[4];
   float fu_sw[3];  // FP16S deviation form: f16_scale * w for directions 0, 1..4, 5..8
   int has_io;      // the case has inlet or outlet cells
+  // time step of the FP16S dithered rounding: the step with parity q reads
+  // tstep[q] and writes tstep[q ^ 1] = t + 1 (graph replays see the current t)
+  uint32_t* tstep;
+  // single phase: chunk map of plain fluid cells, 4 cells per bit (k_plain_chunks); null otherwise
+  const uint32_t* plain;
 };
+
+// Whether the n*4 cells from cell c (a multiple of 4n, n = 1 or 2) are all
+// plain fluid cells with no wall neighbour.
+template <int n>
+__device__ __forceinline__ bool plain_cells(const uint32_t* plain, uint32_t c) {
+  const uint32_t word = plain[c >> 7], bit = (c >> 2) & 31u;
+  constexpr uint32_t m = (1u << n) - 1u;
+  return ((word >> bit) & m) == m;
+}
 
 __device__ __forceinline__ bool same_bits(double a, double b) {
   return __double_as_longlong(a) == __double_as_longlong(b);

@@ -78,6 +78,8 @@ struct flb_engine {
   double* d_partial = nullptr;
   double* d_scalar = nullptr;
   unsigned long long* d_counts = nullptr;
+  uint32_t* d_tstep = nullptr;  // [2] time step by parity (FP16S dithered rounding)
+  uint32_t* d_plain = nullptr;  // single phase: plain-fluid chunk map (k_plain_chunks)
   GraphSlot g_pair, g_big;
   std::string err;
 };
@@ -179,6 +181,23 @@ void refresh_params(flb_engine* h) {
   k.rho_snap = h->d_rho_snap;
   k.u_snap = h->d_u_snap;
   k.has_io = h->has_io ? 1 : 0;
+  k.tstep = h->d_tstep;
+  k.plain = h->d_plain;
+}
+
+// Rebuilds the single-phase plain-fluid chunk map from the current flags.
+void refresh_plain(flb_engine* h) {
+  if (h->fs || !h->d_plain) return;
+  launch_plain_chunks(h->d_flags[h->cur], h->hw ? h->d_nbmask : nullptr, h->N, h->d_plain, h->stream);
+  h->launches++;
+}
+
+// Sets the device time-step counter to t (its parity slot).
+flb_status set_tstep(flb_engine* h) {
+  const uint32_t t32 = (uint32_t)h->t;
+  FLB_CUDA(h, cudaMemcpyAsync(h->d_tstep + (h->t & 1u), &t32, sizeof(t32), cudaMemcpyHostToDevice, h->stream));
+  FLB_CUDA(h, cudaStreamSynchronize(h->stream));
+  return FLB_OK;
 }
 
 // Super-tile lists consumed by the step at t (built by the step before) and the
@@ -273,7 +292,8 @@ void free_all(flb_engine* h) {
                   h->d_geo,        h->d_nbmask,      h->d_mass,        h->d_excess,      h->d_phi,
                   h->d_recon,      h->d_recon_mask,  h->d_rho_snap,    h->d_u_snap,      h->d_partial,
                   h->d_scalar,     h->d_counts,      h->d_nz,          h->d_nz_prev,     h->d_list[0][0],
-                  h->d_list[0][1], h->d_list[1][0],  h->d_list[1][1],  h->d_lcount};
+                  h->d_list[0][1], h->d_list[1][0],  h->d_list[1][1],  h->d_lcount,     h->d_tstep,
+                  h->d_plain};
   for (void* p : bufs)
     if (p) cudaFree(p);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -341,6 +361,8 @@ flb_status initialise(flb_engine* h) {
   h->launches++;
   if (h->fs) FLB_CUDA(h, cudaMemcpyAsync(h->d_flags[1], h->d_flags[0], h->N, cudaMemcpyDeviceToDevice, h->stream));
   if (h->d_recon_mask) FLB_CUDA(h, cudaMemsetAsync(h->d_recon_mask, 0, h->N, h->stream));
+  FLB_CUDA(h, cudaMemsetAsync(h->d_tstep, 0, 2 * sizeof(uint32_t), h->stream));
+  refresh_plain(h);
   h->trust = true;  // flags[1] = flags[0] and the initial fields satisfy the skip invariants
   h->lists_valid = false;
   FLB_CUDA(h, cudaGetLastError());
@@ -461,6 +483,8 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
       {(void**)&h->d_partial, blocks * sizeof(double), true},
       {(void**)&h->d_scalar, sizeof(double), true},
       {(void**)&h->d_counts, 8 * sizeof(unsigned long long), true},
+      {(void**)&h->d_tstep, 2 * sizeof(uint32_t), true},
+      {(void**)&h->d_plain, (((size_t)N + 3) / 4 + 31) / 32 * sizeof(uint32_t), !h->fs},
       {(void**)&h->d_nz, tiles * sizeof(uint32_t), h->fs},
       {(void**)&h->d_nz_prev, tiles * sizeof(uint32_t), h->fs},
       {(void**)&h->d_list[0][0], tiles * sizeof(uint32_t), h->fs},
@@ -728,6 +752,7 @@ FLB_API flb_status flb_write_field(flb_handle h, int field, const void* src, int
   } else {
     FLB_CUDA(h, cudaMemcpyAsync(dst, src, bytes, kind, h->stream));
   }
+  if (field == FLB_FIELD_FLAGS) refresh_plain(h);
   h->trust = false;
   h->lists_valid = false;
   FLB_CUDA(h, cudaStreamSynchronize(h->stream));
@@ -980,7 +1005,8 @@ FLB_API flb_status flb_load_checkpoint(flb_handle h, const char* path) {
   h->trust = false;
   h->lists_valid = false;
   refresh_params(h);
-  return FLB_OK;
+  refresh_plain(h);
+  return set_tstep(h);
 }
 
 FLB_API const char* flb_last_error(flb_handle h) { return h ? h->err.c_str() : "null handle"; }

@@ -84,6 +84,31 @@ __global__ void k_nbmask(const uint8_t* __restrict__ flags, uint8_t* __restrict_
   nbmask[x + y * nx] = (uint8_t)m;
 }
 
+// Single-phase chunk map: bit c % 32 of plain[c / 32] is set when the four
+// cells 4c..4c+3 are all plain FLUID (no inlet, outlet, wall or gas) with no
+// wall neighbour, so that the vector stream-collide can skip reading their
+// flag and neighbour-mask bytes.  nbmask may be null (no half-way walls).
+__global__ void k_plain_chunks(const uint8_t* __restrict__ flags, const uint8_t* __restrict__ nbmask, uint32_t N,
+                               uint32_t* __restrict__ plain) {
+  const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t nchunk = (N + 3u) / 4u;
+  bool pl = c < nchunk;
+  if (pl) {
+#pragma unroll
+    for (uint32_t k = 0; k < 4; k++) {
+      const uint32_t cell = 4u * c + k;
+      pl = pl && cell < N && flags[cell] == kFluid && (!nbmask || nbmask[cell] == 0);
+    }
+  }
+  const uint32_t b = __ballot_sync(0xffffffffu, pl);
+  if ((threadIdx.x & 31u) == 0u && c < nchunk) plain[c >> 5] = b;
+}
+
+void launch_plain_chunks(const uint8_t* flags, const uint8_t* nbmask, uint32_t N, uint32_t* plain, cudaStream_t st) {
+  const uint32_t nchunk = (N + 3u) / 4u;
+  k_plain_chunks<<<(nchunk + kBlock - 1) / kBlock, kBlock, 0, st>>>(flags, nbmask, N, plain);
+}
+
 // f = feq(rho=1, u) with the host's double arithmetic (initEquilibriumDDF2Q9,
 // initData.h:75-100) stored with the t=1 pattern (initData.h:102-112, :155);
 // rho = 1; u = inlet velocity on INLET cells, else 0 (initData.h:125-148).

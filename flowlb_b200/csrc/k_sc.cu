@@ -49,9 +49,10 @@ namespace flb {
 // FU: the fused SRT arithmetic (collide_fused) for cells that are neither inlet
 // nor outlet; the host selects it only for SRT without the subgrid model.
 // DEV: f holds FP16S deviations h = (f - w) * scale (single phase with FU).
+// tnow: the time step (DEV only, for the dithered rounding).
 template <class C, class M, bool FS, bool WM, bool FU, bool DEV = false>
 __device__ __forceinline__ void collide_cell(const KParams& p, uint32_t idx, uint32_t x, uint32_t y, uint8_t flag,
-                                             uint32_t nbm, C* f) {
+                                             uint32_t nbm, C* f, uint32_t tnow = 0u) {
   const uint32_t N = p.N;
   if constexpr (DEV) {
     if (flag & (kInlet | kOutlet)) {
@@ -61,15 +62,18 @@ __device__ __forceinline__ void collide_cell(const KParams& p, uint32_t idx, uin
       collide_cell<C, M, FS, WM, false, false>(p, idx, x, y, flag, nbm, f);
 #pragma unroll
       for (int i = 0; i < 9; i++) f[i] = (f[i] - wgt<C>(i)) * p.f16_scale;
-      return;
+    } else {
+      const DevOut o = collide_fused_dev(f, p.f16_inv, p.inv_tau, p.fu_omc, p.fu_nk3, p.fu_hfx, p.fu_hfy, p.fu_fx,
+                                         p.fu_fy, p.u_max, p.fu_g, p.fu_h, p.fu_sw);
+      if (WM) {
+        static_cast<C*>(p.u)[idx] = o.ux;
+        static_cast<C*>(p.u)[idx + N] = o.uy;
+        static_cast<C*>(p.rho)[idx] = o.rho;
+      }
     }
-    const DevOut o = collide_fused_dev(f, p.f16_inv, p.inv_tau, p.fu_omc, p.fu_nk3, p.fu_hfx, p.fu_hfy, p.fu_fx,
-                                       p.fu_fy, p.u_max, p.fu_g, p.fu_h, p.fu_sw);
-    if (WM) {
-      static_cast<C*>(p.u)[idx] = o.ux;
-      static_cast<C*>(p.u)[idx + N] = o.uy;
-      static_cast<C*>(p.rho)[idx] = o.rho;
-    }
+    const uint32_t base = f16_dither_base(idx, tnow);
+#pragma unroll
+    for (int i = 0; i < 9; i++) f[i] = f16_dithered(f[i], f16_dither(base, i));
     return;
   }
   if constexpr (FS) {
@@ -243,7 +247,7 @@ __device__ __forceinline__ void sc_cell(const KParams& p, uint32_t x, uint32_t y
     if (HW) nbm = p.nbmask[idx];
     load_in<S, C, HW, ODD, K>(p, idx, nb, nbm, f);
   }
-  collide_cell<C, M, FS, WM, FU, DEV>(p, idx, x, y, flag, nbm, f);
+  collide_cell<C, M, FS, WM, FU, DEV>(p, idx, x, y, flag, nbm, f, DEV ? p.tstep[ODD] : 0u);
   store_post<S, C, ODD, K>(p, idx, nb, f);
 }
 
@@ -251,6 +255,7 @@ template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD, bool F
 __global__ void __launch_bounds__(kBlock, FLB_SC_MIN_BLOCKS) k_sc_scalar(const __grid_constant__ KParams p) {
   const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x;
   const uint32_t y = blockIdx.y;
+  if (kDev<S, FS, FU> && x == 0 && y == 0) p.tstep[!ODD] = p.tstep[ODD] + 1u;
   if (x >= p.nx) return;
   sc_cell<S, C, M, FS, HW, WM, ODD, FU>(p, x, y);
 }
@@ -349,12 +354,20 @@ __global__ void __launch_bounds__(kVecBlock, FU ? (std::is_same<S, __half>::valu
   const uint32_t rowd = (y == 0u ? ny - 1u : y - 1u) * nx;
   const bool tail = (lane == 31u) || (x0 + V >= nx);  // the cell past this lane is not the next lane's
   const uint32_t xn = (x0 + V >= nx) ? 0u : x0 + V;   // position past this lane (periodic wrap)
+  if (DEV && x0 == 0 && y == 0) p.tstep[!ODD] = p.tstep[ODD] + 1u;
 
   uint8_t fl[V];
   bool act[V];
   bool any = false;
   S raw0[V], own[4][V], nbr[4][V], tmp[4][V];
-  if (inrow) load_bytes<V>(p.flags + row + x0, fl);
+  bool plain = false;  // single phase: all V cells plain fluid, flag and mask bytes not read
+  if constexpr (!FS && V == 4) plain = inrow && p.plain && plain_cells<1>(p.plain, row + x0);
+  if (plain) {
+#pragma unroll
+    for (int k = 0; k < V; k++) fl[k] = kFluid;
+  } else if (inrow) {
+    load_bytes<V>(p.flags + row + x0, fl);
+  }
   if constexpr (!FS) {
     // single phase: load the populations with the flags
     if (inrow) {
@@ -405,7 +418,7 @@ __global__ void __launch_bounds__(kVecBlock, FU ? (std::is_same<S, __half>::valu
   uint8_t nbmv[V];
 #pragma unroll
   for (int k = 0; k < V; k++) nbmv[k] = 0;
-  if (HW && inrow) load_bytes<V>(p.nbmask + row + x0, nbmv);
+  if (HW && inrow && !plain) load_bytes<V>(p.nbmask + row + x0, nbmv);
 
   // ---- per-cell collision; cells not updated keep their raw values ---------
 #pragma unroll
@@ -433,7 +446,7 @@ __global__ void __launch_bounds__(kVecBlock, FU ? (std::is_same<S, __half>::valu
         if ((nbm >> (i - 1)) & 1u) f[i + 1] = K::ld(slotp<S>(p, slot_a<ODD>(i)), nb[i], i + 1, p.f16_inv);
       }
     }
-    collide_cell<C, M, FS, WM, FU, DEV>(p, idx, x, y, fl[k], nbm, f);
+    collide_cell<C, M, FS, WM, FU, DEV>(p, idx, x, y, fl[k], nbm, f, DEV ? p.tstep[ODD] : 0u);
     K::st(raw0, k, 0, f[0], p.f16_scale);
 #pragma unroll
     for (int q = 0; q < 4; q++) {
@@ -473,69 +486,123 @@ __global__ void __launch_bounds__(kVecBlock, FU ? (std::is_same<S, __half>::valu
 }
 
 // ---- FP16S single phase, fused deviation arithmetic, binary16 pairs --------
-// The vector data path of k_sc_vec (4 cells per thread, one 8-byte access per
-// population slot) specialised for FP16S storage with collide_fused_dev: the
-// four halves of a slot stay packed in two 32-bit words, two cells are
-// converted per instruction pair (__half22float2) and packed back with one
-// conversion per two values, and the one-cell shift of the x+1 slots is a byte
-// permutation of the packed words.  Cells that are not updated (wall, gas)
-// keep their loaded halves through a per-half mask.  Used when the case has
-// no inlet or outlet cells (those need the reference expressions).
+// The vector data path of k_sc_vec specialised for FP16S storage with
+// collide_fused_dev: 2W cells per thread, the 2W halves of a population slot
+// moved with one 4W-byte access and kept packed in W 32-bit words; two cells
+// are converted per instruction pair (__half22float2) and packed back with one
+// conversion per two values, and the one-cell shift of the x+1 slots is a
+// byte permutation of the packed words.  Cells that are not updated (wall,
+// gas) keep their loaded halves through a per-half mask.  Used when the case
+// has no inlet or outlet cells (those need the reference expressions).
+#ifndef FLB_H16_WORDS
+#define FLB_H16_WORDS 4  // 32-bit words (cell pairs) per thread and slot: 8 cells
+#endif
+// measured on a B200 (8192x2048): 128-thread blocks, 6 per SM (80 registers),
+// 157 GLUPS; 256 x 3: 149; 64 x 12: 157; 512 x 1: 116; a persistent
+// grid-stride loop over row chunks: 135; evict-first cache hints on the slot
+// accesses: -9 %; the slots staged in shared memory by bulk async copies
+// (cp.async.bulk, two stages, 2 blocks per SM): 135
+#ifndef FLB_H16_BLOCK
+#define FLB_H16_BLOCK 128
+#endif
+#ifndef FLB_H16_MIN_BLOCKS
+#define FLB_H16_MIN_BLOCKS 6
+#endif
+// two floats -> binary16 pair, rounded toward zero (inputs dithered, f16_dither)
+__device__ __forceinline__ uint32_t f2h(float lo, float hi) {
+  uint32_t w;
+  asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(w) : "f"(hi), "f"(lo));
+  return w;
+}
 __device__ __forceinline__ float2 h2f(uint32_t w) {
   __half2 h;
   memcpy(&h, &w, 4);
   return __half22float2(h);
 }
-__device__ __forceinline__ uint32_t f2h(float lo, float hi) {
-  const __half2 h = __floats2half2_rn(lo, hi);
-  uint32_t w;
-  memcpy(&w, &h, 4);
-  return w;
-}
 // words (a, b) = halves [a0 a1 b0 b1] -> [a1 b0]
 __device__ __forceinline__ uint32_t mid(uint32_t a, uint32_t b) { return __byte_perm(a, b, 0x5432); }
-__device__ __forceinline__ uint2 ldw(const __half* base, uint32_t at) {
-  return *reinterpret_cast<const uint2*>(base + at);
-}
-__device__ __forceinline__ void stw(__half* base, uint32_t at, uint2 v) { *reinterpret_cast<uint2*>(base + at) = v; }
 
-template <bool HW, bool WM, bool ODD>
-__global__ void __launch_bounds__(kVecBlock, FLB_F16_MIN_BLOCKS) k_sc_h16(const __grid_constant__ KParams p) {
+template <int W>
+struct Words {
+  uint32_t w[W];
+};
+template <int W>
+__device__ __forceinline__ Words<W> ldw(const void* base, uint32_t at_bytes) {
+  Words<W> r;
+  const char* q = static_cast<const char*>(base) + at_bytes;
+  if constexpr (W == 1) {
+    r.w[0] = *reinterpret_cast<const uint32_t*>(q);
+  } else if constexpr (W == 2) {
+    const uint2 v = *reinterpret_cast<const uint2*>(q);
+    r.w[0] = v.x; r.w[1] = v.y;
+  } else {
+    const uint4 v = *reinterpret_cast<const uint4*>(q);
+    r.w[0] = v.x; r.w[1] = v.y; r.w[2] = v.z; r.w[3] = v.w;
+  }
+  return r;
+}
+template <int W>
+__device__ __forceinline__ void stw(void* base, uint32_t at_bytes, const Words<W>& r) {
+  char* q = static_cast<char*>(base) + at_bytes;
+  if constexpr (W == 2) *reinterpret_cast<uint2*>(q) = make_uint2(r.w[0], r.w[1]);
+  else *reinterpret_cast<uint4*>(q) = make_uint4(r.w[0], r.w[1], r.w[2], r.w[3]);
+}
+
+// V = 2W cells from (x0, y); every lane of the warp calls it with the same y.
+// LIM: the velocity limiter is on.
+template <bool HW, bool WM, bool ODD, bool LIM>
+__device__ __forceinline__ void h16_cells(const KParams& p, const uint32_t x0, const uint32_t y) {
+  constexpr int W = FLB_H16_WORDS, V = 2 * W;
   const uint32_t nx = p.nx, ny = p.ny;
   const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t x0 = (blockIdx.x * blockDim.x + threadIdx.x) * 4u;
-  const uint32_t y = blockIdx.y;
   const bool inrow = x0 < nx;
   const uint32_t row = y * nx;
   const uint32_t rowu = (y + 1u == ny ? 0u : y + 1u) * nx;
   const uint32_t rowd = (y == 0u ? ny - 1u : y - 1u) * nx;
-  const bool tail = (lane == 31u) || (x0 + 4u >= nx);
-  const uint32_t xn = (x0 + 4u >= nx) ? 0u : x0 + 4u;
+  const bool tail = (lane == 31u) || (x0 + V >= nx);
+  const uint32_t xn = (x0 + V >= nx) ? 0u : x0 + V;
+  const uint32_t at = (row + x0) * 2u;  // byte offset of this thread's cells in a slot
 
-  uint32_t fl = 0, nbw = 0;
-  uint2 w0 = make_uint2(0u, 0u), own[4], tmp[4], nbr[4];
+  Words<W / 2> flw{}, nbmw{};  // V flag / neighbour-mask bytes
+  Words<W> w0{}, own[4], tmp[4], nbr[4];
 #pragma unroll
-  for (int q = 0; q < 4; q++) own[q] = tmp[q] = make_uint2(0u, 0u);
+  for (int q = 0; q < 4; q++) own[q] = tmp[q] = Words<W>{};
+  bool plain = false;  // all V cells plain fluid: flag and mask bytes not read
   if (inrow) {
-    fl = *reinterpret_cast<const uint32_t*>(p.flags + row + x0);
-    w0 = ldw(slotp<__half>(p, 0), row + x0);
+    // the population loads first: the chunk-map word must not delay them
+    w0 = ldw<W>(p.slot[0], at);
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const int i = 2 * q + 1;
       const uint32_t r = (i == 1) ? row : (i == 7 ? rowd : rowu);
-      own[q] = ldw(slotp<__half>(p, slot_a<ODD>(i)), row + x0);
-      tmp[q] = ldw(slotp<__half>(p, slot_b<ODD>(i)), r + x0);
+      own[q] = ldw<W>(p.slot[slot_a<ODD>(i)], at);
+      tmp[q] = ldw<W>(p.slot[slot_b<ODD>(i)], (r + x0) * 2u);
     }
-    if (HW) nbw = *reinterpret_cast<const uint32_t*>(p.nbmask + row + x0);
+    plain = p.plain && plain_cells<V / 4>(p.plain, row + x0);
+    if (plain) {
+#pragma unroll
+      for (int j = 0; j < W / 2; j++) flw.w[j] = 0x01010101u;
+    } else {
+      flw = ldw<W / 2>(p.flags, row + x0);
+    }
+    if (HW && !plain) nbmw = ldw<W / 2>(p.nbmask, row + x0);
   }
-  bool act[4];
+  // per-half masks of the updated cells (0xffff: not gas, not wall), pair P
+  // in word P; a lane past the row end updates nothing
+  uint32_t upd[W];
   bool any = false;
 #pragma unroll
-  for (int k = 0; k < 4; k++) {
-    act[k] = inrow && !((fl >> (8 * k)) & (kGas | kWall));
-    any |= act[k];
+  for (int P = 0; P < W; P++) {
+    const uint32_t two = __byte_perm(flw.w[P >> 1], 0u, (P & 1) ? 0x3322u : 0x1100u);  // bytes k, k, k+1, k+1
+    upd[P] = inrow ? __vcmpeq4(two & 0x0a0a0a0au, 0u) : 0u;
+    any |= upd[P] != 0u;
   }
   if (!__any_sync(0xffffffffu, any)) return;
+  bool walls = false;  // some cell of this thread has a wall neighbour
+  if (HW) {
+#pragma unroll
+    for (int j = 0; j < W / 2; j++) walls |= nbmw.w[j] != 0u;
+  }
   // realign the x+1 slots: element k of nbr is cell x0+k+1
 #pragma unroll
   for (int q = 0; q < 4; q++) {
@@ -544,39 +611,41 @@ __global__ void __launch_bounds__(kVecBlock, FLB_F16_MIN_BLOCKS) k_sc_h16(const 
       nbr[q] = tmp[q];
     } else {
       const uint32_t r = (i == 1) ? row : (i == 7 ? rowd : rowu);
-      uint32_t nxt = __shfl_down_sync(0xffffffffu, tmp[q].x, 1);
+      uint32_t nxt = __shfl_down_sync(0xffffffffu, tmp[q].w[0], 1);
       if (tail && inrow) nxt = (uint32_t)__half_as_ushort(slotp<__half>(p, slot_b<ODD>(i))[r + xn]);
-      nbr[q].x = mid(tmp[q].x, tmp[q].y);
-      nbr[q].y = mid(tmp[q].y, nxt);
+#pragma unroll
+      for (int j = 0; j < W - 1; j++) nbr[q].w[j] = mid(tmp[q].w[j], tmp[q].w[j + 1]);
+      nbr[q].w[W - 1] = mid(tmp[q].w[W - 1], nxt);
     }
   }
   const float invS = p.f16_inv;
+  const uint32_t tnow = p.tstep[ODD];
   // two cells (2P, 2P+1) per pass: the low and high halves of word P
 #pragma unroll
-  for (int P = 0; P < 2; P++) {
+  for (int P = 0; P < W; P++) {
     float ha[9], hb[9];
     {
-      const float2 v = h2f(P ? w0.y : w0.x);
+      const float2 v = h2f(w0.w[P]);
       ha[0] = v.x;
       hb[0] = v.y;
     }
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const int i = 2 * q + 1;
-      const float2 vo = h2f(P ? own[q].y : own[q].x);
-      const float2 vn = h2f(P ? nbr[q].y : nbr[q].x);
+      const float2 vo = h2f(own[q].w[P]);
+      const float2 vn = h2f(nbr[q].w[P]);
       ha[i] = vo.x;
       hb[i] = vo.y;
       ha[i + 1] = vn.x;
       hb[i + 1] = vn.y;
     }
-    if (HW) {
+    if (HW && walls) {
       // half-way walls: reflected populations, scalar (wall-adjacent cells only)
 #pragma unroll
       for (int c = 0; c < 2; c++) {
         const int k = 2 * P + c;
-        const uint32_t nbm = (nbw >> (8 * k)) & 0xffu;
-        if (act[k] && nbm) {
+        const uint32_t nbm = (nbmw.w[k >> 2] >> (8 * (k & 3))) & 0xffu;
+        if (((upd[P] >> (16 * c)) & 1u) && nbm) {
           float* h = c ? hb : ha;
           const uint32_t x = x0 + k, idx = row + x;
           uint32_t nb[9];
@@ -590,80 +659,103 @@ __global__ void __launch_bounds__(kVecBlock, FLB_F16_MIN_BLOCKS) k_sc_h16(const 
         }
       }
     }
-    const DevOut oa = collide_fused_dev(ha, invS, p.inv_tau, p.fu_omc, p.fu_nk3, p.fu_hfx, p.fu_hfy, p.fu_fx, p.fu_fy,
-                                        p.u_max, p.fu_g, p.fu_h, p.fu_sw);
-    const DevOut ob = collide_fused_dev(hb, invS, p.inv_tau, p.fu_omc, p.fu_nk3, p.fu_hfx, p.fu_hfy, p.fu_fx, p.fu_fy,
-                                        p.u_max, p.fu_g, p.fu_h, p.fu_sw);
+    const DevOut oa = collide_fused_dev<LIM>(ha, invS, p.inv_tau, p.fu_omc, p.fu_nk3, p.fu_hfx, p.fu_hfy, p.fu_fx,
+                                             p.fu_fy, p.u_max, p.fu_g, p.fu_h, p.fu_sw);
+    const DevOut ob = collide_fused_dev<LIM>(hb, invS, p.inv_tau, p.fu_omc, p.fu_nk3, p.fu_hfx, p.fu_hfy, p.fu_fx,
+                                             p.fu_fy, p.u_max, p.fu_g, p.fu_h, p.fu_sw);
+    const uint32_t idx = row + x0 + 2 * P;
     if (WM) {
       float* R = static_cast<float*>(p.rho);
       float* U = static_cast<float*>(p.u);
-      const uint32_t idx = row + x0 + 2 * P;
-      if (act[2 * P]) {
+      if (upd[P] & 1u) {
         R[idx] = oa.rho;
         U[idx] = oa.ux;
         U[idx + p.N] = oa.uy;
       }
-      if (act[2 * P + 1]) {
+      if (upd[P] >> 16) {
         R[idx + 1] = ob.rho;
         U[idx + 1] = ob.ux;
         U[idx + 1 + p.N] = ob.uy;
       }
     }
+    {
+      const uint32_t ba = f16_dither_base(idx, tnow), bb = f16_dither_base(idx + 1u, tnow);
+#pragma unroll
+      for (int i = 0; i < 9; i++) {
+        ha[i] = f16_dithered(ha[i], f16_dither(ba, i));
+        hb[i] = f16_dithered(hb[i], f16_dither(bb, i));
+      }
+    }
     // computed halves where the cell is updated, loaded ones elsewhere
-    const uint32_t m = (act[2 * P] ? 0x0000ffffu : 0u) | (act[2 * P + 1] ? 0xffff0000u : 0u);
+    const uint32_t m = upd[P];
     auto put = [m](uint32_t& w, uint32_t v) { w = (v & m) | (w & ~m); };
-    if (P) put(w0.y, f2h(ha[0], hb[0]));
-    else put(w0.x, f2h(ha[0], hb[0]));
+    put(w0.w[P], f2h(ha[0], hb[0]));
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const int i = 2 * q + 1;
-      // post f_i -> neighbour slot b (nbr), post f_{i+1} -> own slot a (own)
-      if (P) {
-        put(nbr[q].y, f2h(ha[i], hb[i]));
-        put(own[q].y, f2h(ha[i + 1], hb[i + 1]));
-      } else {
-        put(nbr[q].x, f2h(ha[i], hb[i]));
-        put(own[q].x, f2h(ha[i + 1], hb[i + 1]));
-      }
+      put(nbr[q].w[P], f2h(ha[i], hb[i]));          // post f_i -> neighbour slot b
+      put(own[q].w[P], f2h(ha[i + 1], hb[i + 1]));  // post f_{i+1} -> own slot a
     }
   }
 
   // ---- stores ------------------------------------------------------------------
-  if (inrow) stw(slotp<__half>(p, 0), row + x0, w0);
+  if (inrow) stw<W>(p.slot[0], at, w0);
 #pragma unroll
   for (int q = 0; q < 4; q++) {
     const int i = 2 * q + 1;
-    if (inrow) stw(slotp<__half>(p, slot_a<ODD>(i)), row + x0, own[q]);
+    if (inrow) stw<W>(p.slot[slot_a<ODD>(i)], at, own[q]);
     const uint32_t r = (i == 1) ? row : (i == 7 ? rowd : rowu);
     __half* dst = slotp<__half>(p, slot_b<ODD>(i)) + r;
     if (i == 3) {
-      if (inrow) stw(dst, x0, nbr[q]);
+      if (inrow) stw<W>(dst, x0 * 2u, nbr[q]);
     } else {
-      const uint32_t prev = __shfl_up_sync(0xffffffffu, nbr[q].y, 1);
+      const uint32_t prev = __shfl_up_sync(0xffffffffu, nbr[q].w[W - 1], 1);
       if (inrow) {
         if (lane != 0u) {
-          stw(dst, x0, make_uint2(mid(prev, nbr[q].x), mid(nbr[q].x, nbr[q].y)));
+          Words<W> o;
+          o.w[0] = mid(prev, nbr[q].w[0]);
+#pragma unroll
+          for (int j = 1; j < W; j++) o.w[j] = mid(nbr[q].w[j - 1], nbr[q].w[j]);
+          stw<W>(dst, x0 * 2u, o);
         } else {
           // x0 belongs to the previous warp's last lane
-          dst[x0 + 1] = __ushort_as_half((unsigned short)(nbr[q].x & 0xffffu));
-          *reinterpret_cast<uint32_t*>(dst + x0 + 2) = mid(nbr[q].x, nbr[q].y);
+          dst[x0 + 1] = __ushort_as_half((unsigned short)(nbr[q].w[0] & 0xffffu));
+#pragma unroll
+          for (int j = 1; j < W; j++)
+            *reinterpret_cast<uint32_t*>(dst + x0 + 2 * j) = mid(nbr[q].w[j - 1], nbr[q].w[j]);
         }
-        if (tail) dst[xn] = __ushort_as_half((unsigned short)(nbr[q].y >> 16));
+        if (tail) dst[xn] = __ushort_as_half((unsigned short)(nbr[q].w[W - 1] >> 16));
       }
     }
   }
+}
+
+// One row chunk of blockDim.x * V cells per block.
+template <bool HW, bool WM, bool ODD, bool LIM>
+__global__ void __launch_bounds__(FLB_H16_BLOCK, FLB_H16_MIN_BLOCKS) k_sc_h16(const __grid_constant__ KParams p) {
+  constexpr uint32_t V = 2 * FLB_H16_WORDS;
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) p.tstep[!ODD] = p.tstep[ODD] + 1u;
+  h16_cells<HW, WM, ODD, LIM>(p, (blockIdx.x * blockDim.x + threadIdx.x) * V, blockIdx.y);
 }
 
 // ---- launchers -------------------------------------------------------------------
 template <class S, class C, class M, bool FS, bool HW, bool WM, bool FU>
 static void launch_sc_t(const KParams& kp, cudaStream_t st, uint32_t odd, bool vec) {
   if constexpr (kDev<S, FS, FU>) {
-    if (vec && !kp.has_io) {
-      const uint32_t per_row = kp.nx / 4u;
-      const uint32_t block = per_row >= (uint32_t)kVecBlock ? (uint32_t)kVecBlock : ((per_row + 31u) / 32u) * 32u;
+    constexpr uint32_t V = 2u * FLB_H16_WORDS;
+    if (vec && !kp.has_io && kp.nx % V == 0) {
+      const uint32_t per_row = kp.nx / V;
+      const uint32_t bmax = FLB_H16_BLOCK;
+      const uint32_t block = per_row >= bmax ? bmax : ((per_row + 31u) / 32u) * 32u;
       const dim3 g((per_row + block - 1) / block, kp.ny);
-      if (odd) k_sc_h16<HW, WM, true><<<g, block, 0, st>>>(kp);
-      else k_sc_h16<HW, WM, false><<<g, block, 0, st>>>(kp);
+      const bool lim = kp.u_max > 0.0f;
+      if (odd) {
+        if (lim) k_sc_h16<HW, WM, true, true><<<g, block, 0, st>>>(kp);
+        else k_sc_h16<HW, WM, true, false><<<g, block, 0, st>>>(kp);
+      } else {
+        if (lim) k_sc_h16<HW, WM, false, true><<<g, block, 0, st>>>(kp);
+        else k_sc_h16<HW, WM, false, false><<<g, block, 0, st>>>(kp);
+      }
       return;
     }
   }

@@ -46,6 +46,7 @@ void launch_build_lists(const uint32_t* nz, uint32_t* nz_prev, uint32_t nsx, uin
 void launch_init_flags(const uint8_t* geo, uint8_t* flags, uint32_t nx, uint32_t ny, int free_surface, void* mass,
                        void* excess, void* phi, int mass_f64, cudaStream_t st);
 void launch_nbmask(const uint8_t* geo, uint8_t* nbmask, uint32_t nx, uint32_t ny, cudaStream_t st);
+void launch_plain_chunks(const uint8_t* flags, const uint8_t* nbmask, uint32_t N, uint32_t* plain, cudaStream_t st);
 template <class S, class C, class M>
 void launch_init_ddf(const KParams& kp, cudaStream_t st, const uint8_t* geo, bool hw);
 

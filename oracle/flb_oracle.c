@@ -66,6 +66,29 @@ struct orc_state {
 };
 
 /* calculateNeighborsIdxD2Q9, cellCalculations.cuh:82-109 (periodic wrap). */
+/* FP16S dithered rounding of the engine's fused single-phase step (its
+ * lattice.cuh f16_dither): 13 bits of a Weyl sequence in cell, direction and
+ * time step are added to the float's bits, and the sum is truncated to
+ * binary16 (round toward zero), i.e. stochastic rounding made deterministic. */
+static inline uint32_t orc_dither_base(uint32_t idx, uint32_t t) { return idx * 0x85EBCA6Bu + t * 0x9E3779B9u; }
+static inline uint32_t orc_dither(uint32_t base, int i) { return (base + (uint32_t)i * 0x632BE5ABu) >> 19; }
+
+/* binary32 bits -> binary16 bits, rounding toward zero (overflow gives the
+ * largest finite value, as a round-toward-zero conversion does) */
+static inline uint16_t orc_f16_rz(uint32_t x) {
+  const uint16_t sg = (uint16_t)((x >> 16) & 0x8000u);
+  const int e = (int)((x >> 23) & 0xffu);
+  const uint32_t m = x & 0x7fffffu;
+  if (e == 255) return (uint16_t)(sg | (m ? 0x7e00u : 0x7c00u));
+  const int E = e - 127 + 15;
+  if (E >= 31) return (uint16_t)(sg | 0x7bffu);
+  if (E <= 0) {
+    if (E < -10) return sg;
+    return (uint16_t)(sg | ((m | 0x800000u) >> (14 - E)));
+  }
+  return (uint16_t)(sg | ((uint32_t)E << 10) | (m >> 13));
+}
+
 static inline void orc_nbrs(uint32_t idx, uint32_t x, uint32_t y, uint32_t nx, uint32_t ny, uint32_t* nb) {
   const uint32_t yc = y * nx;
   const uint32_t yu = ((y + 1u) % ny) * nx;
