@@ -371,6 +371,65 @@ flb_status initialise(flb_engine* h) {
 
 }  // namespace
 
+namespace flb {
+// The per-case constants of KParams (relaxation, forcing, codec, fused-
+// arithmetic factors) from a validated descriptor; pointers are left null.
+void fill_case_constants(const flb_case_desc* desc, KParams& k) {
+  std::memset(&k, 0, sizeof(k));
+  const float tau = desc->tau;  // float, as cudaInitData.cu:81-82
+  k.inv_tau = 1.0f / tau;
+  k.use_force = desc->use_volumetric_force ? 1 : 0;
+  k.fx = desc->use_volumetric_force ? desc->fx : 0.0f;
+  k.fy = desc->use_volumetric_force ? desc->fy : 0.0f;
+  k.subgrid = desc->subgrid ? 1 : 0;
+  k.collision = desc->collision;
+  k.f16_scale = desc->f16_scale == 0.0f ? 4096.0f : desc->f16_scale;
+  k.f16_inv = 1.0f / k.f16_scale;
+  k.inlet_ux = desc->inlet_ux;
+  k.inlet_uy = desc->inlet_uy;
+  k.fs_cons = desc->fs_mode == FLB_FS_CONSERVATIVE ? 1 : 0;
+  k.u_max = desc->u_max > 0.0f ? desc->u_max : 0.0f;
+  {
+    // cx[i]*Fx + cy[i]*Fy in float, the same IEEE operations the reference
+    // kernel evaluates per cell (cellCalculations.cuh:71); volatile keeps the
+    // host compiler from contracting or folding them
+    const int cxs[9] = {0, 1, -1, 0, 0, 1, -1, 1, -1}, cys[9] = {0, 0, 0, 1, -1, 1, -1, -1, 1};
+    for (int i = 0; i < 9; i++) {
+      volatile float a = (float)cxs[i] * k.fx;
+      volatile float b = (float)cys[i] * k.fy;
+      k.cF[i] = a + b;
+    }
+    // constants of the fused arithmetic, float, uncontracted (the oracle
+    // computes the same ones)
+    volatile float om = k.inv_tau;
+    volatile float omc = 1.0f - om;
+    volatile float half = 0.5f * om;
+    volatile float kk = 1.0f - half;
+    volatile float k3 = 3.0f * kk;
+    volatile float k9 = 9.0f * kk;
+    k.fu_omc = omc;
+    k.fu_nk3 = -k3;
+    k.fu_fx = k.fx;
+    k.fu_fy = k.fy;
+    volatile float hx = 0.5f * k.fx, hy = 0.5f * k.fy;
+    k.fu_hfx = hx;
+    k.fu_hfy = hy;
+    k.fu_sw[0] = k.f16_scale * wgt<float>(0);  // exact: power-of-two scale
+    k.fu_sw[1] = k.f16_scale * wgt<float>(1);
+    k.fu_sw[2] = k.f16_scale * wgt<float>(5);
+    for (int q = 0; q < 4; q++) {
+      volatile float g = k3 * k.cF[2 * q + 1];
+      volatile float hh = k9 * k.cF[2 * q + 1];
+      k.fu_g[q] = g;
+      k.fu_h[q] = hh;
+    }
+  }
+}
+
+flb_status validate_desc(const flb_case_desc* d, std::string& msg) { return validate(d, msg); }
+
+}  // namespace flb
+
 // =============================================================================
 extern "C" {
 
@@ -503,56 +562,7 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
     dispatch(h, [&](auto ops) { ops.grids(h, nsm > 0 ? nsm : 1); });
   }
-  KParams& k = h->kp;
-  std::memset(&k, 0, sizeof(k));
-  const float tau = desc->tau;  // float, as cudaInitData.cu:81-82
-  k.inv_tau = 1.0f / tau;
-  k.use_force = desc->use_volumetric_force ? 1 : 0;
-  k.fx = desc->use_volumetric_force ? desc->fx : 0.0f;
-  k.fy = desc->use_volumetric_force ? desc->fy : 0.0f;
-  k.subgrid = desc->subgrid ? 1 : 0;
-  k.collision = desc->collision;
-  k.f16_scale = desc->f16_scale == 0.0f ? 4096.0f : desc->f16_scale;
-  k.f16_inv = 1.0f / k.f16_scale;
-  k.inlet_ux = desc->inlet_ux;
-  k.inlet_uy = desc->inlet_uy;
-  k.fs_cons = desc->fs_mode == FLB_FS_CONSERVATIVE ? 1 : 0;
-  k.u_max = desc->u_max > 0.0f ? desc->u_max : 0.0f;
-  {
-    // cx[i]*Fx + cy[i]*Fy in float, the same IEEE operations the reference
-    // kernel evaluates per cell (cellCalculations.cuh:71); volatile keeps the
-    // host compiler from contracting or folding them
-    const int cxs[9] = {0, 1, -1, 0, 0, 1, -1, 1, -1}, cys[9] = {0, 0, 0, 1, -1, 1, -1, -1, 1};
-    for (int i = 0; i < 9; i++) {
-      volatile float a = (float)cxs[i] * k.fx;
-      volatile float b = (float)cys[i] * k.fy;
-      k.cF[i] = a + b;
-    }
-    // constants of the fused arithmetic, float, uncontracted (the oracle
-    // computes the same ones)
-    volatile float om = k.inv_tau;
-    volatile float omc = 1.0f - om;
-    volatile float half = 0.5f * om;
-    volatile float kk = 1.0f - half;
-    volatile float k3 = 3.0f * kk;
-    volatile float k9 = 9.0f * kk;
-    k.fu_omc = omc;
-    k.fu_nk3 = -k3;
-    k.fu_fx = k.fx;
-    k.fu_fy = k.fy;
-    volatile float hx = 0.5f * k.fx, hy = 0.5f * k.fy;
-    k.fu_hfx = hx;
-    k.fu_hfy = hy;
-    k.fu_sw[0] = k.f16_scale * wgt<float>(0);  // exact: power-of-two scale
-    k.fu_sw[1] = k.f16_scale * wgt<float>(1);
-    k.fu_sw[2] = k.f16_scale * wgt<float>(5);
-    for (int q = 0; q < 4; q++) {
-      volatile float g = k3 * k.cF[2 * q + 1];
-      volatile float hh = k9 * k.cF[2 * q + 1];
-      k.fu_g[q] = g;
-      k.fu_h[q] = hh;
-    }
-  }
+  fill_case_constants(desc, h->kp);
   cudaError_t e = cudaMemcpyAsync(h->d_geo, desc->flags, N, cudaMemcpyHostToDevice, h->stream);
   if (e != cudaSuccess) return bail(cuda_fail(h, e, "cudaMemcpyAsync"));
   s = initialise(h);

@@ -7,6 +7,9 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <string>
+
+#include "../../include/flowlb.h"
 #include "common.cuh"
 
 // (storage, arithmetic, mass) type triples
@@ -17,6 +20,10 @@
   X(float, float, float)
 
 namespace flb {
+
+// engine.cu: descriptor checks and per-case constants shared with the batch
+flb_status validate_desc(const flb_case_desc* d, std::string& msg);
+void fill_case_constants(const flb_case_desc* desc, KParams& k);
 
 // stream-collide; vec selects the V-cells-per-thread data path, fu the fused
 // SRT arithmetic

@@ -30,6 +30,8 @@ EXPORTS = [
     "flb_set_stream", "flb_get_stream", "flb_field_info", "flb_read_field", "flb_write_field", "flb_total_mass",
     "flb_total_mass_noalloc", "flb_cell_counts", "flb_check_finite", "flb_run_pass", "flb_profile_steps", "flb_launch_count", "flb_save_checkpoint",
     "flb_load_checkpoint", "flb_last_error", "flb_status_string", "flb_version",
+    "flb_batch_create", "flb_batch_step", "flb_batch_sync", "flb_batch_reset", "flb_batch_read_field",
+    "flb_batch_info", "flb_batch_destroy", "flb_batch_last_error",
 ]
 
 
@@ -89,6 +91,14 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "flb_last_error": (C.c_char_p, [H]),
         "flb_status_string": (C.c_char_p, [C.c_int]),
         "flb_version": (C.c_char_p, []),
+        "flb_batch_create": (C.c_int, [C.POINTER(CaseDesc), C.c_uint32, C.c_int, C.POINTER(H)]),
+        "flb_batch_step": (C.c_int, [H, C.c_uint64]),
+        "flb_batch_sync": (C.c_int, [H]),
+        "flb_batch_reset": (C.c_int, [H]),
+        "flb_batch_read_field": (C.c_int, [H, C.c_uint32, C.c_int, C.c_void_p, C.c_int]),
+        "flb_batch_info": (C.c_int, [H, C.POINTER(C.c_int64)]),
+        "flb_batch_destroy": (C.c_int, [H]),
+        "flb_batch_last_error": (C.c_char_p, [H]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -282,3 +292,73 @@ class Solver:
 
     def load_checkpoint(self, path: str):
         self._check(load_library().flb_load_checkpoint(self._h, path.encode()))
+
+
+class Batch:
+    """Many independent single-phase FP32 cases advanced by one persistent
+    kernel per ``step`` call (``flb_batch_*``).  ``cases``: a list of
+    ``(flags, tau, fx, fy)``; the wall treatment and arithmetic are shared.
+    ``autotune``: 0 fixed launch shape, 1 timed search at creation (or a probe
+    step count > 1)."""
+
+    def __init__(self, cases, *, bounce_back: int = BB_HALFWAY, arithmetic: int = ARITH_FUSED, autotune: int = 1,
+                 device: int = -1, stream: int | None = None):
+        L = load_library()
+        self._flags = [np.ascontiguousarray(c[0], dtype=np.uint8) for c in cases]
+        n = len(self._flags)
+        descs = (CaseDesc * n)()
+        self.shapes = []
+        for i, (g, c) in enumerate(zip(self._flags, cases)):
+            d = descs[i]
+            L.flb_case_desc_init(C.byref(d))
+            ny, nx = g.shape
+            self.shapes.append((ny, nx))
+            d.nx, d.ny, d.flags = nx, ny, g.ctypes.data
+            d.precision = 32
+            d.tau, d.fx, d.fy = float(c[1]), float(c[2]), float(c[3])
+            d.bounce_back, d.arithmetic, d.device = int(bounce_back), int(arithmetic), int(device)
+            d.stream = stream or None
+        h = C.c_void_p()
+        st = L.flb_batch_create(descs, n, int(autotune), C.byref(h))
+        if st != 0:
+            raise FlowLBError(st, "flb_batch_create failed")
+        self._h = h
+        self.n = n
+
+    def _check(self, st: int):
+        if st != 0:
+            msg = load_library().flb_batch_last_error(self._h)
+            raise FlowLBError(st, msg.decode() if msg else "")
+
+    def step(self, n: int = 1):
+        self._check(load_library().flb_batch_step(self._h, int(n)))
+
+    def sync(self):
+        self._check(load_library().flb_batch_sync(self._h))
+
+    def reset(self):
+        self._check(load_library().flb_batch_reset(self._h))
+
+    def info(self) -> dict:
+        a = (C.c_int64 * 7)()
+        self._check(load_library().flb_batch_info(self._h, a))
+        return dict(cases=a[0], cells=a[1], t=a[2], cluster=a[3], clusters=a[4], tuned=bool(a[5]), threads=a[6])
+
+    def read(self, i: int, field: int) -> np.ndarray:
+        ny, nx = self.shapes[i]
+        N = nx * ny
+        count = {FIELD_F: 9 * N, FIELD_RHO: N, FIELD_U: 2 * N, FIELD_FLAGS: N}[field]
+        out = np.empty(count, dtype=np.uint8 if field == FIELD_FLAGS else np.float32)
+        self._check(load_library().flb_batch_read_field(self._h, int(i), field, out.ctypes.data, 0))
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().flb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

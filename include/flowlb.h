@@ -205,6 +205,30 @@ FLB_API flb_status flb_launch_count(flb_handle h, uint64_t* launches);
 FLB_API flb_status flb_save_checkpoint(flb_handle h, const char* path);
 FLB_API flb_status flb_load_checkpoint(flb_handle h, const char* path);
 
+/* ---- batched ensemble (no counterpart in the reference, which runs one case
+ * per call) ------------------------------------------------------------------
+ * n independent single-phase FP32 cases (their own sizes, geometry, tau and
+ * body force; one bounce-back, arithmetic, collision and subgrid setting for
+ * all; no inlet/outlet cells) advanced together: flb_batch_step(b, k) is one
+ * graph launch of one persistent kernel that runs all k steps of every case.
+ * Each case ends bit-identical to k flb_step calls on its own handle.
+ * autotune: 0 uses 8-CTA clusters, one CTA per SM; 1 (or a probe step count
+ * > 1) times the candidate cluster sizes and counts on the batch itself and
+ * keeps the fastest, then rebuilds the initial state.  The device, and the
+ * stream if given, come from cases[0]. */
+typedef struct flb_batch_s* flb_batch;
+FLB_API flb_status flb_batch_create(const flb_case_desc* cases, uint32_t n, int autotune, flb_batch* out);
+FLB_API flb_status flb_batch_step(flb_batch b, uint64_t n);
+FLB_API flb_status flb_batch_sync(flb_batch b);
+/* back to the initial state, t = 0 */
+FLB_API flb_status flb_batch_reset(flb_batch b);
+/* FLB_FIELD_F, _RHO, _U or _FLAGS of case i (float, as a precision-32 handle) */
+FLB_API flb_status flb_batch_read_field(flb_batch b, uint32_t i, int field, void* dst, int on_device);
+/* info[0..6] = cases, cells, t, cluster size, clusters, autotuned, threads per CTA */
+FLB_API flb_status flb_batch_info(flb_batch b, int64_t info[7]);
+FLB_API flb_status flb_batch_destroy(flb_batch b);
+FLB_API const char* flb_batch_last_error(flb_batch b);
+
 FLB_API const char* flb_last_error(flb_handle h);
 FLB_API const char* flb_status_string(flb_status s);
 FLB_API const char* flb_version(void);

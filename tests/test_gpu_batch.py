@@ -1,0 +1,62 @@
+"""Batched ensemble (flb_batch_*) against one handle per case.
+
+The batch kernel updates cells with the same per-cell code as the
+single-case kernels, so after the same number of steps every case must equal
+its own Solver run bit for bit (populations, density, velocity, flags).
+"""
+import numpy as np
+import pytest
+
+from conftest import exact_equal, first_mismatch
+from flowlb_b200 import cases
+from flowlb_b200 import engine as E
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_ensemble(n, seed):
+    """Seeded cases of the ensemble's kind, scaled down (and some tiny ones)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        nx = int(rng.integers(9, 300))
+        ny = int(rng.integers(5, 70))
+        w = max(1, int(round(rng.uniform(0.05, 0.2) * nx)))
+        h = max(1, int(round(rng.uniform(0.2, 0.6) * ny)))
+        x0 = nx // 2 - w // 2
+        flags = cases.channel_with_block(nx, ny, x0, x0 + w, min(ny - 2, 1 + h))
+        tau = float(np.float32(rng.uniform(0.52, 0.8)))
+        gx = float(np.float32(10.0 ** rng.uniform(-7.0, -4.0)))
+        out.append((flags, tau, gx, 0.0))
+    return out
+
+
+@pytest.mark.parametrize("bb", [E.BB_HALFWAY, E.BB_IMPLICIT], ids=["halfway", "implicit"])
+@pytest.mark.parametrize("arith", [E.ARITH_FUSED, E.ARITH_REFERENCE], ids=["fused", "ref-arith"])
+@pytest.mark.parametrize("autotune", [0, 4], ids=["fixed", "tuned"])
+def test_batch_matches_single_handles(bb, arith, autotune):
+    ens = _small_ensemble(23, 20261203)
+    b = E.Batch(ens, bounce_back=bb, arithmetic=arith, autotune=autotune)
+    info = b.info()
+    assert info["cases"] == len(ens) and info["tuned"] == bool(autotune)
+    for n in (1, 37, 64):  # odd and even starting parities, one launch each
+        b.step(n)
+    b.sync()
+    assert b.info()["t"] == 102
+    for i, (flags, tau, gx, gy) in enumerate(ens):
+        s = E.Solver(flags, precision=32, tau=tau, fx=gx, fy=gy, bounce_back=bb, arithmetic=arith)
+        s.step(102)
+        for name, fid, ref in (("f", E.FIELD_F, s.f), ("rho", E.FIELD_RHO, s.rho), ("u", E.FIELD_U, s.u),
+                               ("flags", E.FIELD_FLAGS, s.flags)):
+            got = b.read(i, fid)
+            assert exact_equal(got, ref), f"case {i} {flags.shape} {name}: {first_mismatch(got, ref)}"
+        s.close()
+    b.reset()
+    assert b.info()["t"] == 0
+    b.close()
+
+
+def test_batch_rejects_unsupported_cases():
+    ens = _small_ensemble(2, 1)
+    with pytest.raises(E.FlowLBError):
+        E.Batch(ens, bounce_back=E.BB_HALFWAY, arithmetic=7)
