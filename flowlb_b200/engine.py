@@ -32,6 +32,9 @@ EXPORTS = [
     "flb_load_checkpoint", "flb_last_error", "flb_status_string", "flb_version",
     "flb_batch_create", "flb_batch_step", "flb_batch_sync", "flb_batch_reset", "flb_batch_read_field",
     "flb_batch_info", "flb_batch_destroy", "flb_batch_last_error",
+    "flb_adjoint_desc_init", "flb_adjoint_create", "flb_adjoint_set_porosity", "flb_adjoint_set_force",
+    "flb_adjoint_forward", "flb_adjoint_backward", "flb_adjoint_timing", "flb_adjoint_destroy",
+    "flb_adjoint_last_error",
 ]
 
 
@@ -43,6 +46,15 @@ class CaseDesc(C.Structure):
         ("fy", C.c_float), ("bounce_back", C.c_int32), ("fs_mode", C.c_int32), ("f16_scale", C.c_float),
         ("device", C.c_int32), ("stream", C.c_void_p), ("inlet_ux", C.c_double), ("inlet_uy", C.c_double),
         ("kernel_variant", C.c_int32), ("u_max", C.c_float), ("arithmetic", C.c_int32),
+    ]
+
+
+class AdjointDesc(C.Structure):
+    _fields_ = [
+        ("nx", C.c_uint32), ("ny", C.c_uint32), ("flags", C.c_void_p), ("porosity", C.c_void_p),
+        ("precision", C.c_int32), ("tau", C.c_double), ("gx", C.c_double), ("gy", C.c_double),
+        ("steps", C.c_uint64), ("window", C.c_uint64), ("checkpoint_every", C.c_uint32), ("device", C.c_int32),
+        ("stream", C.c_void_p),
     ]
 
 
@@ -99,6 +111,15 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "flb_batch_info": (C.c_int, [H, C.POINTER(C.c_int64)]),
         "flb_batch_destroy": (C.c_int, [H]),
         "flb_batch_last_error": (C.c_char_p, [H]),
+        "flb_adjoint_desc_init": (None, [C.POINTER(AdjointDesc)]),
+        "flb_adjoint_create": (C.c_int, [C.POINTER(AdjointDesc), C.POINTER(H)]),
+        "flb_adjoint_set_porosity": (C.c_int, [H, C.c_void_p]),
+        "flb_adjoint_set_force": (C.c_int, [H, C.c_double, C.c_double]),
+        "flb_adjoint_forward": (C.c_int, [H, C.POINTER(C.c_double)]),
+        "flb_adjoint_backward": (C.c_int, [H, C.c_void_p, C.c_void_p]),
+        "flb_adjoint_timing": (C.c_int, [H, C.POINTER(C.c_double)]),
+        "flb_adjoint_destroy": (C.c_int, [H]),
+        "flb_adjoint_last_error": (C.c_char_p, [H]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -355,6 +376,71 @@ class Batch:
     def close(self):
         if getattr(self, "_h", None):
             load_library().flb_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Adjoint:
+    """Forward/backward pair of the Brinkman-porosity single phase
+    (``flb_adjoint_*``): ``forward()`` returns J, ``backward()`` returns
+    (dJ/ds as (ny, nx), dJ/dg as (2,))."""
+
+    def __init__(self, flags: np.ndarray, porosity: np.ndarray, *, tau: float = 0.6, gx: float = 0.0,
+                 gy: float = 0.0, precision: int = 32, steps: int = 4096, window: int = 512,
+                 checkpoint_every: int = 64, device: int = -1, stream: int | None = None):
+        L = load_library()
+        self._flags = np.ascontiguousarray(flags, dtype=np.uint8)
+        s = np.ascontiguousarray(porosity, dtype=np.float64)
+        self.ny, self.nx = self._flags.shape
+        d = AdjointDesc()
+        L.flb_adjoint_desc_init(C.byref(d))
+        d.nx, d.ny, d.flags, d.porosity = self.nx, self.ny, self._flags.ctypes.data, s.ctypes.data
+        d.precision, d.tau, d.gx, d.gy = int(precision), float(tau), float(gx), float(gy)
+        d.steps, d.window, d.checkpoint_every = int(steps), int(window), int(checkpoint_every)
+        d.device, d.stream = int(device), stream or None
+        h = C.c_void_p()
+        st = L.flb_adjoint_create(C.byref(d), C.byref(h))
+        if st != 0:
+            raise FlowLBError(st, "flb_adjoint_create failed")
+        self._h = h
+
+    def _check(self, st: int):
+        if st != 0:
+            msg = load_library().flb_adjoint_last_error(self._h)
+            raise FlowLBError(st, msg.decode() if msg else "")
+
+    def set_porosity(self, porosity: np.ndarray):
+        s = np.ascontiguousarray(porosity, dtype=np.float64)
+        assert s.size == self.nx * self.ny
+        self._check(load_library().flb_adjoint_set_porosity(self._h, s.ctypes.data))
+
+    def set_force(self, gx: float, gy: float = 0.0):
+        self._check(load_library().flb_adjoint_set_force(self._h, float(gx), float(gy)))
+
+    def forward(self) -> float:
+        J = C.c_double()
+        self._check(load_library().flb_adjoint_forward(self._h, C.byref(J)))
+        return float(J.value)
+
+    def backward(self):
+        ds = np.empty(self.nx * self.ny)
+        dg = np.empty(2)
+        self._check(load_library().flb_adjoint_backward(self._h, ds.ctypes.data, dg.ctypes.data))
+        return ds.reshape(self.ny, self.nx), dg
+
+    def timing(self) -> tuple[float, float]:
+        a = (C.c_double * 2)()
+        self._check(load_library().flb_adjoint_timing(self._h, a))
+        return float(a[0]), float(a[1])
+
+    def close(self):
+        if getattr(self, "_h", None):
+            load_library().flb_adjoint_destroy(self._h)
             self._h = None
 
     def __del__(self):

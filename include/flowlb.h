@@ -229,6 +229,42 @@ FLB_API flb_status flb_batch_info(flb_batch b, int64_t info[7]);
 FLB_API flb_status flb_batch_destroy(flb_batch b);
 FLB_API const char* flb_batch_last_error(flb_batch b);
 
+/* ---- adjoint of the Brinkman-porosity single phase (no counterpart in the
+ * reference) -------------------------------------------------------------------
+ * Forward model per fluid cell (pull streaming, half-way walls, x periodic):
+ * rho = sum f, v = j/rho, u = (v + g/2)/(1 + s/2), F = rho (g - s u), BGK with
+ * Guo forcing; s in [0,1] is a per-cell drag coefficient (0 free fluid, 1 a
+ * quasi-solid).  Objective J = (1/window) * sum over the last `window` steps
+ * of sum_y rho u_x in the last column.  flb_adjoint_forward runs the steps from
+ * rest and keeps a checkpoint every checkpoint_every steps; flb_adjoint_backward
+ * recomputes each segment from its checkpoint and runs the hand-written
+ * adjoint step backwards, giving dJ/ds per cell and dJ/dg. */
+typedef struct flb_adjoint_desc {
+  uint32_t nx, ny;
+  const uint8_t* flags;      /* N bytes: FLUID or WALL */
+  const double* porosity;    /* N drag coefficients s in [0,1] */
+  int32_t precision;         /* 32 or 64 (arithmetic and storage) */
+  double tau;                /* relaxation time */
+  double gx, gy;             /* body acceleration, lattice units */
+  uint64_t steps;            /* a multiple of checkpoint_every */
+  uint64_t window;           /* objective steps at the end, 1..steps */
+  uint32_t checkpoint_every; /* even */
+  int32_t device;
+  void* stream;
+} flb_adjoint_desc;
+typedef struct flb_adjoint_s* flb_adjoint;
+FLB_API void flb_adjoint_desc_init(flb_adjoint_desc* d);
+FLB_API flb_status flb_adjoint_create(const flb_adjoint_desc* d, flb_adjoint* out);
+FLB_API flb_status flb_adjoint_set_porosity(flb_adjoint a, const double* s);
+FLB_API flb_status flb_adjoint_set_force(flb_adjoint a, double gx, double gy);
+FLB_API flb_status flb_adjoint_forward(flb_adjoint a, double* J);
+/* dJ_ds: N doubles (host, may be null); dJ_dg: {dJ/dgx, dJ/dgy} (may be null) */
+FLB_API flb_status flb_adjoint_backward(flb_adjoint a, double* dJ_ds, double dJ_dg[2]);
+/* device milliseconds of the last forward and backward calls */
+FLB_API flb_status flb_adjoint_timing(flb_adjoint a, double ms[2]);
+FLB_API flb_status flb_adjoint_destroy(flb_adjoint a);
+FLB_API const char* flb_adjoint_last_error(flb_adjoint a);
+
 FLB_API const char* flb_last_error(flb_handle h);
 FLB_API const char* flb_status_string(flb_status s);
 FLB_API const char* flb_version(void);

@@ -50,6 +50,10 @@ def lib() -> C.CDLL:
         if not os.path.exists(path):
             raise FileNotFoundError(f"{path} missing: run `make -C oracle`")
         L = C.CDLL(path)
+        L.orc_adj_run.restype = C.c_int
+        L.orc_adj_run.argtypes = [C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_double, C.c_double,
+                                  C.c_double, C.c_uint64, C.c_uint64, C.POINTER(C.c_double), C.c_void_p,
+                                  C.c_void_p]
         L.orc_create.restype = C.c_void_p
         L.orc_create.argtypes = [C.POINTER(OrcParams), C.c_void_p]
         L.orc_destroy.argtypes = [C.c_void_p]
@@ -243,3 +247,20 @@ def ref_cuda_run(state: dict, nx: int, ny: int, precision: int, free_surface: bo
     if rc != 0:
         raise RuntimeError(f"ref_cuda_run failed: {rc}")
     return s
+
+
+def adjoint_run(flags: np.ndarray, porosity: np.ndarray, tau: float, gx: float, gy: float, steps: int,
+                window: int, grad: bool = True):
+    """FP64 CPU tape adjoint of the Brinkman-porosity step (flb_adjoint_oracle.c):
+    returns (J, dJ/ds as (ny, nx), dJ/dg as (2,)) or (J, None, None)."""
+    g = np.ascontiguousarray(flags, dtype=np.uint8)
+    sv = np.ascontiguousarray(porosity, dtype=np.float64)
+    ny, nx = g.shape
+    J = C.c_double()
+    ds = np.zeros(nx * ny) if grad else None
+    dg = np.zeros(2) if grad else None
+    rc = lib().orc_adj_run(nx, ny, g.ctypes.data, sv.ctypes.data, tau, gx, gy, steps, window, C.byref(J),
+                           ds.ctypes.data if grad else None, dg.ctypes.data if grad else None)
+    if rc != 0:
+        raise MemoryError("orc_adj_run")
+    return float(J.value), (ds.reshape(ny, nx) if grad else None), dg
