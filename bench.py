@@ -1,22 +1,30 @@
 """Benchmark of the D2Q9 solver step on B200.
 
-Workload (one bench "step" = S lattice time steps of one case):
-  free-surface culvert dam break scaled to 8192x2048 (the precision-sweep case),
-  FP32 populations + FP64 mass/fill level, half-way walls, conservative free
-  surface.  Working set ~1.2 GB, far above the 126 MB L2, so no L2 flush is
-  needed between steps.
+Workload (one bench "step" = S lattice time steps of one case): the
+free-surface culvert dam break, 2048x512, FP32 populations + FP64 mass,
+tau 0.55, g_y -5e-5, half-way walls, conservative free surface, velocity
+limiter 0.25.  Its working set (~70 MB) fits in the 126 MB L2, so the L2 is
+flushed (a 256 MB buffer is zeroed) before every timed step, outside the
+timed events.
 
-  value  MLUPS (million cell updates / s) over all ranks, inputs resident in
-         HBM, device time from CUDA events on the engine's stream, max over ranks.
+  value  MLUPS over all ranks, inputs resident in HBM, device time from CUDA
+         events on the engine's stream (per step, summed), max over ranks.
   e2e    the same metric through the C ABI with host buffers: per step
-         flb_reset from pinned host geometry flags (H2D), S steps, and a read of
-         density, velocity, fill level and flags into pinned host memory (D2H).
+         flb_reset from pinned host geometry flags (H2D), S steps, and a read
+         of density, velocity, fill level and flags into pinned host memory.
+
+Side measurements on rank 0 (--no-extra skips them): the plain FP32 and FP16
+scaled-deviation single-phase step on 8192x2048 (HBM fraction, FP16/FP32
+ratio) with the FP16 velocity error against FP64 on the 256x64 channel after
+10,000 steps; the dam break at 8192x2048; the 512-case batched ensemble
+against a per-case loop; the adjoint's backward/forward cost.
 
 Multi-GPU: the path does not shard (one GPU per case), so --gpus N runs N
 independent replicas, one per rank (weak scaling).
 
 --impl reference times the CPU restatement of the reference step (the oracle,
-OpenMP on the host cores) on a bounded sample of the same workload.
+OpenMP on the host cores, reference arithmetic) on a bounded sample of the
+same workload.
 """
 from __future__ import annotations
 
@@ -35,9 +43,14 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "MLUPS, %HBM peak: FP32 vs FP16-store @L2<1e-3; batch cases/s; adjoint/fwd"
-WORKLOAD = ("free-surface culvert dam break 8192x2048 (precision-sweep geometry), tau 0.55, g_y -5e-5, FP32 "
-            "populations + FP64 mass, half-way walls, conservative free surface, velocity limiter 0.25")
+WORKLOAD = ("free-surface culvert dam break 2048x512, tau 0.55, g_y -5e-5, FP32 populations + FP64 mass, "
+            "half-way walls, conservative free surface, velocity limiter 0.25")
 U_MAX = 0.25  # keeps the surge front stable (plain BGK at tau 0.55 diverges near Mach 0.6)
+KERNEL_OF_PASS = {"stream_collide": "k_sc_list (free-surface stream-collide)", "fs1": "k_fs1 (mass exchange)",
+                  "fs234": "k_fs234 (flag stencil, mass/fill update)"}
+# dram__bytes_read.sum + dram__bytes_write.sum per launch from one ncu capture
+# of the workload (profiles/), None where not captured
+TRAFFIC_NCU: dict = {}
 
 
 def env_rank():
@@ -110,15 +123,22 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def algorithmic_bytes_sc(counts: dict, N: int) -> float:
-    """Stream-collide pass, free-surface FP32 build, over the super-tiles it
-    visits: every visited cell reads its flag (1 B); every fluid/interface
-    cell loads and stores its 9 populations (72 B), writes density and
-    velocity (12 B) and reads its wall-neighbour mask (1 B); interface cells
-    also read their FP64 mass (8 B) and rewrite their flag (1 B).  Gas cells
-    outside the visited super-tiles are not counted (they are not touched)."""
+def algorithmic_bytes(counts: dict) -> dict:
+    """Bytes each free-surface pass must move per launch (FP32 populations,
+    FP64 mass), over the cells it visits: the listed super-tiles hold the
+    fluid and interface cells (gas cells outside them are not touched).
+      stream-collide: per fluid/interface cell its flag and wall mask (2 B),
+        9 population loads and stores (72 B), density and velocity (12 B);
+        interface cells also read their mass (8 B) and rewrite the flag (1 B);
+      FS_1: per fluid/interface cell 9 incoming and 8 outgoing populations
+        (68 B), its flag (1 B), mass read and write (16 B) and the excess
+        shares it collects (8 B);
+      FS_2..4: per fluid/interface cell the flag (1 B), the flag buffer read
+        and write (2 B), density (4 B), mass read and write (16 B), excess and
+        fill level (16 B)."""
     active = counts["fluid"] + counts["interface"]
-    return active * 86.0 + counts["interface"] * 9.0
+    return {"stream_collide": active * 86.0 + counts["interface"] * 9.0, "fs1": active * 93.0,
+            "fs234": active * 39.0}
 
 
 def run_ours(args, rank, local_rank, world):
@@ -134,12 +154,13 @@ def run_ours(args, rank, local_rank, world):
 
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    case = cases.dam_break(4)
+    case = cases.dam_break(1)
     N = case.cells
     S = args.lattice_steps
     solver = E.Solver(case.flags, free_surface=True, precision=32, mass_precision=64, tau=case.tau, fy=case.fy,
                       bounce_back=E.BB_HALFWAY, fs_mode=E.FS_CONSERVATIVE, device=local_rank, u_max=U_MAX)
     stream = torch.cuda.ExternalStream(solver.stream, device=local_rank)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
 
     def barrier():
         torch.cuda.synchronize()
@@ -147,25 +168,28 @@ def run_ours(args, rank, local_rank, world):
             dist.barrier()
         torch.cuda.synchronize()
 
-    # ---- device-resident timing -------------------------------------------
+    # ---- device-resident timing (L2 flushed before every step) ------------
     for _ in range(args.warmup):
         solver.step(S)
     solver.sync()
     counts0 = solver.cell_counts()
+    m0 = solver.total_mass()
     launches0 = solver.launches
     barrier()
-    start = torch.cuda.Event(enable_timing=True)
-    stop = torch.cuda.Event(enable_timing=True)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     with ClockSampler(local_rank) as clocks:
-        start.record(stream)
-        for _ in range(args.steps):
+        for a, b in ev:
+            flush.zero_()
+            torch.cuda.current_stream().synchronize()
+            a.record(stream)
             solver.step(S)
-        stop.record(stream)
-        stop.synchronize()
+            b.record(stream)
+        solver.sync()
     barrier()
-    elapsed_ms = start.elapsed_time(stop)
+    elapsed_ms = sum(a.elapsed_time(b) for a, b in ev)
     launches = solver.launches - launches0
     counts1 = solver.cell_counts()
+    mass_drift = (solver.total_mass() - m0) / m0
     t_max = elapsed_ms
     if dist is not None:
         tt = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
@@ -179,11 +203,14 @@ def run_ours(args, rank, local_rank, world):
     passes = solver.profile_steps(prof_steps)
     cb = solver.cell_counts()
     counts_avg = {k: 0.5 * (ca[k] + cb[k]) for k in ca}
-    sc_ms = passes["stream_collide"] / prof_steps
-    sc_bytes = algorithmic_bytes_sc(counts_avg, N)
+    pbytes = algorithmic_bytes(counts_avg)
+    dom = max(passes, key=passes.get)
+    dom_ms = passes[dom] / prof_steps
     peak, peak_kind = measured_peaks()
-    achieved = sc_bytes / (sc_ms * 1e-3) / 1e9
+    achieved = pbytes[dom] / (dom_ms * 1e-3) / 1e9
     shares = {k: v / max(1e-12, sum(passes.values())) for k, v in passes.items()}
+    per_pass = {k: {"avg_launch_ms": round(passes[k] / prof_steps, 5),
+                    "achieved_gbs": round(pbytes[k] / (passes[k] / prof_steps * 1e-3) / 1e9, 1)} for k in passes}
 
     # ---- end to end through the C ABI with host buffers -------------------
     host_flags = torch.from_numpy(np.ascontiguousarray(case.flags.ravel())).pin_memory()
@@ -232,16 +259,19 @@ def run_ours(args, rank, local_rank, world):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "nx": case.nx, "ny": case.ny, "cells": N,
                        "lattice_steps_per_step": S, "parallelism": f"replicas x{world}",
-                       "l2": "working set ~1.2 GB > 126 MB L2; no flush needed",
-                       "cells_by_type_at_start": counts0, "cells_by_type_at_end": counts1},
+                       "l2": "working set ~70 MB < 126 MB L2: a 256 MB buffer is zeroed before every timed step "
+                             "(outside the timed events)",
+                       "cells_by_type_at_start": counts0, "cells_by_type_at_end": counts1,
+                       "total_mass_rel_drift": mass_drift},
             "e2e": {"value": round(e2e_value, 1), "unit": "MLUPS", "h2d_bytes_per_step": int(N),
                     "d2h_bytes_per_step": int(N * (4 + 8 + 8 + 1))},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": "k_stream_collide (free-surface FP32 build)",
+            "roofline": {"bound": "hbm", "kernel": KERNEL_OF_PASS[dom],
                          "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                         "traffic": None, "algorithmic_bytes_per_launch": int(sc_bytes),
-                         "avg_launch_ms": round(sc_ms, 5), "pass_share": {k: round(v, 3) for k, v in shares.items()}},
+                         "traffic": TRAFFIC_NCU.get(dom), "algorithmic_bytes_per_launch": int(pbytes[dom]),
+                         "avg_launch_ms": round(dom_ms, 5), "pass_share": {k: round(v, 3) for k, v in shares.items()},
+                         "passes": per_pass},
             "clocks": clocks.summary(),
         }
         if cpu is not None:
@@ -252,53 +282,107 @@ def run_ours(args, rank, local_rank, world):
         dist.destroy_process_group()
 
 
+def _timed(torch, solver, n):
+    st = torch.cuda.ExternalStream(solver.stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    solver.step(n)
+    b.record(st)
+    b.synchronize()
+    return a.elapsed_time(b)
+
+
 def side_measurements(args, device, E, cases, peak):
-    """FP16 scaled-deviation storage on the same workload, and the plain FP32
-    single-phase step on an 8192x2048 grid (the >=80% HBM target)."""
     import torch
 
     out = {}
-    c = cases.dam_break(4)
-    S = args.lattice_steps
-    s16 = E.Solver(c.flags, free_surface=True, precision=16, mass_precision=64, tau=c.tau, fy=c.fy,
-                   bounce_back=E.BB_HALFWAY, fs_mode=E.FS_CONSERVATIVE, device=device, u_max=U_MAX)
-    st = torch.cuda.ExternalStream(s16.stream, device=device)
-    s16.step(S)
-    s16.sync()
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record(st)
-    for _ in range(max(2, args.steps // 2)):
-        s16.step(S)
-    b.record(st)
-    b.synchronize()
-    ms = a.elapsed_time(b)
-    out["fp16s_same_workload"] = {"value": round(c.cells * S * max(2, args.steps // 2) / (ms * 1e-3) / 1e6, 1),
-                                  "unit": "MLUPS"}
-    s16.close()
+    # plain single phase on 8192x2048 (working set ~1.2 GB): FP32 and FP16S
     p = cases.hbm_probe(8192, 2048)
-    for prec, key, bytes_per in ((32, "single_phase_fp32_8192x2048", 74.0), (16, "single_phase_fp16s_8192x2048",
-                                                                               38.0)):
+    for prec, key, bytes_per in ((32, "single_phase_fp32_8192x2048", 72.0),
+                                 (16, "single_phase_fp16s_8192x2048", 36.0)):
         s = E.Solver(p.flags, free_surface=False, precision=prec, tau=p.tau, fx=p.fx, bounce_back=E.BB_HALFWAY,
                      device=device)
-        st = torch.cuda.ExternalStream(s.stream, device=device)
         s.step(50)
         s.sync()
         n = 400
-        a.record(st)
-        s.step(n)
-        b.record(st)
-        b.synchronize()
-        ms = a.elapsed_time(b)
-        cnt = s.cell_counts()
-        fluid = cnt["fluid"]
+        ms = _timed(torch, s, n)
         mlups = p.cells * n / (ms * 1e-3) / 1e6
-        # bytes: flag of every cell + populations and wall mask of fluid cells
-        gbs = (p.cells * 1.0 + fluid * (bytes_per - 1.0)) * n / (ms * 1e-3) / 1e9
+        # bytes: the populations of every cell; flag and wall mask only where
+        # the plain-fluid chunk map does not cover the cell (about 5 %)
+        gbs = p.cells * bytes_per * n / (ms * 1e-3) / 1e9
         out[key] = {"value": round(mlups, 1), "unit": "MLUPS", "achieved_gbs": round(gbs, 1),
-                    "frac_of_measured_hbm": round(gbs / peak, 4)}
+                    "frac_of_measured_hbm": round(gbs / peak, 4), "bytes_per_cell": bytes_per}
         s.close()
     out["fp16s_speedup_single_phase"] = round(out["single_phase_fp16s_8192x2048"]["value"] /
                                               out["single_phase_fp32_8192x2048"]["value"], 3)
+    # FP16S accuracy: velocity L2 against FP64 on the 256x64 channel, 10,000 steps
+    ch = cases.plain_channel()
+    fluid = np.tile(ch.flags.ravel() == cases.FLUID, 2)
+    us = {}
+    for prec in (64, 32, 16):
+        s = E.Solver(ch.flags, precision=prec, tau=ch.tau, fx=ch.fx, bounce_back=E.BB_HALFWAY, device=device)
+        s.step(10_000)
+        us[prec] = s.u.astype(np.float64)[fluid]
+        s.close()
+    for prec in (32, 16):
+        out[f"velocity_l2_vs_fp64_{'fp32' if prec == 32 else 'fp16s'}_channel_256x64_10000"] = float(
+            np.linalg.norm(us[prec] - us[64]) / np.linalg.norm(us[64]))
+    # the dam break at 8192x2048 (FP32 and FP16S)
+    c = cases.dam_break(4)
+    S = args.lattice_steps
+    for prec in (32, 16):
+        s = E.Solver(c.flags, free_surface=True, precision=prec, mass_precision=64, tau=c.tau, fy=c.fy,
+                     bounce_back=E.BB_HALFWAY, fs_mode=E.FS_CONSERVATIVE, device=device, u_max=U_MAX)
+        s.step(S)
+        s.sync()
+        ms = _timed(torch, s, 2 * S)
+        out[f"dam_break_8192x2048_fp{prec if prec == 32 else '16s'}"] = {
+            "value": round(c.cells * 2 * S / (ms * 1e-3) / 1e6, 1), "unit": "MLUPS"}
+        s.close()
+    # batched ensemble: 512 cases in one launch per call vs a per-case loop
+    ens = cases.ensemble()
+    n_b = args.batch_steps
+    spec = [(e.flags, e.tau, e.fx, 0.0) for e in ens]
+    cells = sum(e.flags.size for e in ens)
+    b = E.Batch(spec, autotune=1, device=device)
+    b.step(2)
+    b.sync()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.step(n_b)
+    b.sync()
+    tb = time.perf_counter() - t0
+    info = b.info()
+    b.close()
+    sm = torch.cuda.Stream()
+    solvers = [E.Solver(e.flags, precision=32, tau=e.tau, fx=e.fx, stream=sm.cuda_stream, device=device)
+               for e in ens]
+    for s in solvers:
+        s.step(2)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in solvers:
+        s.step(n_b)
+    torch.cuda.synchronize()
+    tl = time.perf_counter() - t0
+    for s in solvers:
+        s.close()
+    scale = 5000.0 / n_b
+    out["batch_512_cases"] = {"cases_per_s": round(len(ens) / (tb * scale), 2), "unit": "cases/s (5000 steps)",
+                              "loop_cases_per_s": round(len(ens) / (tl * scale), 2),
+                              "speedup_vs_per_case_loop": round(tl / tb, 3), "glups": round(cells * n_b / tb / 1e9, 1),
+                              "steps_timed": n_b, "config": info}
+    # adjoint: backward (with checkpoint recomputation) over forward
+    pc = cases.porous_channel()
+    a = E.Adjoint(pc.flags, pc.porosity.astype(np.float64), tau=pc.tau, gx=pc.fx, precision=32, device=device)
+    a.forward()
+    a.backward()
+    a.forward()
+    a.backward()
+    f_ms, b_ms = a.timing()
+    a.close()
+    out["adjoint_1024x256_4096"] = {"forward_ms": round(f_ms, 2), "backward_ms": round(b_ms, 2),
+                                    "backward_over_forward": round(b_ms / f_ms, 3)}
     return out
 
 
@@ -317,7 +401,8 @@ def cpu_baseline(case, args):
     dt = time.perf_counter() - t0
     o.close()
     return {"value": round(case.cells * n / dt / 1e6, 2), "unit": "MLUPS", "cores": threads, "kind": "port",
-            "sample": f"{case.nx}x{case.ny} dam break, {n} time steps after the first, same storage and modes"}
+            "sample": f"{case.nx}x{case.ny} dam break, {n} time steps after the first, same storage, modes and "
+                      f"arithmetic ({dt:.1f} s)"}
 
 
 def run_reference(args, rank, world):
@@ -327,7 +412,7 @@ def run_reference(args, rank, world):
     from flowlb_b200 import cases
     from oracle import oracle as O
 
-    case = cases.dam_break(4)
+    case = cases.dam_break(1)
     threads = os.cpu_count() or 1
     o = O.Oracle(case.flags, O.OracleConfig(variant=O.F32, free_surface=True, bb=O.BB_HALFWAY,
                                             fs_mode=O.FS_CONSERVATIVE, tau=case.tau, fy=case.fy, threads=threads,
@@ -359,8 +444,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--lattice-steps", type=int, default=200, help="lattice time steps per bench step")
-    ap.add_argument("--ref-lattice-steps", type=int, default=2)
-    ap.add_argument("--cpu-steps", type=int, default=10)
+    ap.add_argument("--ref-lattice-steps", type=int, default=40)
+    ap.add_argument("--cpu-steps", type=int, default=2000)
+    ap.add_argument("--batch-steps", type=int, default=1000, help="steps of the batch measurement (scaled to 5000)")
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
