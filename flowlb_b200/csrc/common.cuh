@@ -86,6 +86,12 @@ __device__ __forceinline__ bool same_bits(float a, float b) { return __float_as_
 // persistent grid.  all = 1 visits every super-tile (first step after the
 // state was set from outside).
 constexpr uint32_t kSTW = 128, kSTH = 8;
+// threads per block of the listed stream-collide and FS_1 kernels: 1024 take
+// a super-tile in one pass (one cell per thread), 256 in four (row chunks)
+#ifndef FLB_LIST_BLOCK
+#define FLB_LIST_BLOCK 1024
+#endif
+constexpr int kListBlock = FLB_LIST_BLOCK;
 
 struct TileList {
   const uint32_t* list;

@@ -137,7 +137,7 @@ struct Ops {
   static void grids(flb_engine* h, int nsm) {
     h->grid_sc = (uint32_t)(nsm * sc_list_blocks_per_sm<S, C, M>());
     h->grid_fs1 = (uint32_t)(nsm * fs_blocks_per_sm<S, C, M>(0));
-    h->grid_fs234 = (uint32_t)(nsm * fs_blocks_per_sm<S, C, M>(1));
+    h->grid_fs234 = (uint32_t)(nsm * fs_blocks_per_sm<S, C, M>(h->ntiles <= 4096u ? 1 : 2));
   }
   static void apply_recon(flb_engine* h, uint32_t odd) { launch_apply_recon<S, C, M>(h->kp, h->stream, odd); }
   static void init_ddf(flb_engine* h) { launch_init_ddf<S, C, M>(h->kp, h->stream, h->d_geo, h->hw); }

@@ -108,16 +108,18 @@ __device__ __forceinline__ void fs1_cell(const KParams& p, uint32_t x, uint32_t 
 
 // The listed super-tiles, one row of a super-tile per warp.
 template <class S, class C, class M, bool HW, bool ODD>
-__global__ void __launch_bounds__(kBlock) k_fs1(const __grid_constant__ KParams p, const TileList tl) {
+__global__ void __launch_bounds__(kListBlock, 1024 / kListBlock) k_fs1(const __grid_constant__ KParams p,
+                                                                       const TileList tl) {
   const uint32_t n = tile_count(tl);
-  const uint32_t lane = threadIdx.x & 31u, row = threadIdx.x >> 5;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t row = warp % kSTH, chunk = warp / kSTH, cpr = (blockDim.x >> 5) / kSTH;
   for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
     const uint32_t t = tile_at(tl, i);
     const uint32_t y = (t / tl.nsx) * kSTH + row;
     if (y >= p.ny) continue;
     const uint32_t xb = (t % tl.nsx) * kSTW + lane;
 #pragma unroll 1
-    for (uint32_t j = 0; j < kSTW; j += 32)
+    for (uint32_t j = chunk * 32u; j < kSTW; j += 32u * cpr)
       if (xb + j < p.nx) fs1_cell<S, C, M, HW, ODD>(p, xb + j, y);
   }
 }
@@ -149,29 +151,36 @@ __global__ void k_apply_recon(const __grid_constant__ KParams p, uint32_t odd) {
 
 // ---- FS_2 + FS_3 + FS_4 fused: lbmKernel2D.cu:124-303 ----------------------
 // The three reference passes are flag stencils of radius one, chained; a tile
-// of 32x8 cells stages the flags of its 3-cell halo in shared memory and
+// of kTX x 8 cells stages the flags of its 3-cell halo in shared memory and
 // evaluates the chain there, so neighbour flags are never read while another
 // block rewrites them.  Reads p.flags, writes p.flags_out.
-constexpr int kTX = 32, kTY = 8, kHalo = 3;
-constexpr int kSX = kTX + 2 * kHalo, kSY = kTY + 2 * kHalo;
-
+// Tile width of the flag pass: 128 (a whole super-tile, 1024 threads) or 32
+// (a quarter, 256 threads).  Measured on a B200, dam break: 2048x512 (about
+// 300 active super-tiles) 31 vs 25 GLUPS in favour of 128; 8192x2048 (about
+// 4400) 53 vs 59 in favour of 32 (more resident warps).  launch_fs234 picks by
+// the grid's super-tile count (kWideTiles).
+constexpr int kTY = 8, kHalo = 3;
+constexpr uint32_t kWideTiles = 4096;
 __device__ __forceinline__ int wrapi(int v, int n) {
   v %= n;
   return v < 0 ? v + n : v;
 }
 
+template <int TW>
 struct FlagTiles {
+  static constexpr int kSX = TW + 2 * kHalo, kSY = kTY + 2 * kHalo;
   uint8_t s0[kSY][kSX];  // after stream-collide
   uint8_t s1[kSY][kSX];  // after FS_2
   uint8_t s2[kSY][kSX];  // after FS_3
   uint8_t s3[kSY][kSX];  // after FS_4 conversion
 };
 
-// One 32x8 tile (tile coordinates tx, ty) with the 256 threads of the block;
+// One kTX x 8 tile (tile coordinates tx, ty) with the kTX*8 threads of the block;
 // every thread of the block must call it.  Returns whether this thread's cell
 // is fluid or interface after the pass.
-template <class S, class C, class M, bool ODD>
-__device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int tid, FlagTiles& sm) {
+template <class S, class C, class M, bool ODD, int TW>
+__device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int tid, FlagTiles<TW>& sm) {
+  constexpr int kTX = TW, kSX = FlagTiles<TW>::kSX, kSY = FlagTiles<TW>::kSY;
   auto& s0 = sm.s0;
   auto& s1 = sm.s1;
   auto& s2 = sm.s2;
@@ -353,10 +362,11 @@ __device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int
 // The listed super-tiles: each block runs the tile pass on the 4 tiles of a
 // super-tile and records in nz whether the super-tile holds fluid or
 // interface cells afterwards.
-template <class S, class C, class M, bool ODD>
-__global__ void __launch_bounds__(kTX* kTY) k_fs234(const __grid_constant__ KParams p, const TileList tl,
+template <class S, class C, class M, bool ODD, int TW>
+__global__ void __launch_bounds__(TW* kTY) k_fs234(const __grid_constant__ KParams p, const TileList tl,
                                                     uint32_t* __restrict__ nz) {
-  __shared__ FlagTiles sm;
+  __shared__ FlagTiles<TW> sm;
+  constexpr int kTX = TW;
   const int tid = threadIdx.x;
   const uint32_t n = tile_count(tl);
   for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
@@ -366,7 +376,7 @@ __global__ void __launch_bounds__(kTX* kTY) k_fs234(const __grid_constant__ KPar
 #pragma unroll 1
     for (int j = 0; j < (int)(kSTW / kTX); j++) {
       const int tx = sx * (int)(kSTW / kTX) + j;
-      if (tx * kTX < (int)p.nx) live |= fs234_tile<S, C, M, ODD>(p, tx, sy, tid, sm);
+      if (tx * kTX < (int)p.nx) live |= fs234_tile<S, C, M, ODD, TW>(p, tx, sy, tid, sm);
       __syncthreads();
     }
     live = __syncthreads_or(live);
@@ -419,11 +429,11 @@ __global__ void k_build_lists(const uint32_t* __restrict__ nz, uint32_t* __restr
 template <class S, class C, class M>
 void launch_fs1(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl, uint32_t grid) {
   if (hw) {
-    if (odd) k_fs1<S, C, M, true, true><<<grid, kBlock, 0, st>>>(kp, tl);
-    else k_fs1<S, C, M, true, false><<<grid, kBlock, 0, st>>>(kp, tl);
+    if (odd) k_fs1<S, C, M, true, true><<<grid, kListBlock, 0, st>>>(kp, tl);
+    else k_fs1<S, C, M, true, false><<<grid, kListBlock, 0, st>>>(kp, tl);
   } else {
-    if (odd) k_fs1<S, C, M, false, true><<<grid, kBlock, 0, st>>>(kp, tl);
-    else k_fs1<S, C, M, false, false><<<grid, kBlock, 0, st>>>(kp, tl);
+    if (odd) k_fs1<S, C, M, false, true><<<grid, kListBlock, 0, st>>>(kp, tl);
+    else k_fs1<S, C, M, false, false><<<grid, kListBlock, 0, st>>>(kp, tl);
   }
 }
 
@@ -434,15 +444,21 @@ void launch_apply_recon(const KParams& kp, cudaStream_t st, uint32_t odd) {
 
 template <class S, class C, class M>
 void launch_fs234(const KParams& kp, cudaStream_t st, uint32_t odd, const TileList& tl, uint32_t grid, uint32_t* nz) {
-  if (odd) k_fs234<S, C, M, true><<<grid, kTX * kTY, 0, st>>>(kp, tl, nz);
-  else k_fs234<S, C, M, false><<<grid, kTX * kTY, 0, st>>>(kp, tl, nz);
+  if (tl.ntiles <= kWideTiles) {
+    if (odd) k_fs234<S, C, M, true, 128><<<grid, 128 * kTY, 0, st>>>(kp, tl, nz);
+    else k_fs234<S, C, M, false, 128><<<grid, 128 * kTY, 0, st>>>(kp, tl, nz);
+  } else {
+    if (odd) k_fs234<S, C, M, true, 32><<<grid, 32 * kTY, 0, st>>>(kp, tl, nz);
+    else k_fs234<S, C, M, false, 32><<<grid, 32 * kTY, 0, st>>>(kp, tl, nz);
+  }
 }
 
 template <class S, class C, class M>
 int fs_blocks_per_sm(int which) {
   int n = 0;
-  if (which == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fs1<S, C, M, true, false>, kBlock, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fs234<S, C, M, false>, kTX * kTY, 0);
+  if (which == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fs1<S, C, M, true, false>, kListBlock, 0);
+  else if (which == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fs234<S, C, M, false, 128>, 128 * kTY, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fs234<S, C, M, false, 32>, 32 * kTY, 0);
   return n > 0 ? n : 1;
 }
 

@@ -54,17 +54,18 @@ __global__ void __launch_bounds__(kBlock, FLB_SC_MIN_BLOCKS) k_sc_scalar(const _
 
 // Free surface: the listed super-tiles, one row of a super-tile per warp.
 template <class S, class C, class M, bool HW, bool ODD, bool FU>
-__global__ void __launch_bounds__(kBlock, FLB_SC_MIN_BLOCKS) k_sc_list(const __grid_constant__ KParams p,
-                                                                       const TileList tl) {
+__global__ void __launch_bounds__(kListBlock, 2048 / kListBlock) k_sc_list(const __grid_constant__ KParams p,
+                                                                           const TileList tl) {
   const uint32_t n = tile_count(tl);
-  const uint32_t lane = threadIdx.x & 31u, row = threadIdx.x >> 5;
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t row = warp % kSTH, chunk = warp / kSTH, cpr = (blockDim.x >> 5) / kSTH;
   for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
     const uint32_t t = tile_at(tl, i);
     const uint32_t y = (t / tl.nsx) * kSTH + row;
     if (y >= p.ny) continue;
     const uint32_t xb = (t % tl.nsx) * kSTW + lane;
 #pragma unroll 1
-    for (uint32_t j = 0; j < kSTW; j += 32)
+    for (uint32_t j = chunk * 32u; j < kSTW; j += 32u * cpr)
       if (xb + j < p.nx) sc_cell<S, C, M, true, HW, true, ODD, FU>(p, xb + j, y);
   }
 }
@@ -593,11 +594,11 @@ template <class S, class C, class M, bool FU>
 static void launch_sc_list_f(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl,
                              uint32_t grid) {
   if (hw) {
-    if (odd) k_sc_list<S, C, M, true, true, FU><<<grid, kBlock, 0, st>>>(kp, tl);
-    else k_sc_list<S, C, M, true, false, FU><<<grid, kBlock, 0, st>>>(kp, tl);
+    if (odd) k_sc_list<S, C, M, true, true, FU><<<grid, kListBlock, 0, st>>>(kp, tl);
+    else k_sc_list<S, C, M, true, false, FU><<<grid, kListBlock, 0, st>>>(kp, tl);
   } else {
-    if (odd) k_sc_list<S, C, M, false, true, FU><<<grid, kBlock, 0, st>>>(kp, tl);
-    else k_sc_list<S, C, M, false, false, FU><<<grid, kBlock, 0, st>>>(kp, tl);
+    if (odd) k_sc_list<S, C, M, false, true, FU><<<grid, kListBlock, 0, st>>>(kp, tl);
+    else k_sc_list<S, C, M, false, false, FU><<<grid, kListBlock, 0, st>>>(kp, tl);
   }
 }
 
@@ -611,8 +612,8 @@ void launch_sc_list(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, c
 template <class S, class C, class M>
 int sc_list_blocks_per_sm() {
   int n = 0, m = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sc_list<S, C, M, true, false, false>, kBlock, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_sc_list<S, C, M, true, false, true>, kBlock, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sc_list<S, C, M, true, false, false>, kListBlock, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_sc_list<S, C, M, true, false, true>, kListBlock, 0);
   n = n < m ? n : m;
   return n > 0 ? n : 1;
 }
