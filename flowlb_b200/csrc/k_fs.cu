@@ -161,6 +161,9 @@ __global__ void k_apply_recon(const __grid_constant__ KParams p, uint32_t odd) {
 // the grid's super-tile count (kWideTiles).
 constexpr int kTY = 8, kHalo = 3;
 constexpr uint32_t kWideTiles = 4096;
+#ifndef FLB_FS_WIDE_MIN_BLOCKS
+#define FLB_FS_WIDE_MIN_BLOCKS 2
+#endif
 __device__ __forceinline__ int wrapi(int v, int n) {
   v %= n;
   return v < 0 ? v + n : v;
@@ -188,6 +191,23 @@ __device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int
   const int nx = (int)p.nx, ny = (int)p.ny;
   const int x0 = tx * kTX - kHalo, y0 = ty * kTY - kHalo;
   const uint8_t* flags = p.flags;
+  // this thread's cell: its own values are loaded now, so that their latency
+  // overlaps the staging of the flags and the stencil stages
+  const int gx = tx * kTX + tid % kTX, gy = ty * kTY + tid / kTX;
+  const bool in = gx < nx && gy < ny;
+  const uint32_t idx = in ? (uint32_t)gx + (uint32_t)gy * (uint32_t)nx : 0u;
+  M* Ms = static_cast<M*>(p.mass);
+  M* Exs = static_cast<M*>(p.excess);
+  const C* R = static_cast<const C*>(p.rho);
+  uint8_t old = 0;
+  M m_old = M(0), ex_old = M(0);
+  C rho_own = C(0);
+  if (in) {
+    old = p.flags_out[idx];
+    m_old = Ms[idx];
+    ex_old = Exs[idx];
+    rho_own = R[idx];
+  }
   for (int k = tid; k < kSX * kSY; k += kTX * kTY) {
     const int lx = k % kSX, ly = k / kSX;
     s0[ly][lx] = flags[wrapi(x0 + lx, nx) + wrapi(y0 + ly, ny) * nx];
@@ -239,9 +259,8 @@ __device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int
   }
   __syncthreads();
   const int lx = tid % kTX + kHalo, ly = tid / kTX + kHalo;
-  const int gx = tx * kTX + tid % kTX, gy = ty * kTY + tid / kTX;
-  if (gx >= nx || gy >= ny) return false;
-  const uint32_t N = p.N, idx = (uint32_t)gx + (uint32_t)gy * (uint32_t)nx;
+  if (!in) return false;
+  const uint32_t N = p.N;
   const uint8_t f1 = s1[ly][lx];
   const uint8_t f3 = s2[ly][lx];
   const uint8_t fin = s3[ly][lx];
@@ -257,9 +276,7 @@ __device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int
   //    zeros; a gas cell with no fluid or interface neighbour keeps its mass,
   //    lbmKernel2D.cu:296, so nothing else is assumed about them).
   const bool trust = p.trust_prev != 0;
-  const uint8_t old = p.flags_out[idx];
   if (!trust || old != fin) p.flags_out[idx] = fin;
-  const C* R = static_cast<const C*>(p.rho);
   const C* U = static_cast<const C*>(p.u);
   uint32_t nb[9];
   neighbours((uint32_t)gx, (uint32_t)gy, (uint32_t)nx, (uint32_t)ny, nb);
@@ -295,10 +312,7 @@ __device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int
   const uint8_t sw0 = s0[ly][lx] & (kFGI | kGasInterface);
   const bool gas_stays = trust && sw4 == kGas && sw0 == kGas;
   const bool keep_phi = gas_stays || (trust && sw4 == kFluid && sw0 == kFluid);
-  M* Ms = static_cast<M*>(p.mass);
-  M* Exs = static_cast<M*>(p.excess);
-  const C rho = sw4 == kGas ? C(0) : R[idx];  // the gas case does not use the density
-  const M m_old = Ms[idx];
+  const C rho = sw4 == kGas ? C(0) : rho_own;  // the gas case does not use the density
   M m = m_old;
   M ex = 0.0f, ph = 0.0f;
   switch (f3 & (kFGI | kGasInterface)) {
@@ -350,7 +364,7 @@ __device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int
   ex = cont > 0 ? ex / (float)cont : 0.0f;
   if (gas_stays) {
     if (!same_bits(m, m_old)) Ms[idx] = m;
-    if (!same_bits(ex, Exs[idx])) Exs[idx] = ex;
+    if (!same_bits(ex, ex_old)) Exs[idx] = ex;
   } else {
     Ms[idx] = m;
     Exs[idx] = ex;
@@ -363,7 +377,7 @@ __device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int
 // super-tile and records in nz whether the super-tile holds fluid or
 // interface cells afterwards.
 template <class S, class C, class M, bool ODD, int TW>
-__global__ void __launch_bounds__(TW* kTY) k_fs234(const __grid_constant__ KParams p, const TileList tl,
+__global__ void __launch_bounds__(TW* kTY, TW == 128 ? FLB_FS_WIDE_MIN_BLOCKS : 6) k_fs234(const __grid_constant__ KParams p, const TileList tl,
                                                     uint32_t* __restrict__ nz) {
   __shared__ FlagTiles<TW> sm;
   constexpr int kTX = TW;
