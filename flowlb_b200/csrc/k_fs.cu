@@ -164,9 +164,13 @@ constexpr uint32_t kWideTiles = 4096;
 #ifndef FLB_FS_WIDE_MIN_BLOCKS
 #define FLB_FS_WIDE_MIN_BLOCKS 2
 #endif
+// periodic index; halos of in-range tiles need one add or subtract, the
+// modulo is only reached on grids narrower than a tile
 __device__ __forceinline__ int wrapi(int v, int n) {
-  v %= n;
-  return v < 0 ? v + n : v;
+  if (v < 0) v += n;
+  else if (v >= n) v -= n;
+  if ((unsigned)v >= (unsigned)n) v = ((v % n) + n) % n;
+  return v;
 }
 
 template <int TW>
