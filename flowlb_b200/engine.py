@@ -35,6 +35,8 @@ EXPORTS = [
     "flb_adjoint_desc_init", "flb_adjoint_create", "flb_adjoint_set_porosity", "flb_adjoint_set_force",
     "flb_adjoint_forward", "flb_adjoint_backward", "flb_adjoint_timing", "flb_adjoint_destroy",
     "flb_adjoint_last_error",
+    "flb_setup_from_files", "flb_setup_free", "flb_setup_initial_flags", "flb_setup_write_mesh_vti",
+    "flb_create_from_files", "flb_write_vti", "flb_write_vti_series", "flb_run_from_files",
 ]
 
 
@@ -56,6 +58,31 @@ class AdjointDesc(C.Structure):
         ("steps", C.c_uint64), ("window", C.c_uint64), ("checkpoint_every", C.c_uint32), ("device", C.c_int32),
         ("stream", C.c_void_p),
     ]
+
+
+class SetupStruct(C.Structure):
+    _fields_ = [
+        ("nx", C.c_uint32), ("ny", C.c_uint32), ("x_min", C.c_double), ("y_min", C.c_double),
+        ("z_min", C.c_double), ("spacing", C.c_double), ("flags", C.c_void_p), ("desc", CaseDesc),
+        ("time_steps", C.c_uint64), ("save_every", C.c_uint64), ("time_simulation", C.c_float),
+        ("time_save", C.c_float), ("nu_lattice", C.c_float), ("length_to_si", C.c_double),
+        ("time_to_si", C.c_double), ("mass_to_si", C.c_double), ("velocity_to_si", C.c_double),
+        ("rho_to_si", C.c_double), ("graphics_api", C.c_int32), ("reference_precision", C.c_int32),
+        ("cuda_block", C.c_uint32 * 3), ("error", C.c_char * 256),
+    ]
+
+
+VTI_UINT8, VTI_FLOAT32, VTI_FLOAT64 = 0, 1, 2
+
+
+class VtiField(C.Structure):
+    _fields_ = [("name", C.c_char_p), ("type", C.c_int32), ("components", C.c_int32), ("data", C.c_void_p),
+                ("to_si", C.c_double), ("flip_y", C.c_int32)]
+
+
+class RunInfo(C.Structure):
+    _fields_ = [("steps", C.c_uint64), ("files", C.c_uint32), ("directory", C.c_char * 512),
+                ("error", C.c_char * 256)]
 
 
 class FlowLBError(RuntimeError):
@@ -120,6 +147,15 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "flb_adjoint_timing": (C.c_int, [H, C.POINTER(C.c_double)]),
         "flb_adjoint_destroy": (C.c_int, [H]),
         "flb_adjoint_last_error": (C.c_char_p, [H]),
+        "flb_setup_from_files": (C.c_int, [C.c_char_p, C.c_char_p, C.c_int, C.POINTER(SetupStruct)]),
+        "flb_setup_free": (None, [C.POINTER(SetupStruct)]),
+        "flb_setup_initial_flags": (C.c_int, [C.POINTER(SetupStruct), C.c_void_p]),
+        "flb_setup_write_mesh_vti": (C.c_int, [C.POINTER(SetupStruct), C.c_char_p]),
+        "flb_create_from_files": (C.c_int, [C.c_char_p, C.c_char_p, C.POINTER(H)]),
+        "flb_write_vti": (C.c_int, [C.c_char_p, C.c_uint32, C.c_uint32, C.c_double, C.c_double, C.c_double,
+                                    C.c_double, C.POINTER(VtiField), C.c_uint32]),
+        "flb_write_vti_series": (C.c_int, [C.c_char_p, C.c_uint32, C.c_double]),
+        "flb_run_from_files": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_uint64, C.POINTER(RunInfo)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -313,6 +349,95 @@ class Solver:
 
     def load_checkpoint(self, path: str):
         self._check(load_library().flb_load_checkpoint(self._h, path.encode()))
+
+    @classmethod
+    def from_files(cls, geometry_txt: str, options_txt: str) -> "Solver":
+        """``flb_create_from_files``: the case FlowLB's ``App::calculate`` would
+        run from these two files, in the reference's modes."""
+        L = load_library()
+        st_setup = Setup(geometry_txt, options_txt)  # raises with the reader's message
+        h = C.c_void_p()
+        st = L.flb_create_from_files(geometry_txt.encode(), options_txt.encode(), C.byref(h))
+        if st != 0:
+            raise FlowLBError(st, "flb_create_from_files failed")
+        self = cls.__new__(cls)
+        self._h = h
+        self.nx, self.ny, self.N = st_setup.nx, st_setup.ny, st_setup.nx * st_setup.ny
+        self._desc = st_setup.desc
+        self.free_surface = bool(st_setup.desc.free_surface)
+        self.precision = int(st_setup.desc.precision)
+        return self
+
+
+class Setup:
+    """``flb_setup_from_files``: Geometry.txt + OptionsCalc.txt to geometry
+    flags, tau, force, inlet velocity and loop bounds (host only, no GPU)."""
+
+    def __init__(self, geometry_txt: str, options_txt: str, mesh_only: bool = False):
+        L = load_library()
+        s = SetupStruct()
+        st = L.flb_setup_from_files(geometry_txt.encode(), options_txt.encode(), int(mesh_only), C.byref(s))
+        if st != 0:
+            raise FlowLBError(st, s.error.decode(errors="replace"))
+        try:
+            self.nx, self.ny = int(s.nx), int(s.ny)
+            self.flags = np.ctypeslib.as_array(C.cast(s.flags, C.POINTER(C.c_uint8)), (self.ny, self.nx)).copy()
+            init = np.empty((self.ny, self.nx), np.uint8)
+            st = L.flb_setup_initial_flags(C.byref(s), init.ctypes.data)
+            if st != 0:
+                raise FlowLBError(st, "flb_setup_initial_flags failed")
+            self.initial_flags = init
+            self.origin = (s.x_min, s.y_min, s.z_min)
+            self.spacing = s.spacing
+            d = CaseDesc()
+            C.memmove(C.byref(d), C.byref(s.desc), C.sizeof(CaseDesc))
+            d.flags = None
+            self.desc = d
+            self.time_steps, self.save_every = int(s.time_steps), int(s.save_every)
+            self.time_simulation, self.time_save = float(s.time_simulation), float(s.time_save)
+            self.nu_lattice = float(s.nu_lattice)
+            self.units = dict(length=s.length_to_si, time=s.time_to_si, mass=s.mass_to_si,
+                              velocity=s.velocity_to_si, rho=s.rho_to_si)
+            self.graphics_api, self.reference_precision = int(s.graphics_api), int(s.reference_precision)
+            self.cuda_block = tuple(int(v) for v in s.cuda_block)
+        finally:
+            L.flb_setup_free(C.byref(s))
+
+    def write_mesh_vti(self, path: str):
+        """App::createDomain's mesh.vti for these flags."""
+        write_vti(path, [("Flags", self.initial_flags.ravel(), 1, 1.0, False)], self.nx, self.ny,
+                  self.origin, self.spacing)
+
+
+def write_vti(path: str, fields, nx: int, ny: int, origin=(0.0, 0.0, 0.0), spacing: float = 1.0):
+    """``flb_write_vti``.  ``fields``: (name, array, components, to_si, flip_y)
+    with arrays of uint8, float32 or float64 holding components x N values."""
+    L = load_library()
+    keep = []
+    arr = (VtiField * max(1, len(fields)))()
+    kinds = {np.dtype(np.uint8): VTI_UINT8, np.dtype(np.float32): VTI_FLOAT32, np.dtype(np.float64): VTI_FLOAT64}
+    for k, (name, data, comps, to_si, flip) in enumerate(fields):
+        a = np.ascontiguousarray(data)
+        if a.dtype not in kinds or a.size != comps * nx * ny:
+            raise ValueError(f"field {name}: need {comps}*{nx}*{ny} values of uint8/float32/float64")
+        nm = name.encode()
+        keep += [a, nm]
+        arr[k] = VtiField(nm, kinds[a.dtype], int(comps), a.ctypes.data, float(to_si), int(bool(flip)))
+    st = L.flb_write_vti(path.encode(), nx, ny, float(origin[0]), float(origin[1]), float(origin[2]),
+                         float(spacing), arr, len(fields))
+    if st != 0:
+        raise FlowLBError(st, f"flb_write_vti({path}) failed")
+
+
+def run_from_files(geometry_txt: str, options_txt: str, save_dir: str, max_steps: int = 0) -> dict:
+    """``flb_run_from_files``: FlowLB's headless run from its two input files."""
+    L = load_library()
+    info = RunInfo()
+    st = L.flb_run_from_files(geometry_txt.encode(), options_txt.encode(), save_dir.encode(), int(max_steps),
+                              C.byref(info))
+    if st != 0:
+        raise FlowLBError(st, info.error.decode(errors="replace"))
+    return dict(steps=int(info.steps), files=int(info.files), directory=info.directory.decode())
 
 
 class Batch:

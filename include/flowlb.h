@@ -265,6 +265,97 @@ FLB_API flb_status flb_adjoint_timing(flb_adjoint a, double ms[2]);
 FLB_API flb_status flb_adjoint_destroy(flb_adjoint a);
 FLB_API const char* flb_adjoint_last_error(flb_adjoint a);
 
+/* ---- File-based set-up: Geometry.txt + OptionsCalc.txt ------------------ */
+/* What App::calculate (src/ui/app.cpp:241-310) derives from the two input
+ * files before the solver starts: GeometryReader::readGeometryOptions
+ * (src/io/reader.cpp:1192-1217) and Mesh::init (src/geometry/mesh.cpp:11-51),
+ * CalculationReader::readOptionsCalculation (reader.cpp:694-713), the unit
+ * conversion (src/utils.cpp:7-82, runCuda.cu:71-79), the geometry sweep of
+ * initData (src/initData.h:220-317), tau and the body force
+ * (src/cuda/cudaInitData.cu:57-82) and the loop bounds (runCuda.cu:497-499).
+ * Host code only: no CUDA call is made. */
+typedef struct flb_setup {
+  uint32_t nx, ny;              /* lattice size (Mesh::calculateNumberPointsMesh) */
+  double x_min, y_min, z_min;   /* mesh origin (m) */
+  double spacing;               /* SIZE (m) */
+  uint8_t* flags;               /* nx*ny geometry flags, owned here (flb_setup_free) */
+  flb_case_desc desc;           /* ready for flb_create, in the reference's modes (IMPLICIT walls,
+                                   REFERENCE free surface and arithmetic); desc.flags == flags */
+  uint64_t time_steps;          /* T: the reference loop runs t = 0..T, T+1 steps */
+  uint64_t save_every;          /* tSave: results after the steps with t % tSave == 0 */
+  float time_simulation, time_save;  /* TIME_SIMULATION, TIME_SAVE (s) */
+  float nu_lattice;             /* kinematic viscosity in lattice units (float, as h_nu) */
+  double length_to_si, time_to_si, mass_to_si, velocity_to_si, rho_to_si;  /* FLB::Units */
+  int32_t graphics_api;         /* GRAPHICS_API: 0 NONE, 1 OPENGL (the engine is headless either way) */
+  int32_t reference_precision;  /* PRECISION as read: 16, 32 or 64 */
+  uint32_t cuda_block[3];       /* CUDA_BLOCK_SIZE as read (checked, not used) */
+  char error[256];              /* the reader's message when a call fails */
+} flb_setup;
+
+/* Reads both files.  mesh_only = 0 follows App::calculate (every option read
+ * and checked); mesh_only = 1 follows App::createDomain (src/ui/app.cpp:202-238,
+ * reader.cpp:715-742): only TYPE_PROBLEM, the four boundaries and the initial
+ * conditions are read, and only the boundaries are checked.  CSV_2D shapes are
+ * read from the folder of the file that names them.  Errors: FLB_ERR_IO for a
+ * file that cannot be opened, FLB_ERR_UNSUPPORTED for 3D, otherwise
+ * FLB_ERR_INVALID_ARGUMENT with the reader's message in out->error. */
+FLB_API flb_status flb_setup_from_files(const char* geometry_txt, const char* options_txt, int mesh_only,
+                                        flb_setup* out);
+FLB_API void flb_setup_free(flb_setup* s);
+
+/* The flags after the free-surface sweep of initFreeSurfaceFlags
+ * (src/initData.cpp:13-37): the content of FlowLB's mesh.vti, and of
+ * FLB_FIELD_FLAGS right after flb_create.  out holds nx*ny bytes. */
+FLB_API flb_status flb_setup_initial_flags(const flb_setup* s, uint8_t* out);
+
+/* App::createDomain's mesh.vti (app.cpp:233-238): the initial flags as one
+ * UInt8 field, written by the VTK writer below. */
+FLB_API flb_status flb_setup_write_mesh_vti(const flb_setup* s, const char* path);
+
+/* flb_setup_from_files (mesh_only = 0) followed by flb_create of its desc:
+ * the whole set-up half of h_launchCudaCalculations2D from the two files.
+ * The reader's message goes to stderr; flb_setup_from_files returns it. */
+FLB_API flb_status flb_create_from_files(const char* geometry_txt, const char* options_txt, flb_handle* out);
+
+/* ---- VTK ImageData output (src/io/writer.cpp:15-252) --------------------- */
+enum { FLB_VTI_UINT8 = 0, FLB_VTI_FLOAT32 = 1, FLB_VTI_FLOAT64 = 2 };
+
+typedef struct flb_vti_field {
+  const char* name;       /* DataArray Name: "Flags", "U", "rho", "phi" */
+  int32_t type;           /* FLB_VTI_*: element type of data and the DataArray type */
+  int32_t components;     /* 1 scalar; 2 or 3: component k of cell i at data[i + k*N] */
+  const void* data;       /* host memory, N = nx*ny cells per component */
+  double to_si;           /* factor applied to every value (the writer's constantToSI) */
+  int32_t flip_y;         /* nonzero: the second component is negated */
+} flb_vti_field;
+
+/* One ASCII .vti file byte-identical to FlowLB's VTIWriter for the same
+ * fields: values printed as std::ostream prints a double by default,
+ * origin and spacing as std::to_string does. */
+FLB_API flb_status flb_write_vti(const char* path, uint32_t nx, uint32_t ny, double x0, double y0, double z0,
+                                 double spacing, const flb_vti_field* fields, uint32_t n_fields);
+
+/* <directory>/loaderFiles.vti.series listing result_0.vti .. result_<n-1>.vti
+ * at times i * time_interval (Writer::createTimeSeriesFile, writer.cpp:163-182). */
+FLB_API flb_status flb_write_vti_series(const char* directory, uint32_t n_files, double time_interval);
+
+typedef struct flb_run_info {
+  uint64_t steps;         /* time steps run */
+  uint32_t files;         /* result_<i>.vti files written */
+  char directory[512];    /* the results_<k> folder created under save_dir */
+  char error[256];
+} flb_run_info;
+
+/* The headless run of FlowLB from its two input files
+ * (h_runCudaMonoFluidNoGraphics2D / h_runCudaFreeSurfaceNoGraphics2D,
+ * runCuda.cu:460-528): set-up as flb_create_from_files, then T+1 steps (at
+ * most max_steps when nonzero), and after every step with t % tSave == 0 the
+ * reference's fields written to save_dir/results_<k>/result_<i>.vti with the
+ * series file rewritten; mono-fluid U and rho in SI units, free-surface
+ * fields in lattice units, as the reference writes them. */
+FLB_API flb_status flb_run_from_files(const char* geometry_txt, const char* options_txt, const char* save_dir,
+                                      uint64_t max_steps, flb_run_info* info);
+
 FLB_API const char* flb_last_error(flb_handle h);
 FLB_API const char* flb_status_string(flb_status s);
 FLB_API const char* flb_version(void);
