@@ -369,6 +369,21 @@ flb_status initialise(flb_engine* h) {
   return FLB_OK;
 }
 
+// Runs a visualisation launch into dst (device) or through a temporary (host).
+template <class Launch>
+flb_status viz_run(flb_handle h, size_t bytes, void* dst, int on_device, Launch&& launch) {
+  uint8_t* out = static_cast<uint8_t*>(dst);
+  if (!on_device) FLB_CUDA(h, cudaMallocAsync((void**)&out, bytes, h->stream));
+  launch(out);
+  h->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess && !on_device) e = cudaMemcpyAsync(dst, out, bytes, cudaMemcpyDeviceToHost, h->stream);
+  if (!on_device) cudaFreeAsync(out, h->stream);
+  if (e != cudaSuccess) return cuda_fail(h, e, "visualisation kernel");
+  FLB_CUDA(h, cudaStreamSynchronize(h->stream));
+  return FLB_OK;
+}
+
 }  // namespace
 
 namespace flb {
@@ -767,6 +782,66 @@ FLB_API flb_status flb_write_field(flb_handle h, int field, const void* src, int
   h->lists_valid = false;
   FLB_CUDA(h, cudaStreamSynchronize(h->stream));
   return FLB_OK;
+}
+
+// ---- headless visualisation (k_viz.cu) --------------------------------------
+// Output goes straight to dst when it is device memory, else through a
+// stream-ordered temporary that is copied to the host.
+
+FLB_API flb_status flb_viz_velocity(flb_handle h, float* dst, int on_device) {
+  if (!h || !dst) return FLB_ERR_INVALID_ARGUMENT;
+  DeviceGuard guard(h->device);
+  const bool dbl = h->c_size == 8;
+  return viz_run(h, 2 * sizeof(float) * (size_t)h->N, dst, on_device, [&](uint8_t* out) {
+    if (dbl) flb::launch_viz_uv<double>(h->d_u, (float*)out, h->N, h->stream);
+    else flb::launch_viz_uv<float>(h->d_u, (float*)out, h->N, h->stream);
+  });
+}
+
+FLB_API flb_status flb_viz_shade(flb_handle h, int quantity, const float* colormap_rgb, uint32_t n_colors,
+                                 float max_value, float min_value, uint8_t* rgba, int on_device) {
+  if (!h || !rgba || !colormap_rgb) return FLB_ERR_INVALID_ARGUMENT;
+  if (quantity < FLB_VIZ_UX || quantity > FLB_VIZ_PRESSURE)
+    return fail(h, FLB_ERR_INVALID_ARGUMENT, "quantity must be FLB_VIZ_UX, _UY, _MAGNITUDE or _PRESSURE");
+  if (n_colors == 0 || n_colors > 4096) return fail(h, FLB_ERR_INVALID_ARGUMENT, "n_colors must be 1..4096");
+  DeviceGuard guard(h->device);
+  float* cmap = nullptr;
+  const size_t cbytes = 3 * sizeof(float) * (size_t)n_colors;
+  FLB_CUDA(h, cudaMallocAsync((void**)&cmap, cbytes, h->stream));
+  cudaError_t e = cudaMemcpyAsync(cmap, colormap_rgb, cbytes, cudaMemcpyHostToDevice, h->stream);
+  if (e != cudaSuccess) {
+    cudaFreeAsync(cmap, h->stream);
+    return cuda_fail(h, e, "cudaMemcpyAsync");
+  }
+  const bool dbl = h->c_size == 8;
+  flb_status s = viz_run(h, 4 * (size_t)h->N, rgba, on_device, [&](uint8_t* out) {
+    if (dbl) flb::launch_viz_shade<double>(h->d_u, h->N, quantity, cmap, n_colors, max_value, min_value, out, h->stream);
+    else flb::launch_viz_shade<float>(h->d_u, h->N, quantity, cmap, n_colors, max_value, min_value, out, h->stream);
+  });
+  cudaFreeAsync(cmap, h->stream);
+  return s;
+}
+
+FLB_API flb_status flb_viz_isoline(flb_handle h, int field, float iso_value, uint32_t width, uint32_t height,
+                                   const uint32_t camera_bounds[4], uint8_t* image, int on_device) {
+  if (!h || !image || !camera_bounds) return FLB_ERR_INVALID_ARGUMENT;
+  if (field != FLB_FIELD_U && !(field == FLB_FIELD_PHI && h->fs))
+    return fail(h, FLB_ERR_INVALID_ARGUMENT, "field must be FLB_FIELD_U, or FLB_FIELD_PHI with a free surface");
+  if (width == 0 || height == 0 || width > 32768 || height > 32768)
+    return fail(h, FLB_ERR_INVALID_ARGUMENT, "image size must be 1..32768 in each direction");
+  const uint32_t* b = camera_bounds;
+  if (!(b[0] < b[1] && b[1] <= h->nx && b[2] < b[3] && b[3] <= h->ny))
+    return fail(h, FLB_ERR_INVALID_ARGUMENT, "camera bounds must satisfy b0 < b1 <= nx and b2 < b3 <= ny");
+  DeviceGuard guard(h->device);
+  const size_t bytes = (size_t)width * height;
+  const bool vec = field == FLB_FIELD_U;
+  const bool dbl = vec ? h->c_size == 8 : h->m_size == 8;
+  const void* src = vec ? h->d_u : h->d_phi;
+  return viz_run(h, bytes, image, on_device, [&](uint8_t* out) {
+    cudaMemsetAsync(out, 0, bytes, h->stream);
+    if (dbl) flb::launch_viz_isoline<double>(src, vec, h->nx, h->ny, iso_value, width, height, b, out, h->stream);
+    else flb::launch_viz_isoline<float>(src, vec, h->nx, h->ny, iso_value, width, height, b, out, h->stream);
+  });
 }
 
 FLB_API flb_status flb_total_mass(flb_handle h, double* mass) {

@@ -49,6 +49,16 @@ int fs_blocks_per_sm(int which);  // 0: FS_1, 1: FS_2..4 on 128-wide tiles, 2: o
 void launch_build_lists(const uint32_t* nz, uint32_t* nz_prev, uint32_t nsx, uint32_t nsy, int prev_unknown,
                         uint32_t* list_sc, uint32_t* list_fs, uint32_t* counts, cudaStream_t st);
 
+// headless visualisation (k_viz.cu), T = the arithmetic type of u / the mass type of phi
+template <class T>
+void launch_viz_uv(const void* u, float* out, uint32_t N, cudaStream_t st);
+template <class T>
+void launch_viz_shade(const void* u, uint32_t N, int quantity, const float* cmap, uint32_t n, float vmax, float vmin,
+                      uint8_t* rgba, cudaStream_t st);
+template <class T>
+void launch_viz_isoline(const void* f, bool vec, uint32_t nx, uint32_t ny, float iso, uint32_t width, uint32_t height,
+                        const uint32_t bounds[4], uint8_t* img, cudaStream_t st);
+
 // initial state
 void launch_init_flags(const uint8_t* geo, uint8_t* flags, uint32_t nx, uint32_t ny, int free_surface, void* mass,
                        void* excess, void* phi, int mass_f64, cudaStream_t st);

@@ -37,6 +37,7 @@ EXPORTS = [
     "flb_adjoint_last_error",
     "flb_setup_from_files", "flb_setup_free", "flb_setup_initial_flags", "flb_setup_write_mesh_vti",
     "flb_create_from_files", "flb_write_vti", "flb_write_vti_series", "flb_run_from_files",
+    "flb_viz_velocity", "flb_viz_shade", "flb_viz_isoline",
 ]
 
 
@@ -73,6 +74,7 @@ class SetupStruct(C.Structure):
 
 
 VTI_UINT8, VTI_FLOAT32, VTI_FLOAT64 = 0, 1, 2
+VIZ_UX, VIZ_UY, VIZ_MAGNITUDE, VIZ_PRESSURE = 0, 1, 2, 3
 
 
 class VtiField(C.Structure):
@@ -156,6 +158,10 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
                                     C.c_double, C.POINTER(VtiField), C.c_uint32]),
         "flb_write_vti_series": (C.c_int, [C.c_char_p, C.c_uint32, C.c_double]),
         "flb_run_from_files": (C.c_int, [C.c_char_p, C.c_char_p, C.c_char_p, C.c_uint64, C.POINTER(RunInfo)]),
+        "flb_viz_velocity": (C.c_int, [H, C.c_void_p, C.c_int]),
+        "flb_viz_shade": (C.c_int, [H, C.c_int, C.c_void_p, C.c_uint32, C.c_float, C.c_float, C.c_void_p, C.c_int]),
+        "flb_viz_isoline": (C.c_int, [H, C.c_int, C.c_float, C.c_uint32, C.c_uint32, C.POINTER(C.c_uint32),
+                                      C.c_void_p, C.c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -349,6 +355,29 @@ class Solver:
 
     def load_checkpoint(self, path: str):
         self._check(load_library().flb_load_checkpoint(self._h, path.encode()))
+
+    # -- headless visualisation ----------------------------------------------
+    def viz_velocity(self) -> np.ndarray:
+        """(ny, nx, 2) float32: the velocity image of save2DDataToOpenGL."""
+        out = np.empty((self.ny, self.nx, 2), np.float32)
+        self._check(load_library().flb_viz_velocity(self._h, out.ctypes.data, 0))
+        return out
+
+    def viz_shade(self, quantity: int, colormap: np.ndarray, max_value: float, min_value: float) -> np.ndarray:
+        """(ny, nx, 4) uint8 RGBA: one shaded pixel per node."""
+        cm = np.ascontiguousarray(colormap, np.float32).reshape(-1, 3)
+        out = np.empty((self.ny, self.nx, 4), np.uint8)
+        self._check(load_library().flb_viz_shade(self._h, int(quantity), cm.ctypes.data, cm.shape[0],
+                                                 float(max_value), float(min_value), out.ctypes.data, 0))
+        return out
+
+    def viz_isoline(self, field: int, iso_value: float, width: int, height: int, bounds=None) -> np.ndarray:
+        """(height, width) uint8 image of the iso-line (255 on the line)."""
+        b = (C.c_uint32 * 4)(*(bounds if bounds is not None else (0, self.nx, 0, self.ny)))
+        out = np.empty((height, width), np.uint8)
+        self._check(load_library().flb_viz_isoline(self._h, int(field), float(iso_value), int(width), int(height), b,
+                                                   out.ctypes.data, 0))
+        return out
 
     @classmethod
     def from_files(cls, geometry_txt: str, options_txt: str) -> "Solver":

@@ -265,6 +265,38 @@ FLB_API flb_status flb_adjoint_timing(flb_adjoint a, double ms[2]);
 FLB_API flb_status flb_adjoint_destroy(flb_adjoint a);
 FLB_API const char* flb_adjoint_last_error(flb_adjoint a);
 
+/* ---- Headless visualisation (device buffers in place of the OpenGL view) -- */
+/* FlowLB's OpenGL loops (runCuda.cu:130-458) fill interop surfaces from the
+ * velocity and fill-level fields and shade them with GLSL.  These calls draw
+ * the same pictures into plain buffers (host memory when on_device = 0, the
+ * handle's GPU when 1), from the handle's current fields; no graphics API is
+ * involved. */
+enum { FLB_VIZ_UX = 0, FLB_VIZ_UY = 1, FLB_VIZ_MAGNITUDE = 2, FLB_VIZ_PRESSURE = 3 };
+
+/* save2DDataToOpenGL (src/cuda/cudaUtils.cu:107-118): u as nx*ny interleaved
+ * float pairs (ux, uy), row y at [2*(x + y*nx)]. */
+FLB_API flb_status flb_viz_velocity(flb_handle h, float* dst, int on_device);
+
+/* The texture*2D fragment shaders (assets/shaders/{monoFluid,freeSurface}/):
+ * per node v = ux, uy or |u| (the pressure shader also shades |u|),
+ * s = max((v - min_value)/(max_value - min_value), 0), colour = the n_colors
+ * RGB colour map (host memory, 3 floats per entry, n_colors <= 4096) sampled at
+ * s with linear filtering and mirrored-repeat wrapping as OpenGL does
+ * (OpenGLTexture1D, OpenGLTexture.cpp:44-53); written as RGBA8 (alpha 255),
+ * one pixel per node, rows as the lattice. */
+FLB_API flb_status flb_viz_shade(flb_handle h, int quantity, const float* colormap_rgb, uint32_t n_colors,
+                                 float max_value, float min_value, uint8_t* rgba, int on_device);
+
+/* d_CreateIsoSurfaceVector2D (src/cuda/cudaIsosurface.cuh:33-199): the
+ * iso-line v = iso_value of |u| (field FLB_FIELD_U) or of the fill level
+ * (FLB_FIELD_PHI, free surface) over the camera window of lattice nodes
+ * [b0, b1) x [b2, b3), drawn by marching squares and Bresenham lines as 255
+ * into a width x height uint8 image that is cleared first.  The reference
+ * draws the fill level through its two-component path (reading past the end
+ * of phi); this reads phi as a scalar. */
+FLB_API flb_status flb_viz_isoline(flb_handle h, int field, float iso_value, uint32_t width, uint32_t height,
+                                   const uint32_t camera_bounds[4], uint8_t* image, int on_device);
+
 /* ---- File-based set-up: Geometry.txt + OptionsCalc.txt ------------------ */
 /* What App::calculate (src/ui/app.cpp:241-310) derives from the two input
  * files before the solver starts: GeometryReader::readGeometryOptions
