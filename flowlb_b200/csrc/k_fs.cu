@@ -173,101 +173,177 @@ __device__ __forceinline__ int wrapi(int v, int n) {
   return v;
 }
 
+// Bit-plane form of the stencil chain.  For each row of the tile and of its
+// 3-row halo, and each 32-cell word of the tile plus one word on either side,
+// a warp ballot turns 32 flag bytes into predicate masks (bit i = cell i of the
+// word).  FS_2's and FS_3's "any neighbour with property P" is then an 8-way
+// dilation of a mask (shifts and ORs across neighbouring words and rows), the
+// flag rewrites are bitwise logic on whole words, and FS_4's neighbour count
+// is a popcount of a 3x3 window; each cell finally reads its own bits.  The
+// words at the outer ends of a row lack a neighbour word, so their outermost
+// bits are wrong after each dilation; the three stages reach at most the third
+// bit from either end, and only the innermost 3 bits of those words (the halo)
+// are read.
 template <int TW>
-struct FlagTiles {
-  static constexpr int kSX = TW + 2 * kHalo, kSY = kTY + 2 * kHalo;
-  uint8_t s0[kSY][kSX];  // after stream-collide
-  uint8_t s1[kSY][kSX];  // after FS_2
-  uint8_t s2[kSY][kSX];  // after FS_3
-  uint8_t s3[kSY][kSX];  // after FS_4 conversion
+struct FlagMasks {
+  static constexpr int kW = TW / 32 + 2;      // words per row
+  static constexpr int kR = kTY + 2 * kHalo;  // rows
+  // from the flags after stream-collide (s0)
+  uint32_t a[kR][kW];      // (f & 5) == 5   IF
+  uint32_t gas[kR][kW];    // f & GAS
+  uint32_t gonly[kR][kW];  // (f & 6) == 2   gas, not interface
+  uint32_t gi[kR][kW];     // f & GAS_INTERFACE
+  uint32_t fl[kR][kW];     // FLUID set, INLET clear
+  uint32_t it[kR][kW];     // f & INTERFACE
+  uint32_t fb[kR][kW];     // f & FLUID
+  uint32_t sk[kR][kW];     // f & (WALL | MOVING_WALL | INLET)
+  // derived
+  uint32_t anyif[kR][kW];  // FS_2: a neighbour is IF
+  uint32_t ig1[kR][kW];    // after FS_2: (f & (GI | IG)) == IG
+  uint32_t p1[kR][kW];     // after FS_2: GAS bit
+  uint32_t p7[kR][kW];     // after FS_2: GAS_INTERFACE bit
+  uint32_t anyig[kR][kW];  // FS_3: a neighbour is IG (after FS_2)
+  uint32_t cnt[kR][kW];    // after FS_4's conversion: counted by FS_4's neighbour count
 };
 
-// One kTX x 8 tile (tile coordinates tx, ty) with the kTX*8 threads of the block;
+// 8-neighbourhood of bit i of word c, row r, of mask m (missing words read 0).
+template <int TW>
+__device__ __forceinline__ uint32_t dilate8(const uint32_t (&m)[FlagMasks<TW>::kR][FlagMasks<TW>::kW], int r,
+                                            int c) {
+  constexpr int kW = FlagMasks<TW>::kW;
+  uint32_t out = 0;
+#pragma unroll
+  for (int dr = -1; dr <= 1; dr++) {
+    const uint32_t w = m[r + dr][c];
+    const uint32_t l = c > 0 ? m[r + dr][c - 1] : 0u;
+    const uint32_t rt = c < kW - 1 ? m[r + dr][c + 1] : 0u;
+    const uint32_t sh = (w << 1) | (l >> 31) | (w >> 1) | (rt << 31);  // left and right neighbours
+    out |= dr ? (sh | w) : sh;
+  }
+  return out;
+}
+
+// Bits i-1, i, i+1 of row r around word c (c has words on both sides).
+template <int TW>
+__device__ __forceinline__ uint32_t window3(const uint32_t (&m)[FlagMasks<TW>::kR][FlagMasks<TW>::kW], int r, int c,
+                                            int i) {
+  const uint64_t v = ((uint64_t)m[r][c + 1] << 33) | ((uint64_t)m[r][c] << 1) | (uint64_t)(m[r][c - 1] >> 31);
+  return (uint32_t)(v >> i) & 7u;
+}
+
+template <int TW>
+__device__ __forceinline__ bool bit_at(const uint32_t (&m)[FlagMasks<TW>::kR][FlagMasks<TW>::kW], int r, int c,
+                                       int i) {
+  if (i < 0) {
+    c--;
+    i += 32;
+  } else if (i >= 32) {
+    c++;
+    i -= 32;
+  }
+  return (m[r][c] >> i) & 1u;
+}
+
+// One TW x 8 tile (tile coordinates tx, ty) with the TW*8 threads of the block;
 // every thread of the block must call it.  Returns whether this thread's cell
 // is fluid or interface after the pass.
 template <class S, class C, class M, bool ODD, int TW>
-__device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int tid, FlagTiles<TW>& sm) {
-  constexpr int kTX = TW, kSX = FlagTiles<TW>::kSX, kSY = FlagTiles<TW>::kSY;
-  auto& s0 = sm.s0;
-  auto& s1 = sm.s1;
-  auto& s2 = sm.s2;
-  auto& s3 = sm.s3;
+__device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int tid, FlagMasks<TW>& sm) {
+  constexpr int kTX = TW, kW = FlagMasks<TW>::kW, kR = FlagMasks<TW>::kR;
+  constexpr int kWarps = TW * kTY / 32;
   const int nx = (int)p.nx, ny = (int)p.ny;
-  const int x0 = tx * kTX - kHalo, y0 = ty * kTY - kHalo;
   const uint8_t* flags = p.flags;
   // this thread's cell: its own values are loaded now, so that their latency
-  // overlaps the staging of the flags and the stencil stages
+  // overlaps the mask building and the stencil stages
   const int gx = tx * kTX + tid % kTX, gy = ty * kTY + tid / kTX;
   const bool in = gx < nx && gy < ny;
   const uint32_t idx = in ? (uint32_t)gx + (uint32_t)gy * (uint32_t)nx : 0u;
   M* Ms = static_cast<M*>(p.mass);
   M* Exs = static_cast<M*>(p.excess);
   const C* R = static_cast<const C*>(p.rho);
-  uint8_t old = 0;
+  uint8_t old = 0, f0 = 0;
   M m_old = M(0), ex_old = M(0);
   C rho_own = C(0);
   if (in) {
+    f0 = flags[idx];
     old = p.flags_out[idx];
     m_old = Ms[idx];
     ex_old = Exs[idx];
     rho_own = R[idx];
   }
-  for (int k = tid; k < kSX * kSY; k += kTX * kTY) {
-    const int lx = k % kSX, ly = k / kSX;
-    s0[ly][lx] = flags[wrapi(x0 + lx, nx) + wrapi(y0 + ly, ny) * nx];
+  // masks of the flags after stream-collide
+  const int lane = tid & 31, warp = tid >> 5;
+  const int xw = tx * kTX - 32 + lane;  // word 0 starts one word left of the tile
+  for (int rw = warp; rw < kR * kW; rw += kWarps) {
+    const int r = rw / kW, c = rw % kW;
+    const uint8_t f = flags[wrapi(xw + 32 * c, nx) + wrapi(ty * kTY - kHalo + r, ny) * nx];
+    // one ballot per mask, stored as soon as it is formed (keeps registers free)
+#define FLB_MASK(dst, pred)                                  \
+  {                                                          \
+    const uint32_t b_ = __ballot_sync(0xffffffffu, (pred)); \
+    if (lane == 0) sm.dst[r][c] = b_;                        \
+  }
+    FLB_MASK(a, (f & kIF) == kIF)
+    FLB_MASK(gas, (f & kGas) != 0)
+    FLB_MASK(gonly, (f & kIG) == kGas)
+    FLB_MASK(gi, (f & kGasInterface) != 0)
+    FLB_MASK(fl, (f & (kFluid | kInlet)) == kFluid)
+    FLB_MASK(it, (f & kInterface) != 0)
+    FLB_MASK(fb, (f & kFluid) != 0)
+    FLB_MASK(sk, (f & (kWall | kMovingWall | kInlet)) != 0)
+#undef FLB_MASK
   }
   __syncthreads();
-  // FS_2: next to an IF cell, IG -> I and G -> GI
-  for (int k = tid; k < kSX * kSY; k += kTX * kTY) {
-    const int lx = k % kSX, ly = k / kSX;
-    if (lx < 1 || ly < 1 || lx >= kSX - 1 || ly >= kSY - 1) continue;
-    uint8_t f = s0[ly][lx];
-    bool any_if = false;
-#pragma unroll
-    for (int dy = -1; dy <= 1; dy++)
-#pragma unroll
-      for (int dx = -1; dx <= 1; dx++)
-        if (dx || dy) any_if |= (s0[ly + dy][lx + dx] & kIF) == kIF;
-    if (any_if) {
-      const uint8_t e = f & kIG;
-      if (e == kIG) f = (uint8_t)(f & ~kGas);
-      else if (e == kGas) f = (uint8_t)((f & ~kGas) | kGasInterface);
-    }
-    s1[ly][lx] = f;
+  // FS_2 on rows 1 .. kR-2: next to an IF cell, IG -> I and G -> GI
+  if (tid < (kR - 2) * kW) {
+    const int r = 1 + tid / kW, c = tid % kW;
+    const uint32_t any_if = dilate8<TW>(sm.a, r, c);
+    const uint32_t p1 = sm.gas[r][c] & ~any_if;
+    const uint32_t p7 = sm.gi[r][c] | (any_if & sm.gonly[r][c]);
+    sm.anyif[r][c] = any_if;
+    sm.p1[r][c] = p1;
+    sm.p7[r][c] = p7;
+    sm.ig1[r][c] = p1 & sm.it[r][c] & ~p7;
   }
   __syncthreads();
-  // FS_3 flags: next to an IG cell, F / IF (not inlet) -> I
-  for (int k = tid; k < kSX * kSY; k += kTX * kTY) {
-    const int lx = k % kSX, ly = k / kSX;
-    if (lx < 2 || ly < 2 || lx >= kSX - 2 || ly >= kSY - 2) continue;
-    uint8_t f = s1[ly][lx];
-    const uint8_t e = f & (kInletFluid | kInterface);
-    if (e != kInletFluid && (e == kFluid || e == kIF)) {
-      bool any_ig = false;
-#pragma unroll
-      for (int dy = -1; dy <= 1; dy++)
-#pragma unroll
-        for (int dx = -1; dx <= 1; dx++)
-          if (dx || dy) any_ig |= (s1[ly + dy][lx + dx] & (kGasInterface | kIG)) == kIG;
-      if (any_ig) f = (uint8_t)((f & ~kIF) | kInterface);
-    }
-    s2[ly][lx] = f;
-    // FS_4 conversion
-    uint8_t g = f;
-    if (!(g & (kWall | kMovingWall | kInlet))) {
-      const uint8_t sw = g & (kFGI | kGasInterface);
-      if (sw == kIF || sw == kIG) g = (uint8_t)(g & ~kInterface);
-      else if (sw == kGasInterface) g = (uint8_t)((g & ~kGasInterface) | kInterface);
-    }
-    s3[ly][lx] = g;
+  // FS_3 on rows 2 .. kR-3: next to an IG cell, F / IF (not inlet) -> I; then
+  // FS_4's conversion and the mask of the neighbours FS_4 counts
+  if (tid < (kR - 4) * kW) {
+    const int r = 2 + tid / kW, c = tid % kW;
+    const uint32_t any_ig = dilate8<TW>(sm.ig1, r, c);
+    const uint32_t conv = sm.fl[r][c] & any_ig;
+    const uint32_t P0 = sm.fb[r][c] & ~conv, P1 = sm.p1[r][c], P2 = sm.it[r][c] | conv, P7 = sm.p7[r][c];
+    const uint32_t go = ~sm.sk[r][c];
+    const uint32_t to_plain = go & ((P0 & ~P1 & P2 & ~P7) | (~P0 & P1 & P2 & ~P7));  // IF, IG lose the I bit
+    const uint32_t from_gi = go & (~P0 & ~P1 & ~P2 & P7);                          // GI -> I
+    const uint32_t P2f = (P2 & ~to_plain) | from_gi, P7f = P7 & ~from_gi;
+    sm.anyig[r][c] = any_ig;
+    sm.cnt[r][c] = p.fs_cons ? ((P0 ^ P2f) & ~P1 & go) : ((P0 | P2f) ^ P7f);
   }
   __syncthreads();
-  const int lx = tid % kTX + kHalo, ly = tid / kTX + kHalo;
   if (!in) return false;
+  const int lx = tid % kTX, ly = tid / kTX;
+  const int r = kHalo + ly, c = 1 + lx / 32, i = lx % 32;
+  const bool any_if = (sm.anyif[r][c] >> i) & 1u, any_ig = (sm.anyig[r][c] >> i) & 1u;
+  // the byte chain of the reference passes, for this cell
+  uint8_t f1 = f0;
+  if (any_if) {
+    const uint8_t e = f1 & kIG;
+    if (e == kIG) f1 = (uint8_t)(f1 & ~kGas);
+    else if (e == kGas) f1 = (uint8_t)((f1 & ~kGas) | kGasInterface);
+  }
+  uint8_t f3 = f1;
+  {
+    const uint8_t e = f3 & (kInletFluid | kInterface);
+    if (e != kInletFluid && (e == kFluid || e == kIF) && any_ig) f3 = (uint8_t)((f3 & ~kIF) | kInterface);
+  }
+  uint8_t fin = f3;
+  if (!(fin & (kWall | kMovingWall | kInlet))) {
+    const uint8_t sw = fin & (kFGI | kGasInterface);
+    if (sw == kIF || sw == kIG) fin = (uint8_t)(fin & ~kInterface);
+    else if (sw == kGasInterface) fin = (uint8_t)((fin & ~kGasInterface) | kInterface);
+  }
   const uint32_t N = p.N;
-  const uint8_t f1 = s1[ly][lx];
-  const uint8_t f3 = s2[ly][lx];
-  const uint8_t fin = s3[ly][lx];
   const bool live = (fin & (kWall | kMovingWall)) == 0 && ((fin & kFGI) == kFluid || (fin & kFGI) == kInterface);
   // Write skipping.  flags_out still holds this cell's flag after the previous
   // step's stream-collide ("old").  When the buffers come from consecutive
@@ -291,12 +367,13 @@ __device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int
     const int ddx[9] = {0, 1, -1, 0, 0, 1, -1, 1, -1};
     const int ddy[9] = {0, 0, 0, 1, -1, 1, -1, -1, 1};
 #pragma unroll
-    for (int i = 1; i < 9; i++) {
-      if (s1[ly + ddy[i]][lx + ddx[i]] & kIF) {
+    for (int k = 1; k < 9; k++) {
+      // FLUID or INTERFACE set after FS_2 (FS_2 changes neither bit)
+      if (bit_at<TW>(sm.fb, r + ddy[k], c, i + ddx[k]) || bit_at<TW>(sm.it, r + ddy[k], c, i + ddx[k])) {
         count += 1.0f;
-        lrho += R[nb[i]];
-        lux += U[nb[i]];
-        luy += U[nb[i] + N];
+        lrho += R[nb[k]];
+        lux += U[nb[k]];
+        luy += U[nb[k] + N];
       }
     }
     C rho = count > 0.0f ? lrho / count : 0.0f;
@@ -313,7 +390,7 @@ __device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int
   // FS_4 fields
   if (f3 & (kWall | kMovingWall | kInlet)) return live;
   const uint8_t sw4 = f3 & (kFGI | kGasInterface);
-  const uint8_t sw0 = s0[ly][lx] & (kFGI | kGasInterface);
+  const uint8_t sw0 = f0 & (kFGI | kGasInterface);
   const bool gas_stays = trust && sw4 == kGas && sw0 == kGas;
   const bool keep_phi = gas_stays || (trust && sw4 == kFluid && sw0 == kFluid);
   const C rho = sw4 == kGas ? C(0) : rho_own;  // the gas case does not use the density
@@ -348,22 +425,9 @@ __device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int
     default:
       break;
   }
-  int cont = 0;
-  const bool cons = p.fs_cons != 0;
-#pragma unroll
-  for (int dy = -1; dy <= 1; dy++)
-#pragma unroll
-    for (int dx = -1; dx <= 1; dx++) {
-      if (!dx && !dy) continue;
-      const uint8_t v = s3[ly + dy][lx + dx];  // converted flags
-      if (cons) {
-        const uint8_t ev = v & kFGI;
-        cont += (ev == kFluid || ev == kInterface) && !(v & (kWall | kMovingWall | kInlet));
-      } else {
-        const uint8_t ev = v & (kIF | kGasInterface);
-        cont += ev == kFluid || ev == kInterface || ev == kIF || ev == kGasInterface;
-      }
-    }
+  // FS_4's count of fluid / interface neighbours after the conversion
+  const int cont = __popc(window3<TW>(sm.cnt, r - 1, c, i)) + __popc(window3<TW>(sm.cnt, r, c, i) & 5u) +
+                   __popc(window3<TW>(sm.cnt, r + 1, c, i));
   m += cont > 0 ? 0.0f : ex;
   ex = cont > 0 ? ex / (float)cont : 0.0f;
   if (gas_stays) {
@@ -383,7 +447,7 @@ __device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int
 template <class S, class C, class M, bool ODD, int TW>
 __global__ void __launch_bounds__(TW* kTY, TW == 128 ? FLB_FS_WIDE_MIN_BLOCKS : 6) k_fs234(const __grid_constant__ KParams p, const TileList tl,
                                                     uint32_t* __restrict__ nz) {
-  __shared__ FlagTiles<TW> sm;
+  __shared__ FlagMasks<TW> sm;
   constexpr int kTX = TW;
   const int tid = threadIdx.x;
   const uint32_t n = tile_count(tl);

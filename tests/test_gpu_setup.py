@@ -32,7 +32,7 @@ def paths(case, directory=SETUP):
     return os.path.join(d, "Geometry.txt"), os.path.join(d, "OptionsCalc.txt")
 
 
-@pytest.mark.parametrize("case", ["damBreak", "cavity", "Poiseuille_plano", "modulos"])
+@pytest.mark.parametrize("case", ["damBreak", "Poiseuille_plano", "modulos"])
 def test_create_from_files_builds_reference_initial_flags(require_gpu, case):
     s = E.Solver.from_files(*paths(case))
     try:
@@ -43,6 +43,15 @@ def test_create_from_files_builds_reference_initial_flags(require_gpu, case):
         assert np.all(rho[~solid] == 1.0)
     finally:
         s.close()
+
+
+def test_create_from_files_rejects_an_inlet_in_the_last_cell(require_gpu):
+    """The cavity's lid is an INLET row that ends in the last cell, whose
+    inlet rule reads the density one cell past the end of the lattice
+    (lbmKernel2D.cu:334-340); creation refuses it before allocating."""
+    with pytest.raises(E.FlowLBError) as ei:
+        E.Solver.from_files(*paths("cavity"))
+    assert ei.value.status == 1
 
 
 def _short_run_inputs(tmp_path, case, time_simulation, time_save):
@@ -75,8 +84,9 @@ def _oracle_for(setup):
 
 
 # (case, TIME_SIMULATION, TIME_SAVE): 12 and 5 lattice steps for both (T = 1e-4 s
-# for damBreak, 1e-5 s for cavity), so 13 steps and saves after steps 0, 5, 10.
-RUNS = [("damBreak", 0.0012, 0.0005), ("cavity", 0.00012, 0.00005)]
+# for damBreak, 2.5e-4 s for the channel), so 13 steps and saves after steps 0,
+# 5 and 10.
+RUNS = [("damBreak", 0.0012, 0.0005), ("Poiseuille_plano", 0.003, 0.00125)]
 
 
 @pytest.mark.parametrize("case,t_sim,t_save", RUNS)
