@@ -314,20 +314,29 @@ int max_clusters(flb_batch b, int cs, int threads) {
 }
 
 // Timed search over cluster sizes and cluster counts: probe steps of the whole
-// batch from the initial state for every candidate; the fastest wins.
+// batch from the initial state for every candidate; the fastest wins.  The
+// counts include one sized so that the cases active at a time fit in about
+// half of the L2 (each cluster holds one case at a time): over thousands of
+// steps such a case is stepped from L2 after its first step.  The probe is long
+// enough (100 steps by default) for that reuse to show.
 flb_status btune(flb_batch b, uint32_t probe_steps) {
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
+  int l2 = 0;
+  cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, b->device);
+  // bytes a case touches per step: 9 FP32 populations, flags, wall mask
+  const double case_bytes = (double)b->cells / b->n * (9.0 * 4.0 + 2.0);
+  const int l2_fit = std::max(1, (int)(0.5 * (double)l2 / std::max(1.0, case_bytes)));
   struct Cand {
     int cs, clusters, threads;
   };
   std::vector<Cand> cands;
-  for (int threads : {256, 512, 1024}) {
-    for (int cs : {1, 2, 4, 8, 16}) {
+  for (int threads : {512, 1024}) {
+    for (int cs : {2, 4, 8, 16}) {
       const int mx = max_clusters(b, cs, threads);
       if (mx <= 0) continue;
       const int per_sm = std::max(1, nsm / cs);
-      for (int k : {per_sm / 2, per_sm, 2 * per_sm, mx}) {
+      for (int k : {l2_fit, per_sm / 2, per_sm, 2 * per_sm, mx}) {
         const int cl = std::min(std::max(k, 1), std::min(mx, (int)b->n));
         bool seen = false;
         for (auto& c : cands) seen |= c.cs == cs && c.clusters == cl && c.threads == threads;
@@ -477,7 +486,7 @@ FLB_API flb_status flb_batch_create(const flb_case_desc* cases, uint32_t n, int 
   if (e != cudaSuccess) return bail(bcuda(b, e, "cudaMemcpy"));
   flb_status s = FLB_OK;
   if (autotune) {
-    s = btune(b, autotune > 1 ? (uint32_t)autotune : 20u);
+    s = btune(b, autotune > 1 ? (uint32_t)autotune : 100u);
   } else {
     int nsm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);

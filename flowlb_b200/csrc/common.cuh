@@ -16,6 +16,8 @@
 // S/C/M: storage / arithmetic / mass types.
 #pragma once
 
+#include <utility>
+
 #include <cstdint>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
@@ -98,6 +100,43 @@ struct TileList {
   const uint32_t* count;
   uint32_t ntiles, nsx;
   int all;
+};
+
+// Programmatic dependent launch.  The free-surface step kernels are launched
+// with launch_pdl, so the next kernel on the stream (also inside a CUDA graph)
+// may be scheduled while this one drains.  Each such kernel calls pdl_wait()
+// before its first read of anything the previous kernel wrote (it returns once
+// that kernel has completed and its writes are visible; it returns at once
+// when the kernel was launched without the attribute), then pdl_trigger() to
+// let its own successor be scheduled.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+
+template <class... KArgs, class... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
+// What the list build of a step needs (k_build_lists, or the last block of
+// the flag pass on grids of at most kWideTiles super-tiles).
+struct ListBuild {
+  uint32_t* nz_prev;
+  uint32_t nsx, nsy;
+  int prev_unknown;
+  uint32_t* list_sc;
+  uint32_t* list_fs;
+  uint32_t* counts;  // [2]: lengths of list_sc and list_fs
+  uint32_t* done;    // blocks of the flag pass finished so far (0 between launches)
 };
 
 __device__ __forceinline__ uint32_t tile_count(const TileList& tl) { return tl.all ? tl.ntiles : *tl.count; }

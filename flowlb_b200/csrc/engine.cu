@@ -57,7 +57,7 @@ struct flb_engine {
   uint32_t* d_nz = nullptr;       // super-tile holds fluid/interface after the last flag pass
   uint32_t* d_nz_prev = nullptr;  // the same one step earlier
   uint32_t* d_list[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [step parity][0 FS_1/SC, 1 flag pass]
-  uint32_t* d_lcount = nullptr;   // [step parity][2] list lengths
+  uint32_t* d_lcount = nullptr;   // [step parity][2] list lengths, then the flag pass's finished-block counter
   bool lists_valid = false;       // lists of the current parity were built by the previous step
   uint32_t grid_sc = 0, grid_fs1 = 0, grid_fs234 = 0;
   KParams kp{};
@@ -131,8 +131,8 @@ struct Ops {
   static void fs1(flb_engine* h, uint32_t odd, const TileList& tl) {
     launch_fs1<S, C, M>(h->kp, h->stream, odd, h->hw, tl, h->grid_fs1);
   }
-  static void fs234(flb_engine* h, uint32_t odd, const TileList& tl) {
-    launch_fs234<S, C, M>(h->kp, h->stream, odd, tl, h->grid_fs234, h->d_nz);
+  static int fs234(flb_engine* h, uint32_t odd, const TileList& tl, const ListBuild& lb) {
+    return launch_fs234<S, C, M>(h->kp, h->stream, odd, tl, h->grid_fs234, h->d_nz, lb);
   }
   static void grids(flb_engine* h, int nsm) {
     h->grid_sc = (uint32_t)(nsm * sc_list_blocks_per_sm<S, C, M>());
@@ -218,10 +218,11 @@ FsLists fs_lists(flb_engine* h, uint64_t t) {
   return L;
 }
 
-void build_lists(flb_engine* h, uint64_t t, const FsLists& L) {
+// The list build of the step at t: the lists of t+1 and their lengths.
+ListBuild list_build(flb_engine* h, uint64_t t, const FsLists& L) {
   const int np = (int)((t + 1) & 1u);
-  launch_build_lists(h->d_nz, h->d_nz_prev, h->nsx, h->nsy, L.all ? 1 : 0, h->d_list[np][0], h->d_list[np][1],
-                     L.next_count, h->stream);
+  return ListBuild{h->d_nz_prev, h->nsx, h->nsy, L.all ? 1 : 0, h->d_list[np][0], h->d_list[np][1], L.next_count,
+                   h->d_lcount + 4};
 }
 
 // Issues the passes of one time step at t on the stream.
@@ -236,14 +237,12 @@ uint64_t issue_step(flb_engine* h, uint64_t t, bool write_macro) {
   if (h->fs) {
     h->kp.trust_prev = h->trust ? 1 : 0;
     const FsLists L = fs_lists(h, t);
-    cudaMemsetAsync(L.next_count, 0, 2 * sizeof(uint32_t), h->stream);
+    const ListBuild lb = list_build(h, t, L);
     dispatch(h, [&](auto ops) {
       ops.fs1(h, odd, L.sc);
       ops.sc_list(h, odd, L.sc);
-      ops.fs234(h, odd, L.fs);
+      k = 2 + (uint64_t)ops.fs234(h, odd, L.fs, lb);
     });
-    build_lists(h, t, L);
-    k = 4;
     h->cur ^= 1;
     h->trust = true;
     h->lists_valid = true;
@@ -565,7 +564,7 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
       {(void**)&h->d_list[0][1], tiles * sizeof(uint32_t), h->fs},
       {(void**)&h->d_list[1][0], tiles * sizeof(uint32_t), h->fs},
       {(void**)&h->d_list[1][1], tiles * sizeof(uint32_t), h->fs},
-      {(void**)&h->d_lcount, 4 * sizeof(uint32_t), h->fs},
+      {(void**)&h->d_lcount, 5 * sizeof(uint32_t), h->fs},
   };
   for (Alloc& a : allocs) {
     if (!a.need) continue;
@@ -573,6 +572,9 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
     if (e != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc"));
   }
   if (h->fs) {
+    // list lengths and the flag pass's finished-block counter start at zero
+    cudaError_t e0 = cudaMemsetAsync(h->d_lcount, 0, 5 * sizeof(uint32_t), h->stream);
+    if (e0 != cudaSuccess) return bail(cuda_fail(h, e0, "cudaMemsetAsync"));
     int nsm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
     dispatch(h, [&](auto ops) { ops.grids(h, nsm > 0 ? nsm : 1); });
@@ -910,6 +912,7 @@ FLB_API flb_status flb_run_pass(flb_handle h, int pass) {
   // alone, stream-collide sees no parked populations, and FS_1 writes its
   // rebuilt populations into the population array like the reference kernel
   if (pass == 0 && recon) FLB_CUDA(h, cudaMemsetAsync(h->d_recon_mask, 0, h->N, h->stream));
+  uint64_t k = (pass == 1 && recon) ? 2 : 1;
   dispatch(h, [&](auto ops) {
     if (pass == 0) {
       if (h->fs) ops.sc_list(h, odd, all);
@@ -917,11 +920,12 @@ FLB_API flb_status flb_run_pass(flb_handle h, int pass) {
     } else if (pass == 1) {
       ops.fs1(h, odd, all);
     } else {
-      ops.fs234(h, odd, all);
+      // the lists it builds go unused: lists_valid is false
+      k = (uint64_t)ops.fs234(h, odd, all, list_build(h, h->t, fs_lists(h, h->t)));
     }
     if (pass == 1 && recon) ops.apply_recon(h, odd);
   });
-  h->launches += (pass == 1 && recon) ? 2 : 1;
+  h->launches += k;
   if (pass == 2)  // keep the current buffer index tied to t
     FLB_CUDA(h, cudaMemcpyAsync(h->d_flags[h->cur], h->d_flags[h->cur ^ 1], h->N, cudaMemcpyDeviceToDevice,
                                 h->stream));
@@ -948,16 +952,16 @@ FLB_API flb_status flb_profile_steps(flb_handle h, uint64_t n, double pass_ms[3]
     if (h->fs) {
       h->kp.trust_prev = h->trust ? 1 : 0;
       const FsLists L = fs_lists(h, h->t);
-      cudaMemsetAsync(L.next_count, 0, 2 * sizeof(uint32_t), h->stream);
+      const ListBuild lb = list_build(h, h->t, L);
       cudaEventRecord(ev[0], h->stream);
       dispatch(h, [&](auto ops) { ops.fs1(h, odd, L.sc); });
       cudaEventRecord(ev[1], h->stream);
       dispatch(h, [&](auto ops) { ops.sc_list(h, odd, L.sc); });
       cudaEventRecord(ev[2], h->stream);
-      dispatch(h, [&](auto ops) { ops.fs234(h, odd, L.fs); });
-      build_lists(h, h->t, L);
+      int kf = 0;
+      dispatch(h, [&](auto ops) { kf = ops.fs234(h, odd, L.fs, lb); });
       cudaEventRecord(ev[3], h->stream);
-      h->launches += 4;
+      h->launches += 2 + (uint64_t)kf;
       h->cur ^= 1;
       h->trust = true;
       h->lists_valid = true;

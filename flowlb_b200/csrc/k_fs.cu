@@ -107,9 +107,14 @@ __device__ __forceinline__ void fs1_cell(const KParams& p, uint32_t x, uint32_t 
 }
 
 // The listed super-tiles, one row of a super-tile per warp.
+// FS_1 blocks: 512 threads, two per SM at 64 registers, so that a step's
+// listed super-tiles (a few hundred on a 2048x512 dam break) run in one wave.
+constexpr int kFs1Block = 512;
 template <class S, class C, class M, bool HW, bool ODD>
-__global__ void __launch_bounds__(kListBlock, 1024 / kListBlock) k_fs1(const __grid_constant__ KParams p,
+__global__ void __launch_bounds__(kFs1Block, 2) k_fs1(const __grid_constant__ KParams p,
                                                                        const TileList tl) {
+  pdl_wait();
+  pdl_trigger();
   const uint32_t n = tile_count(tl);
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t row = warp % kSTH, chunk = warp / kSTH, cpr = (blockDim.x >> 5) / kSTH;
@@ -271,12 +276,24 @@ __device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int
     ex_old = Exs[idx];
     rho_own = R[idx];
   }
-  // masks of the flags after stream-collide
+  // masks of the flags after stream-collide: every flag byte a lane needs is
+  // loaded first, so the loads of all its row-words are in flight together
   const int lane = tid & 31, warp = tid >> 5;
   const int xw = tx * kTX - 32 + lane;  // word 0 starts one word left of the tile
-  for (int rw = warp; rw < kR * kW; rw += kWarps) {
+  constexpr int kRW = kR * kW, kIters = (kRW + kWarps - 1) / kWarps;
+  uint8_t fv[kIters];
+#pragma unroll
+  for (int k = 0; k < kIters; k++) {
+    const int rw = warp + k * kWarps;
     const int r = rw / kW, c = rw % kW;
-    const uint8_t f = flags[wrapi(xw + 32 * c, nx) + wrapi(ty * kTY - kHalo + r, ny) * nx];
+    fv[k] = rw < kRW ? flags[wrapi(xw + 32 * c, nx) + wrapi(ty * kTY - kHalo + r, ny) * nx] : 0;
+  }
+#pragma unroll
+  for (int k = 0; k < kIters; k++) {
+    const int rw = warp + k * kWarps;  // the same for the whole warp
+    if (rw >= kRW) break;
+    const int r = rw / kW, c = rw % kW;
+    const uint8_t f = fv[k];
     // one ballot per mask, stored as soon as it is formed (keeps registers free)
 #define FLB_MASK(dst, pred)                                  \
   {                                                          \
@@ -441,14 +458,37 @@ __device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int
   return live;
 }
 
-// The listed super-tiles: each block runs the tile pass on the 4 tiles of a
+// Whether super-tile t is visited next step by stream-collide and FS_1 (sc)
+// and by the flag pass (fs); see k_build_lists.  Updates nz_prev[t].
+__device__ __forceinline__ void list_flags(const uint32_t* nz, const ListBuild& lb, uint32_t t, bool& sc, bool& fs) {
+  const uint32_t nsx = lb.nsx, nsy = lb.nsy;
+  const uint32_t sx = t % nsx, sy = t / nsx;
+  const uint32_t own = __ldcg(nz + t);
+  uint32_t near = 0;
+  for (int dy = -1; dy <= 1; dy++)
+    for (int dx = -1; dx <= 1; dx++) {
+      const uint32_t xx = (sx + nsx + dx) % nsx, yy = (sy + nsy + dy) % nsy;
+      near |= __ldcg(nz + xx + yy * nsx);
+    }
+  sc = own != 0;
+  fs = near != 0 || lb.prev_unknown || lb.nz_prev[t] != 0;
+  lb.nz_prev[t] = own;
+}
+
+// The listed super-tiles: each block runs the tile pass on the tiles of a
 // super-tile and records in nz whether the super-tile holds fluid or
-// interface cells afterwards.
-template <class S, class C, class M, bool ODD, int TW>
-__global__ void __launch_bounds__(TW* kTY, TW == 128 ? FLB_FS_WIDE_MIN_BLOCKS : 6) k_fs234(const __grid_constant__ KParams p, const TileList tl,
-                                                    uint32_t* __restrict__ nz) {
+// interface cells afterwards.  With BUILD, the last block to finish (a ticket
+// taken after a fence) compacts the next step's super-tile lists, in tile
+// order, in place of a separate k_build_lists launch.
+template <class S, class C, class M, bool ODD, int TW, bool BUILD>
+__global__ void __launch_bounds__(TW* kTY, TW == 128 ? FLB_FS_WIDE_MIN_BLOCKS : 6)
+    k_fs234(const __grid_constant__ KParams p, const TileList tl, uint32_t* __restrict__ nz, const ListBuild lb) {
   __shared__ FlagMasks<TW> sm;
+  __shared__ uint32_t wsum[2][TW * kTY / 32];
+  __shared__ int last;
   constexpr int kTX = TW;
+  pdl_wait();
+  pdl_trigger();
   const int tid = threadIdx.x;
   const uint32_t n = tile_count(tl);
   for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
@@ -464,8 +504,52 @@ __global__ void __launch_bounds__(TW* kTY, TW == 128 ? FLB_FS_WIDE_MIN_BLOCKS : 
     live = __syncthreads_or(live);
     if (tid == 0) nz[t] = live ? 1u : 0u;
   }
+  if constexpr (BUILD) {
+    __syncthreads();
+    if (tid == 0) {
+      __threadfence();  // this block's nz writes before its ticket
+      last = atomicAdd(lb.done, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    constexpr int kWarps = TW * kTY / 32;
+    const uint32_t lane = tid & 31, warp = tid >> 5, T = lb.nsx * lb.nsy;
+    uint32_t base_sc = 0, base_fs = 0;
+    for (uint32_t t0 = 0; t0 < T; t0 += TW * kTY) {
+      const uint32_t t = t0 + tid;
+      bool sc = false, fs = false;
+      if (t < T) list_flags(nz, lb, t, sc, fs);
+      const uint32_t bsc = __ballot_sync(0xffffffffu, sc), bfs = __ballot_sync(0xffffffffu, fs);
+      if (lane == 0) {
+        wsum[0][warp] = __popc(bsc);
+        wsum[1][warp] = __popc(bfs);
+      }
+      __syncthreads();
+      uint32_t off_sc = base_sc, off_fs = base_fs, tot_sc = 0, tot_fs = 0;
+      for (int w = 0; w < kWarps; w++) {
+        const uint32_t a = wsum[0][w], b = wsum[1][w];
+        if (w < (int)warp) {
+          off_sc += a;
+          off_fs += b;
+        }
+        tot_sc += a;
+        tot_fs += b;
+      }
+      const uint32_t below = (1u << lane) - 1u;
+      if (sc) lb.list_sc[off_sc + __popc(bsc & below)] = t;
+      if (fs) lb.list_fs[off_fs + __popc(bfs & below)] = t;
+      base_sc += tot_sc;
+      base_fs += tot_fs;
+      __syncthreads();  // wsum is rewritten by the next chunk
+    }
+    if (tid == 0) {
+      lb.counts[0] = base_sc;
+      lb.counts[1] = base_fs;
+      *lb.done = 0;  // ready for the next launch
+    }
+  }
 }
-
 
 // Compacts the super-tiles for the next step: FS_1 and stream-collide visit
 // super-tiles holding fluid or interface cells; the flag pass also visits
@@ -511,11 +595,11 @@ __global__ void k_build_lists(const uint32_t* __restrict__ nz, uint32_t* __restr
 template <class S, class C, class M>
 void launch_fs1(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl, uint32_t grid) {
   if (hw) {
-    if (odd) k_fs1<S, C, M, true, true><<<grid, kListBlock, 0, st>>>(kp, tl);
-    else k_fs1<S, C, M, true, false><<<grid, kListBlock, 0, st>>>(kp, tl);
+    if (odd) launch_pdl(k_fs1<S, C, M, true, true>, grid, kFs1Block, st, kp, tl);
+    else launch_pdl(k_fs1<S, C, M, true, false>, grid, kFs1Block, st, kp, tl);
   } else {
-    if (odd) k_fs1<S, C, M, false, true><<<grid, kListBlock, 0, st>>>(kp, tl);
-    else k_fs1<S, C, M, false, false><<<grid, kListBlock, 0, st>>>(kp, tl);
+    if (odd) launch_pdl(k_fs1<S, C, M, false, true>, grid, kFs1Block, st, kp, tl);
+    else launch_pdl(k_fs1<S, C, M, false, false>, grid, kFs1Block, st, kp, tl);
   }
 }
 
@@ -524,37 +608,41 @@ void launch_apply_recon(const KParams& kp, cudaStream_t st, uint32_t odd) {
   k_apply_recon<S, C><<<dim3((kp.nx + kBlock - 1) / kBlock, kp.ny), kBlock, 0, st>>>(kp, odd);
 }
 
+// The flag pass and the list build of the next step: one launch on grids of
+// at most kWideTiles super-tiles (the build runs in the last block), else the
+// flag pass and k_build_lists.  Returns the number of kernels launched.
 template <class S, class C, class M>
-void launch_fs234(const KParams& kp, cudaStream_t st, uint32_t odd, const TileList& tl, uint32_t grid, uint32_t* nz) {
+int launch_fs234(const KParams& kp, cudaStream_t st, uint32_t odd, const TileList& tl, uint32_t grid, uint32_t* nz,
+                 const ListBuild& lb) {
   if (tl.ntiles <= kWideTiles) {
-    if (odd) k_fs234<S, C, M, true, 128><<<grid, 128 * kTY, 0, st>>>(kp, tl, nz);
-    else k_fs234<S, C, M, false, 128><<<grid, 128 * kTY, 0, st>>>(kp, tl, nz);
-  } else {
-    if (odd) k_fs234<S, C, M, true, 32><<<grid, 32 * kTY, 0, st>>>(kp, tl, nz);
-    else k_fs234<S, C, M, false, 32><<<grid, 32 * kTY, 0, st>>>(kp, tl, nz);
+    if (odd) launch_pdl(k_fs234<S, C, M, true, 128, true>, grid, 128 * kTY, st, kp, tl, nz, lb);
+    else launch_pdl(k_fs234<S, C, M, false, 128, true>, grid, 128 * kTY, st, kp, tl, nz, lb);
+    return 1;
   }
+  cudaMemsetAsync(lb.counts, 0, 2 * sizeof(uint32_t), st);
+  if (odd) k_fs234<S, C, M, true, 32, false><<<grid, 32 * kTY, 0, st>>>(kp, tl, nz, lb);
+  else k_fs234<S, C, M, false, 32, false><<<grid, 32 * kTY, 0, st>>>(kp, tl, nz, lb);
+  const uint32_t T = lb.nsx * lb.nsy;
+  k_build_lists<<<(T + kBlock - 1) / kBlock, kBlock, 0, st>>>(nz, lb.nz_prev, lb.nsx, lb.nsy, lb.prev_unknown,
+                                                              lb.list_sc, lb.list_fs, lb.counts);
+  return 2;
 }
 
 template <class S, class C, class M>
 int fs_blocks_per_sm(int which) {
   int n = 0;
-  if (which == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fs1<S, C, M, true, false>, kListBlock, 0);
-  else if (which == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fs234<S, C, M, false, 128>, 128 * kTY, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fs234<S, C, M, false, 32>, 32 * kTY, 0);
+  if (which == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fs1<S, C, M, true, false>, kFs1Block, 0);
+  else if (which == 1)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fs234<S, C, M, false, 128, true>, 128 * kTY, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fs234<S, C, M, false, 32, false>, 32 * kTY, 0);
   return n > 0 ? n : 1;
-}
-
-void launch_build_lists(const uint32_t* nz, uint32_t* nz_prev, uint32_t nsx, uint32_t nsy, int prev_unknown,
-                        uint32_t* list_sc, uint32_t* list_fs, uint32_t* counts, cudaStream_t st) {
-  const uint32_t T = nsx * nsy;
-  k_build_lists<<<(T + kBlock - 1) / kBlock, kBlock, 0, st>>>(nz, nz_prev, nsx, nsy, prev_unknown, list_sc, list_fs,
-                                                              counts);
 }
 
 #define FLB_INSTANTIATE(S, C, M)                                                                                  \
   template void launch_fs1<S, C, M>(const KParams&, cudaStream_t, uint32_t, bool, const TileList&, uint32_t);     \
   template void launch_apply_recon<S, C, M>(const KParams&, cudaStream_t, uint32_t);                             \
-  template void launch_fs234<S, C, M>(const KParams&, cudaStream_t, uint32_t, const TileList&, uint32_t, uint32_t*); \
+  template int launch_fs234<S, C, M>(const KParams&, cudaStream_t, uint32_t, const TileList&, uint32_t, uint32_t*,   \
+                                     const ListBuild&);                                                          \
   template int fs_blocks_per_sm<S, C, M>(int);
 FLB_FOR_EACH_VARIANT(FLB_INSTANTIATE)
 #undef FLB_INSTANTIATE

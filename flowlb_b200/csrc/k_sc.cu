@@ -56,6 +56,8 @@ __global__ void __launch_bounds__(kBlock, FLB_SC_MIN_BLOCKS) k_sc_scalar(const _
 template <class S, class C, class M, bool HW, bool ODD, bool FU>
 __global__ void __launch_bounds__(kListBlock, 2048 / kListBlock) k_sc_list(const __grid_constant__ KParams p,
                                                                            const TileList tl) {
+  pdl_wait();
+  pdl_trigger();
   const uint32_t n = tile_count(tl);
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t row = warp % kSTH, chunk = warp / kSTH, cpr = (blockDim.x >> 5) / kSTH;
@@ -594,11 +596,11 @@ template <class S, class C, class M, bool FU>
 static void launch_sc_list_f(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl,
                              uint32_t grid) {
   if (hw) {
-    if (odd) k_sc_list<S, C, M, true, true, FU><<<grid, kListBlock, 0, st>>>(kp, tl);
-    else k_sc_list<S, C, M, true, false, FU><<<grid, kListBlock, 0, st>>>(kp, tl);
+    if (odd) launch_pdl(k_sc_list<S, C, M, true, true, FU>, grid, kListBlock, st, kp, tl);
+    else launch_pdl(k_sc_list<S, C, M, true, false, FU>, grid, kListBlock, st, kp, tl);
   } else {
-    if (odd) k_sc_list<S, C, M, false, true, FU><<<grid, kListBlock, 0, st>>>(kp, tl);
-    else k_sc_list<S, C, M, false, false, FU><<<grid, kListBlock, 0, st>>>(kp, tl);
+    if (odd) launch_pdl(k_sc_list<S, C, M, false, true, FU>, grid, kListBlock, st, kp, tl);
+    else launch_pdl(k_sc_list<S, C, M, false, false, FU>, grid, kListBlock, st, kp, tl);
   }
 }
 

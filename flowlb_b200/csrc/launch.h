@@ -43,11 +43,10 @@ void launch_fs1(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const
 template <class S, class C, class M>
 void launch_apply_recon(const KParams& kp, cudaStream_t st, uint32_t odd);
 template <class S, class C, class M>
-void launch_fs234(const KParams& kp, cudaStream_t st, uint32_t odd, const TileList& tl, uint32_t grid, uint32_t* nz);
+int launch_fs234(const KParams& kp, cudaStream_t st, uint32_t odd, const TileList& tl, uint32_t grid, uint32_t* nz,
+                 const ListBuild& lb);
 template <class S, class C, class M>
 int fs_blocks_per_sm(int which);  // 0: FS_1, 1: FS_2..4 on 128-wide tiles, 2: on 32-wide tiles
-void launch_build_lists(const uint32_t* nz, uint32_t* nz_prev, uint32_t nsx, uint32_t nsy, int prev_unknown,
-                        uint32_t* list_sc, uint32_t* list_fs, uint32_t* counts, cudaStream_t st);
 
 // headless visualisation (k_viz.cu), T = the arithmetic type of u / the mass type of phi
 template <class T>

@@ -212,9 +212,9 @@ FLB_API flb_status flb_load_checkpoint(flb_handle h, const char* path);
  * all; no inlet/outlet cells) advanced together: flb_batch_step(b, k) is one
  * graph launch of one persistent kernel that runs all k steps of every case.
  * Each case ends bit-identical to k flb_step calls on its own handle.
- * autotune: 0 uses 8-CTA clusters, one CTA per SM; 1 (or a probe step count
- * > 1) times the candidate cluster sizes and counts on the batch itself and
- * keeps the fastest, then rebuilds the initial state.  The device, and the
+ * autotune: 0 uses 8-CTA clusters, one CTA per SM; 1 (100 probe steps) or a
+ * probe step count > 1 times the candidate cluster sizes and counts on the
+ * batch itself and keeps the fastest, then rebuilds the initial state.  The device, and the
  * stream if given, come from cases[0]. */
 typedef struct flb_batch_s* flb_batch;
 FLB_API flb_status flb_batch_create(const flb_case_desc* cases, uint32_t n, int autotune, flb_batch* out);
