@@ -59,6 +59,7 @@ struct flb_engine {
   uint32_t* d_list[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [step parity][0 FS_1/SC, 1 flag pass]
   uint32_t* d_lcount = nullptr;   // [step parity][2] list lengths, then the flag pass's finished-block counter
   bool lists_valid = false;       // lists of the current parity were built by the previous step
+  bool thin_tiles = false;        // a last super-tile column or row narrower than the flag pass's reach
   uint32_t grid_sc = 0, grid_fs1 = 0, grid_fs234 = 0;
   KParams kp{};
   // device buffers
@@ -221,8 +222,10 @@ FsLists fs_lists(flb_engine* h, uint64_t t) {
 // The list build of the step at t: the lists of t+1 and their lengths.
 ListBuild list_build(flb_engine* h, uint64_t t, const FsLists& L) {
   const int np = (int)((t + 1) & 1u);
-  return ListBuild{h->d_nz_prev, h->nsx, h->nsy, L.all ? 1 : 0, h->d_list[np][0], h->d_list[np][1], L.next_count,
-                   h->d_lcount + 4};
+  // a live cell can reach past a super-tile narrower than 3 cells into the
+  // one beyond it; such grids visit every super-tile in the flag pass
+  return ListBuild{h->d_nz_prev, h->nsx, h->nsy, (L.all || h->thin_tiles) ? 1 : 0, h->d_list[np][0],
+                   h->d_list[np][1], L.next_count, h->d_lcount + 4};
 }
 
 // Issues the passes of one time step at t on the stream.
@@ -536,6 +539,7 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
   const uint64_t blocks = (N + kBlock - 1) / kBlock;
   h->nsx = (h->nx + kSTW - 1) / kSTW;
   h->nsy = (h->ny + kSTH - 1) / kSTH;
+  h->thin_tiles = (h->nx % kSTW != 0 && h->nx % kSTW < 3) || (h->ny % kSTH != 0 && h->ny % kSTH < 3);
   h->ntiles = h->nsx * h->nsy;
   const uint64_t tiles = h->ntiles;
   Alloc allocs[] = {

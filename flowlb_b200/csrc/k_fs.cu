@@ -178,6 +178,16 @@ __device__ __forceinline__ int wrapi(int v, int n) {
   return v;
 }
 
+// ex / cont for a neighbour count of 1..8.  Counts 1, 2, 4 and 8 scale by an
+// exact power of two, which rounds exactly as the division does; only 3, 5, 6
+// and 7 divide (a double division is a long instruction sequence, and deep
+// fluid cells all have 8 neighbours).
+template <class M>
+__device__ __forceinline__ M div_count(M ex, int cont) {
+  if ((cont & (cont - 1)) == 0) return ex * (M)(1.0f / (float)cont);
+  return ex / (M)(float)cont;
+}
+
 // Bit-plane form of the stencil chain.  For each row of the tile and of its
 // 3-row halo, and each 32-cell word of the tile plus one word on either side,
 // a warp ballot turns 32 flag bytes into predicate masks (bit i = cell i of the
@@ -446,7 +456,7 @@ __device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int
   const int cont = __popc(window3<TW>(sm.cnt, r - 1, c, i)) + __popc(window3<TW>(sm.cnt, r, c, i) & 5u) +
                    __popc(window3<TW>(sm.cnt, r + 1, c, i));
   m += cont > 0 ? 0.0f : ex;
-  ex = cont > 0 ? ex / (float)cont : 0.0f;
+  ex = cont > 0 ? div_count(ex, cont) : M(0);
   if (gas_stays) {
     if (!same_bits(m, m_old)) Ms[idx] = m;
     if (!same_bits(ex, ex_old)) Exs[idx] = ex;
@@ -458,21 +468,45 @@ __device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int
   return live;
 }
 
-// Whether super-tile t is visited next step by stream-collide and FS_1 (sc)
-// and by the flag pass (fs); see k_build_lists.  Updates nz_prev[t].
-__device__ __forceinline__ void list_flags(const uint32_t* nz, const ListBuild& lb, uint32_t t, bool& sc, bool& fs) {
-  const uint32_t nsx = lb.nsx, nsy = lb.nsy;
+// Per super-tile activity word written by the flag pass: bit 0 = it holds a
+// fluid or interface cell; bits 1..8 = it holds one within kReach cells of
+// the edge or corner facing the neighbour in direction (dx, dy) (edge_bit).
+// The stencil chain of the flag pass reaches kReach = 3 cells, so a neighbour
+// needs the pass next step only if such a cell faces it.
+constexpr int kReach = 3;
+__host__ __device__ constexpr int edge_bit(int dx, int dy) {
+  return dy == 0 ? (dx > 0 ? 1 : 2) : dx == 0 ? (dy > 0 ? 3 : 4) : dy > 0 ? (dx > 0 ? 5 : 6) : (dx > 0 ? 7 : 8);
+}
+
+// Activity word of a live cell at (lx, ly) in a super-tile of wact x hact cells.
+__device__ __forceinline__ uint32_t activity(int lx, int ly, int wact, int hact) {
+  const bool r = lx >= wact - kReach, l = lx < kReach, u = ly >= hact - kReach, d = ly < kReach;
+  return 1u | ((uint32_t)r << edge_bit(1, 0)) | ((uint32_t)l << edge_bit(-1, 0)) | ((uint32_t)u << edge_bit(0, 1)) |
+         ((uint32_t)d << edge_bit(0, -1)) | ((uint32_t)(u && r) << edge_bit(1, 1)) |
+         ((uint32_t)(u && l) << edge_bit(-1, 1)) | ((uint32_t)(d && r) << edge_bit(1, -1)) |
+         ((uint32_t)(d && l) << edge_bit(-1, -1));
+}
+
+// Whether super-tile t is visited next step by stream-collide and FS_1 (sc:
+// it holds fluid or interface cells) and by the flag pass (fs: it does, or a
+// neighbour holds such a cell within reach of it, or it did a step earlier);
+// updates nz_prev[t].
+__device__ __forceinline__ void list_flags(const uint32_t* nz, uint32_t* nz_prev, uint32_t nsx, uint32_t nsy,
+                                           int prev_unknown, uint32_t t, bool& sc, bool& fs) {
   const uint32_t sx = t % nsx, sy = t / nsx;
-  const uint32_t own = __ldcg(nz + t);
-  uint32_t near = 0;
+  const uint32_t own = __ldcg(nz + t) & 1u;
+  bool near = false;
+#pragma unroll
   for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
     for (int dx = -1; dx <= 1; dx++) {
+      if (!dx && !dy) continue;
       const uint32_t xx = (sx + nsx + dx) % nsx, yy = (sy + nsy + dy) % nsy;
-      near |= __ldcg(nz + xx + yy * nsx);
+      near |= (__ldcg(nz + xx + yy * nsx) >> edge_bit(-dx, -dy)) & 1u;  // its edge facing t
     }
   sc = own != 0;
-  fs = near != 0 || lb.prev_unknown || lb.nz_prev[t] != 0;
-  lb.nz_prev[t] = own;
+  fs = own || near || prev_unknown || nz_prev[t] != 0;
+  nz_prev[t] = own;
 }
 
 // The listed super-tiles: each block runs the tile pass on the tiles of a
@@ -485,6 +519,7 @@ __global__ void __launch_bounds__(TW* kTY, TW == 128 ? FLB_FS_WIDE_MIN_BLOCKS : 
     k_fs234(const __grid_constant__ KParams p, const TileList tl, uint32_t* __restrict__ nz, const ListBuild lb) {
   __shared__ FlagMasks<TW> sm;
   __shared__ uint32_t wsum[2][TW * kTY / 32];
+  __shared__ uint32_t wact_sm[TW * kTY / 32];
   __shared__ int last;
   constexpr int kTX = TW;
   pdl_wait();
@@ -494,15 +529,23 @@ __global__ void __launch_bounds__(TW* kTY, TW == 128 ? FLB_FS_WIDE_MIN_BLOCKS : 
   for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
     const uint32_t t = tile_at(tl, i);
     const int sx = (int)(t % tl.nsx), sy = (int)(t / tl.nsx);
-    bool live = false;
+    const int wact = min((int)kSTW, (int)p.nx - sx * (int)kSTW), hact = min((int)kSTH, (int)p.ny - sy * (int)kSTH);
+    uint32_t act = 0;
 #pragma unroll 1
     for (int j = 0; j < (int)(kSTW / kTX); j++) {
       const int tx = sx * (int)(kSTW / kTX) + j;
-      if (tx * kTX < (int)p.nx) live |= fs234_tile<S, C, M, ODD, TW>(p, tx, sy, tid, sm);
+      if (tx * kTX < (int)p.nx && fs234_tile<S, C, M, ODD, TW>(p, tx, sy, tid, sm))
+        act |= activity(j * kTX + tid % kTX, tid / kTX, wact, hact);
       __syncthreads();
     }
-    live = __syncthreads_or(live);
-    if (tid == 0) nz[t] = live ? 1u : 0u;
+    act = __reduce_or_sync(0xffffffffu, act);
+    if ((tid & 31) == 0) wact_sm[tid >> 5] = act;
+    __syncthreads();
+    if (tid == 0) {
+      uint32_t m = 0;
+      for (int w = 0; w < TW * kTY / 32; w++) m |= wact_sm[w];
+      nz[t] = m;
+    }
   }
   if constexpr (BUILD) {
     __syncthreads();
@@ -519,7 +562,7 @@ __global__ void __launch_bounds__(TW* kTY, TW == 128 ? FLB_FS_WIDE_MIN_BLOCKS : 
     for (uint32_t t0 = 0; t0 < T; t0 += TW * kTY) {
       const uint32_t t = t0 + tid;
       bool sc = false, fs = false;
-      if (t < T) list_flags(nz, lb, t, sc, fs);
+      if (t < T) list_flags(nz, lb.nz_prev, lb.nsx, lb.nsy, lb.prev_unknown, t, sc, fs);
       const uint32_t bsc = __ballot_sync(0xffffffffu, sc), bfs = __ballot_sync(0xffffffffu, fs);
       if (lane == 0) {
         wsum[0][warp] = __popc(bsc);
@@ -552,31 +595,19 @@ __global__ void __launch_bounds__(TW* kTY, TW == 128 ? FLB_FS_WIDE_MIN_BLOCKS : 
 }
 
 // Compacts the super-tiles for the next step: FS_1 and stream-collide visit
-// super-tiles holding fluid or interface cells; the flag pass also visits
-// their neighbours (its stencil chain reaches 3 cells, less than a
-// super-tile) and, once more, super-tiles that held such cells a step earlier
-// (their converted gas cells still clear excess mass and the flag buffers
-// re-synchronise).  Appends with one atomic per warp; list order does not
-// affect results.
+// super-tiles holding fluid or interface cells; the flag pass also visits a
+// neighbour of such a super-tile when one of those cells lies within the
+// chain's reach (3 cells) of their shared edge or corner, and, once more,
+// super-tiles that held such cells a step earlier (their converted gas cells
+// still clear excess mass and the flag buffers re-synchronise).  Appends with
+// one atomic per warp; list order does not affect results.
 __global__ void k_build_lists(const uint32_t* __restrict__ nz, uint32_t* __restrict__ nz_prev, uint32_t nsx,
                               uint32_t nsy, int prev_unknown, uint32_t* __restrict__ list_sc,
                               uint32_t* __restrict__ list_fs, uint32_t* __restrict__ counts) {
   const uint32_t T = nsx * nsy;
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   bool sc = false, fs = false;
-  if (t < T) {
-    const uint32_t sx = t % nsx, sy = t / nsx;
-    const uint32_t own = nz[t];
-    uint32_t near = 0;
-    for (int dy = -1; dy <= 1; dy++)
-      for (int dx = -1; dx <= 1; dx++) {
-        const uint32_t xx = (sx + nsx + dx) % nsx, yy = (sy + nsy + dy) % nsy;
-        near |= nz[xx + yy * nsx];
-      }
-    sc = own != 0;
-    fs = near != 0 || prev_unknown || nz_prev[t] != 0;
-    nz_prev[t] = own;
-  }
+  if (t < T) list_flags(nz, nz_prev, nsx, nsy, prev_unknown, t, sc, fs);
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t bsc = __ballot_sync(0xffffffffu, sc), bfs = __ballot_sync(0xffffffffu, fs);
   uint32_t base_sc = 0, base_fs = 0;
