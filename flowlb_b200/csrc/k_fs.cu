@@ -304,21 +304,29 @@ __device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int
     if (rw >= kRW) break;
     const int r = rw / kW, c = rw % kW;
     const uint8_t f = fv[k];
-    // one ballot per mask, stored as soon as it is formed (keeps registers free)
-#define FLB_MASK(dst, pred)                                  \
-  {                                                          \
-    const uint32_t b_ = __ballot_sync(0xffffffffu, (pred)); \
-    if (lane == 0) sm.dst[r][c] = b_;                        \
-  }
-    FLB_MASK(a, (f & kIF) == kIF)
-    FLB_MASK(gas, (f & kGas) != 0)
-    FLB_MASK(gonly, (f & kIG) == kGas)
-    FLB_MASK(gi, (f & kGasInterface) != 0)
-    FLB_MASK(fl, (f & (kFluid | kInlet)) == kFluid)
-    FLB_MASK(it, (f & kInterface) != 0)
-    FLB_MASK(fb, (f & kFluid) != 0)
-    FLB_MASK(sk, (f & (kWall | kMovingWall | kInlet)) != 0)
-#undef FLB_MASK
+    // ballots of the flag bits; the masks a row needs are formed from them:
+    // the outer halo rows only feed FS_2's IF dilation, the next rows also
+    // FS_2's rewrite, the inner ten rows everything (warp-uniform branches)
+    const uint32_t bF = __ballot_sync(0xffffffffu, (f & kFluid) != 0);
+    const uint32_t bI = __ballot_sync(0xffffffffu, (f & kInterface) != 0);
+    if (lane == 0) sm.a[r][c] = bF & bI;
+    if (r == 0 || r == kR - 1) continue;
+    const uint32_t bG = __ballot_sync(0xffffffffu, (f & kGas) != 0);
+    const uint32_t bGI = __ballot_sync(0xffffffffu, (f & kGasInterface) != 0);
+    if (lane == 0) {
+      sm.gas[r][c] = bG;
+      sm.gonly[r][c] = bG & ~bI;
+      sm.gi[r][c] = bGI;
+      sm.it[r][c] = bI;
+    }
+    if (r == 1 || r == kR - 2) continue;
+    const uint32_t bIn = __ballot_sync(0xffffffffu, (f & kInlet) != 0);
+    const uint32_t bSk = __ballot_sync(0xffffffffu, (f & (kWall | kMovingWall | kInlet)) != 0);
+    if (lane == 0) {
+      sm.fl[r][c] = bF & ~bIn;
+      sm.fb[r][c] = bF;
+      sm.sk[r][c] = bSk;
+    }
   }
   __syncthreads();
   // FS_2 on rows 1 .. kR-2: next to an IF cell, IG -> I and G -> GI
@@ -385,11 +393,11 @@ __device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int
   const bool trust = p.trust_prev != 0;
   if (!trust || old != fin) p.flags_out[idx] = fin;
   const C* U = static_cast<const C*>(p.u);
-  uint32_t nb[9];
-  neighbours((uint32_t)gx, (uint32_t)gy, (uint32_t)nx, (uint32_t)ny, nb);
   // FS_3 fields: a gas->interface cell starts from feq of the neighbour
   // average (calculateAverageValuesNeighbors2D, accumulating in float)
   if ((f1 & (kGasInterface | kIG)) == kGasInterface) {
+    uint32_t nb[9];
+    neighbours((uint32_t)gx, (uint32_t)gy, (uint32_t)nx, (uint32_t)ny, nb);
     float count = 0.0f, lrho = 0.0f, lux = 0.0f, luy = 0.0f;
     const int ddx[9] = {0, 1, -1, 0, 0, 1, -1, 1, -1};
     const int ddy[9] = {0, 0, 0, 1, -1, 1, -1, -1, 1};
