@@ -48,9 +48,11 @@ WORKLOAD = ("free-surface culvert dam break 2048x512, tau 0.55, g_y -5e-5, FP32 
 U_MAX = 0.25  # keeps the surge front stable (plain BGK at tau 0.55 diverges near Mach 0.6)
 KERNEL_OF_PASS = {"stream_collide": "k_sc_list (free-surface stream-collide)", "fs1": "k_fs1 (mass exchange)",
                   "fs234": "k_fs234 (flag stencil, mass/fill update)"}
-# dram__bytes_read.sum + dram__bytes_write.sum per launch from one ncu capture
-# of the workload (profiles/), None where not captured
-TRAFFIC_NCU: dict = {}
+# dram__bytes_read.sum + dram__bytes_write.sum per launch (mean of the two
+# parities) from one ncu capture of the workload at steps 300-303
+# (profiles/dam_break_2048x512_launch_list.md); ncu flushes the caches before
+# each launch, so these are cold-start figures for an L2-resident working set
+TRAFFIC_NCU: dict = {"fs234": 7353088, "stream_collide": 9787008, "fs1": 13900672}
 
 
 def env_rank():
