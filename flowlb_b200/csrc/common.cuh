@@ -60,7 +60,7 @@ struct KParams {
   float fu_g[4], fu_h[4];
   float fu_sw[3];  // FP16S deviation form: f16_scale * w for directions 0, 1..4, 5..8
   int has_io;      // the case has inlet or outlet cells
-  // time step of the FP16S dithered rounding: the step with parity q reads
+  // time step of the FP16S stochastic rounding: the step with parity q reads
   // tstep[q] and writes tstep[q ^ 1] = t + 1 (graph replays see the current t)
   uint32_t* tstep;
   // single phase: chunk map of plain fluid cells, 4 cells per bit (k_plain_chunks); null otherwise

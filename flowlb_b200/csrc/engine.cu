@@ -79,7 +79,7 @@ struct flb_engine {
   double* d_partial = nullptr;
   double* d_scalar = nullptr;
   unsigned long long* d_counts = nullptr;
-  uint32_t* d_tstep = nullptr;  // [2] time step by parity (FP16S dithered rounding)
+  uint32_t* d_tstep = nullptr;  // [2] time step by parity (FP16S stochastic rounding)
   uint32_t* d_plain = nullptr;  // single phase: plain-fluid chunk map (k_plain_chunks)
   GraphSlot g_pair, g_big;
   std::string err;

@@ -303,12 +303,6 @@ __global__ void __launch_bounds__(kVecBlock, FU ? (std::is_same<S, __half>::valu
 #ifndef FLB_H16_MIN_BLOCKS
 #define FLB_H16_MIN_BLOCKS 6
 #endif
-// two floats -> binary16 pair, rounded toward zero (inputs dithered, f16_dither)
-__device__ __forceinline__ uint32_t f2h(float lo, float hi) {
-  uint32_t w;
-  asm("cvt.rz.f16x2.f32 %0, %1, %2;" : "=r"(w) : "f"(hi), "f"(lo));
-  return w;
-}
 __device__ __forceinline__ float2 h2f(uint32_t w) {
   __half2 h;
   memcpy(&h, &w, 4);
@@ -473,23 +467,17 @@ __device__ __forceinline__ void h16_cells(const KParams& p, const uint32_t x0, c
         U[idx + 1 + p.N] = ob.uy;
       }
     }
-    {
-      const uint32_t ba = f16_dither_base(idx, tnow), bb = f16_dither_base(idx + 1u, tnow);
-#pragma unroll
-      for (int i = 0; i < 9; i++) {
-        ha[i] = f16_dithered(ha[i], f16_dither(ba, i));
-        hb[i] = f16_dithered(hb[i], f16_dither(bb, i));
-      }
-    }
+    // stochastic rounding of the pair (idx is even: row and x0 are)
+    const uint32_t base = f16_rs_base(idx, tnow);
     // computed halves where the cell is updated, loaded ones elsewhere
     const uint32_t m = upd[P];
     auto put = [m](uint32_t& w, uint32_t v) { w = (v & m) | (w & ~m); };
-    put(w0.w[P], f2h(ha[0], hb[0]));
+    put(w0.w[P], f2h_rs(ha[0], hb[0], f16_rs_bits(base, 0)));
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const int i = 2 * q + 1;
-      put(nbr[q].w[P], f2h(ha[i], hb[i]));          // post f_i -> neighbour slot b
-      put(own[q].w[P], f2h(ha[i + 1], hb[i + 1]));  // post f_{i+1} -> own slot a
+      put(nbr[q].w[P], f2h_rs(ha[i], hb[i], f16_rs_bits(base, i)));              // post f_i -> neighbour slot b
+      put(own[q].w[P], f2h_rs(ha[i + 1], hb[i + 1], f16_rs_bits(base, i + 1)));  // post f_{i+1} -> own slot a
     }
   }
 

@@ -64,29 +64,47 @@ struct Codec<__half, float> {
 
 // Raw FP16S access: the stored scaled deviation h = (f - w) * scale as a
 // float, for arithmetic done in deviation units (collide_fused_dev).
-// Stores round toward zero: the values arrive dithered (f16_dither), which
-// makes the rounding stochastic.
+// Stores round toward zero: the values arrive already rounded to binary16
+// (f16_rs_one), so the store is exact.
 struct RawHalf {
   __device__ __forceinline__ static float ld(const __half* F, uint32_t a, int, float) { return __half2float(F[a]); }
   __device__ __forceinline__ static void st(__half* F, uint32_t a, int, float v, float) { F[a] = __float2half_rz(v); }
 };
 
-// Dithered rounding of the FP16S deviation units.  Rounding to nearest gives a
-// value that changes slowly from step to step the same rounding error every
+// Stochastic rounding of the FP16S deviation units.  Rounding to nearest gives
+// a value that changes slowly from step to step the same rounding error every
 // step, and in near-steady flow those errors add up: on the 256x64 culvert
 // channel the FP16S velocity drifts 1e-2 (relative L2) from FP64 after 10,000
-// steps.  Instead, 13 pseudo-random bits r (a Weyl sequence in the cell index,
-// the direction and the time step) are added to the float's bits and the sum
-// is truncated to binary16: the value rounds up with probability equal to its
-// distance from the lower neighbour (stochastic rounding), deterministically,
-// and the drift stays at 5e-4.
-__host__ __device__ __forceinline__ uint32_t f16_dither_base(uint32_t idx, uint32_t t) {
-  return idx * 0x85EBCA6Bu + t * 0x9E3779B9u;
+// steps.  Instead every stored value rounds up with probability equal to its
+// distance from the lower binary16 neighbour, deterministically: the pair of
+// cells (2k, 2k+1) draws one 32-bit word per time step (a multiplicative hash
+// of 2k and t, mixed by xor-shift and multiply), population i adds i*K to it,
+// and cvt.rs.f16x2.f32 converts the pair with it: the low 13 bits round the
+// even cell, bits 16..28 the odd one, each added below the last binary16 bit
+// kept (subnormal results included) before truncation.
+__host__ __device__ __forceinline__ uint32_t f16_rs_base(uint32_t idx_even, uint32_t t) {
+  uint32_t x = idx_even * 0x85EBCA6Bu + t * 0x9E3779B9u;
+  x ^= x >> 16;
+  x *= 0x7FEB352Du;
+  x ^= x >> 15;
+  return x;
 }
-__host__ __device__ __forceinline__ uint32_t f16_dither(uint32_t base, int i) {
-  return (base + (uint32_t)i * 0x632BE5ABu) >> 19;
+__host__ __device__ __forceinline__ uint32_t f16_rs_bits(uint32_t base, int i) {
+  return base + (uint32_t)i * 0x632BE5ABu;
 }
-__device__ __forceinline__ float f16_dithered(float v, uint32_t r) { return __uint_as_float(__float_as_uint(v) + r); }
+// lo -> low half (even cell), hi -> high half (odd cell)
+__device__ __forceinline__ uint32_t f2h_rs(float lo, float hi, uint32_t rbits) {
+  uint32_t w;
+  asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(w) : "f"(hi), "f"(lo), "r"(rbits));
+  return w;
+}
+// One value of cell idx rounded as in its pair, returned as the exact float of
+// the binary16 result (a later round-toward-zero store keeps it).
+__device__ __forceinline__ float f16_rs_one(float v, uint32_t idx, uint32_t rbits) {
+  const bool odd = (idx & 1u) != 0;
+  const uint32_t w = odd ? f2h_rs(0.0f, v, rbits) : f2h_rs(v, 0.0f, rbits);
+  return __half2float(__ushort_as_half((unsigned short)(odd ? (w >> 16) : (w & 0xffffu))));
+}
 
 // ---- per-cell arithmetic, cellCalculations.cuh ----------------------------
 

@@ -16,7 +16,7 @@ namespace flb {
 // FU: the fused SRT arithmetic (collide_fused) for cells that are neither inlet
 // nor outlet; the host selects it only for SRT without the subgrid model.
 // DEV: f holds FP16S deviations h = (f - w) * scale (single phase with FU).
-// tnow: the time step (DEV only, for the dithered rounding).
+// tnow: the time step (DEV only, for the stochastic rounding).
 template <class C, class M, bool FS, bool WM, bool FU, bool DEV = false>
 __device__ __forceinline__ void collide_cell(const KParams& p, uint32_t idx, uint32_t x, uint32_t y, uint8_t flag,
                                              uint32_t nbm, C* f, uint32_t tnow = 0u) {
@@ -38,9 +38,9 @@ __device__ __forceinline__ void collide_cell(const KParams& p, uint32_t idx, uin
         static_cast<C*>(p.rho)[idx] = o.rho;
       }
     }
-    const uint32_t base = f16_dither_base(idx, tnow);
+    const uint32_t base = f16_rs_base(idx & ~1u, tnow);
 #pragma unroll
-    for (int i = 0; i < 9; i++) f[i] = f16_dithered(f[i], f16_dither(base, i));
+    for (int i = 0; i < 9; i++) f[i] = f16_rs_one(f[i], idx, f16_rs_bits(base, i));
     return;
   }
   if constexpr (FS) {

@@ -66,12 +66,24 @@ struct orc_state {
 };
 
 /* calculateNeighborsIdxD2Q9, cellCalculations.cuh:82-109 (periodic wrap). */
-/* FP16S dithered rounding of the engine's fused single-phase step (its
- * lattice.cuh f16_dither): 13 bits of a Weyl sequence in cell, direction and
- * time step are added to the float's bits, and the sum is truncated to
- * binary16 (round toward zero), i.e. stochastic rounding made deterministic. */
-static inline uint32_t orc_dither_base(uint32_t idx, uint32_t t) { return idx * 0x85EBCA6Bu + t * 0x9E3779B9u; }
-static inline uint32_t orc_dither(uint32_t base, int i) { return (base + (uint32_t)i * 0x632BE5ABu) >> 19; }
+/* FP16S stochastic rounding of the engine's fused single-phase step (its
+ * lattice.cuh f16_rs_*): the cell pair (2k, 2k+1) draws a 32-bit word per time
+ * step (multiplicative hash of 2k and t, xor-shift / multiply mix), population
+ * i adds i*K; the low 13 bits round the even cell, bits 16..28 the odd one.
+ * orc_f16_rs restates the binary32 -> binary16 conversion with 13 random bits
+ * r (the engine's cvt.rs.f16x2.f32): r is added just below the last binary16
+ * bit kept, then the value is truncated; on the binary16 normal range that is
+ * r added to the binary32 bits, on the subnormal range r is aligned to the
+ * wider discarded field.  Checked against the instruction on the GPU for
+ * normal, subnormal and near-maximum values. */
+static inline uint32_t orc_rs_base(uint32_t idx_even, uint32_t t) {
+  uint32_t x = idx_even * 0x85EBCA6Bu + t * 0x9E3779B9u;
+  x ^= x >> 16;
+  x *= 0x7FEB352Du;
+  x ^= x >> 15;
+  return x;
+}
+static inline uint32_t orc_rs_bits(uint32_t base, int i) { return base + (uint32_t)i * 0x632BE5ABu; }
 
 /* binary32 bits -> binary16 bits, rounding toward zero (overflow gives the
  * largest finite value, as a round-toward-zero conversion does) */
@@ -87,6 +99,19 @@ static inline uint16_t orc_f16_rz(uint32_t x) {
     return (uint16_t)(sg | ((m | 0x800000u) >> (14 - E)));
   }
   return (uint16_t)(sg | ((uint32_t)E << 10) | (m >> 13));
+}
+
+/* binary32 bits x -> binary16 bits, stochastic rounding with the 13 bits r */
+static inline uint16_t orc_f16_rs(uint32_t x, uint32_t r) {
+  const uint16_t sg = (uint16_t)((x >> 16) & 0x8000u);
+  const int e = (int)((x >> 23) & 0xffu);
+  const uint32_t m = x & 0x7fffffu;
+  if (e == 255) return (uint16_t)(sg | (m ? 0x7e00u : 0x7c00u));
+  if (e - 127 >= -14) return (uint16_t)(sg | orc_f16_rz((x & 0x7fffffffu) + r));
+  const uint64_t full = e ? (uint64_t)(m | 0x800000u) : (uint64_t)m;
+  const int shift = -(e ? e - 127 : -126) - 1; /* bits below the binary16 subnormal unit */
+  if (shift >= 64) return sg;
+  return (uint16_t)(sg | (uint16_t)((full + ((uint64_t)r << (shift - 13))) >> shift));
 }
 
 static inline void orc_nbrs(uint32_t idx, uint32_t x, uint32_t y, uint32_t nx, uint32_t ny, uint32_t* nb) {
@@ -489,3 +514,10 @@ int orc_fs4_options(const orc_state* s, size_t idx, double* out3) {
 }
 
 double orc_total_mass(const orc_state* s) { return s ? ORC_VT[s->p.variant].total_mass(s) : 0.0; }
+
+/* The FP16S pair conversion as the engine issues it: binary32 bits a (upper
+ * half) and b (lower half) with the random word r; for checking the
+ * restatement against the instruction's recorded outputs. */
+uint32_t orc_f16_rs_pair(uint32_t a, uint32_t b, uint32_t r) {
+  return ((uint32_t)orc_f16_rs(a, (r >> 16) & 0x1fffu) << 16) | orc_f16_rs(b, r & 0x1fffu);
+}

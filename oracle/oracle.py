@@ -69,6 +69,8 @@ def lib() -> C.CDLL:
         L.orc_read_f64.argtypes = [C.c_void_p, C.c_void_p]
         L.orc_total_mass.restype = C.c_double
         L.orc_total_mass.argtypes = [C.c_void_p]
+        L.orc_f16_rs_pair.restype = C.c_uint32
+        L.orc_f16_rs_pair.argtypes = [C.c_uint32, C.c_uint32, C.c_uint32]
         L.orc_fs1_options.restype = C.c_int
         L.orc_fs1_options.argtypes = [C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p, C.c_void_p]
         L.orc_fs4_options.restype = C.c_int

@@ -209,3 +209,19 @@ def test_oracle_deterministic():
         outs.append((o.f.copy(), o.mass.copy(), o.flags.copy()))
     for a, b in zip(*outs):
         assert exact_equal(a, b)
+
+
+def test_f16_stochastic_rounding_matches_recorded_instruction():
+    """orc_f16_rs (the FP16S stores' rounding) against cvt.rs.f16x2.f32 as
+    recorded on a B200 (tests/golden/f16_rs_probe.npz): binary16 normal,
+    subnormal and near-maximum results."""
+    import os
+
+    import numpy as np
+
+    from oracle import oracle as O
+    d = np.load(os.path.join(os.path.dirname(__file__), "golden", "f16_rs_probe.npz"))
+    L = O.lib()
+    got = np.array([L.orc_f16_rs_pair(int(x), int(y), int(z)) for x, y, z in zip(d["a"], d["b"], d["r"])],
+                   np.uint32)
+    np.testing.assert_array_equal(got, d["out"])
