@@ -2,6 +2,11 @@
 (``src/cuda/runCuda.cu:460-528``) for the synthetic cases.
 
     python -m flowlb_b200.run_case --case dam-break --scale 4 --precision 32 --steps 200
+    python -m flowlb_b200.run_case --files DIR [--out OUT] [--steps N]
+
+``--files DIR`` is FlowLB's own headless run: DIR/Geometry.txt and
+DIR/OptionsCalc.txt set the case up and the VTK results go to
+OUT/results_<k>/ (``flb_run_from_files``; ``--steps`` caps the step count).
 
 Prints one JSON line with the device time (CUDA events on the engine's
 stream), MLUPS, total mass and the cell census.  ``--profile`` reports the
@@ -41,7 +46,18 @@ def main(argv=None):
     ap.add_argument("--profile", action="store_true", help="per-pass CUDA-event times")
     ap.add_argument("--u-max", type=float, default=0.0, help="velocity limiter (0 = off)")
     ap.add_argument("--arithmetic", default="fused", choices=["fused", "reference"])
+    ap.add_argument("--files", default="", help="folder with Geometry.txt and OptionsCalc.txt")
+    ap.add_argument("--out", default="", help="where --files writes results_<k>/ (default: the folder itself)")
     a = ap.parse_args(argv)
+    if a.files:
+        import os
+        geo, opt = os.path.join(a.files, "Geometry.txt"), os.path.join(a.files, "OptionsCalc.txt")
+        import sys
+        given = argv if argv is not None else sys.argv[1:]
+        capped = any(x == "--steps" or x.startswith("--steps=") for x in given)
+        info = E.run_from_files(geo, opt, a.out or a.files, max_steps=a.steps if capped else 0)
+        print(json.dumps(info))
+        return
     case = CASES[a.case](a)
     s = E.Solver(case.flags, free_surface=case.free_surface, precision=a.precision,
                  mass_precision=a.mass_precision, tau=case.tau, fx=case.fx, fy=case.fy, subgrid=a.subgrid,
