@@ -60,6 +60,18 @@ def env_rank():
             int(os.environ.get("WORLD_SIZE", 1)))
 
 
+def max_over_ranks(value: float, dist=None, device: str = "cuda") -> float:
+    """The largest of every rank's value (the job's device time is that of its
+    slowest replica); the value itself on one rank."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -192,11 +204,7 @@ def run_ours(args, rank, local_rank, world):
     launches = solver.launches - launches0
     counts1 = solver.cell_counts()
     mass_drift = (solver.total_mass() - m0) / m0
-    t_max = elapsed_ms
-    if dist is not None:
-        tt = torch.tensor([elapsed_ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
+    t_max = max_over_ranks(elapsed_ms, dist)
     value = world * N * S * args.steps / (t_max * 1e-3) / 1e6
 
     # ---- dominant-kernel roofline: per-pass CUDA-event timing -------------
@@ -236,10 +244,7 @@ def run_ours(args, rank, local_rank, world):
         e2e_step()
     barrier()
     e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        tt = torch.tensor([e2e_s], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+    e2e_s = max_over_ranks(e2e_s, dist)
     e2e_value = world * N * S * args.steps / e2e_s / 1e6
 
     # ---- side measurements on rank 0 (FP16 storage, single-phase probe) ---
