@@ -127,16 +127,15 @@ inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, c
   return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
-// What the list build of a step needs (k_build_lists, or the last block of
-// the flag pass on grids of at most kWideTiles super-tiles).
+// What the list build of a step needs (k_build_lists).
 struct ListBuild {
   uint32_t* nz_prev;
   uint32_t nsx, nsy;
   int prev_unknown;
   uint32_t* list_sc;
   uint32_t* list_fs;
-  uint32_t* counts;  // [2]: lengths of list_sc and list_fs
-  uint32_t* done;    // blocks of the flag pass finished so far (0 between launches)
+  uint32_t* counts;        // [2]: lengths of list_sc and list_fs, zero on entry
+  uint32_t* other_counts;  // [2]: the other parity's lengths, zeroed by the build
 };
 
 __device__ __forceinline__ uint32_t tile_count(const TileList& tl) { return tl.all ? tl.ntiles : *tl.count; }

@@ -57,7 +57,7 @@ struct flb_engine {
   uint32_t* d_nz = nullptr;       // super-tile holds fluid/interface after the last flag pass
   uint32_t* d_nz_prev = nullptr;  // the same one step earlier
   uint32_t* d_list[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [step parity][0 FS_1/SC, 1 flag pass]
-  uint32_t* d_lcount = nullptr;   // [step parity][2] list lengths, then the flag pass's finished-block counter
+  uint32_t* d_lcount = nullptr;   // [step parity][2] list lengths
   bool lists_valid = false;       // lists of the current parity were built by the previous step
   bool thin_tiles = false;        // a last super-tile column or row narrower than the flag pass's reach
   uint32_t grid_sc = 0, grid_fs1 = 0, grid_fs234 = 0;
@@ -225,7 +225,7 @@ ListBuild list_build(flb_engine* h, uint64_t t, const FsLists& L) {
   // a live cell can reach past a super-tile narrower than 3 cells into the
   // one beyond it; such grids visit every super-tile in the flag pass
   return ListBuild{h->d_nz_prev, h->nsx, h->nsy, (L.all || h->thin_tiles) ? 1 : 0, h->d_list[np][0],
-                   h->d_list[np][1], L.next_count, h->d_lcount + 4};
+                   h->d_list[np][1], L.next_count, h->d_lcount + 2 * (1 - np)};
 }
 
 // Issues the passes of one time step at t on the stream.
@@ -241,6 +241,9 @@ uint64_t issue_step(flb_engine* h, uint64_t t, bool write_macro) {
     h->kp.trust_prev = h->trust ? 1 : 0;
     const FsLists L = fs_lists(h, t);
     const ListBuild lb = list_build(h, t, L);
+    // the first step after the state was written from outside: the list
+    // lengths may be stale, and each build appends to zeroed ones
+    if (L.all) cudaMemsetAsync(h->d_lcount, 0, 4 * sizeof(uint32_t), h->stream);
     dispatch(h, [&](auto ops) {
       ops.fs1(h, odd, L.sc);
       ops.sc_list(h, odd, L.sc);
@@ -568,7 +571,7 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
       {(void**)&h->d_list[0][1], tiles * sizeof(uint32_t), h->fs},
       {(void**)&h->d_list[1][0], tiles * sizeof(uint32_t), h->fs},
       {(void**)&h->d_list[1][1], tiles * sizeof(uint32_t), h->fs},
-      {(void**)&h->d_lcount, 5 * sizeof(uint32_t), h->fs},
+      {(void**)&h->d_lcount, 4 * sizeof(uint32_t), h->fs},
   };
   for (Alloc& a : allocs) {
     if (!a.need) continue;
@@ -576,8 +579,8 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
     if (e != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc"));
   }
   if (h->fs) {
-    // list lengths and the flag pass's finished-block counter start at zero
-    cudaError_t e0 = cudaMemsetAsync(h->d_lcount, 0, 5 * sizeof(uint32_t), h->stream);
+    // list lengths start at zero
+    cudaError_t e0 = cudaMemsetAsync(h->d_lcount, 0, 4 * sizeof(uint32_t), h->stream);
     if (e0 != cudaSuccess) return bail(cuda_fail(h, e0, "cudaMemsetAsync"));
     int nsm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
@@ -925,6 +928,7 @@ FLB_API flb_status flb_run_pass(flb_handle h, int pass) {
       ops.fs1(h, odd, all);
     } else {
       // the lists it builds go unused: lists_valid is false
+      cudaMemsetAsync(h->d_lcount, 0, 4 * sizeof(uint32_t), h->stream);
       k = (uint64_t)ops.fs234(h, odd, all, list_build(h, h->t, fs_lists(h, h->t)));
     }
     if (pass == 1 && recon) ops.apply_recon(h, odd);
@@ -957,6 +961,7 @@ FLB_API flb_status flb_profile_steps(flb_handle h, uint64_t n, double pass_ms[3]
       h->kp.trust_prev = h->trust ? 1 : 0;
       const FsLists L = fs_lists(h, h->t);
       const ListBuild lb = list_build(h, h->t, L);
+      if (L.all) cudaMemsetAsync(h->d_lcount, 0, 4 * sizeof(uint32_t), h->stream);
       cudaEventRecord(ev[0], h->stream);
       dispatch(h, [&](auto ops) { ops.fs1(h, odd, L.sc); });
       cudaEventRecord(ev[1], h->stream);
