@@ -138,7 +138,7 @@ struct ListBuild {
   uint32_t* other_counts;  // [2]: the other parity's lengths, zeroed by the build
 };
 
-__device__ __forceinline__ uint32_t tile_count(const TileList& tl) { return tl.all ? tl.ntiles : *tl.count; }
+__device__ __forceinline__ uint32_t tile_count(const TileList& tl) { return tl.all ? tl.ntiles : __ldcg(tl.count); }
 __device__ __forceinline__ uint32_t tile_at(const TileList& tl, uint32_t i) { return tl.all ? i : tl.list[i]; }
 
 template <class S>

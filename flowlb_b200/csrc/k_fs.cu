@@ -525,10 +525,12 @@ __global__ void __launch_bounds__(TW* kTY, TW == 128 ? FLB_FS_WIDE_MIN_BLOCKS : 
   __shared__ FlagMasks<TW> sm;
   __shared__ uint32_t wact_sm[TW * kTY / 32];
   constexpr int kTX = TW;
+  // the list was built by the previous step (FS_1 waited for it), so it is
+  // read before waiting for stream-collide, whose flags the pass needs
+  const uint32_t n = tile_count(tl);
   pdl_wait();
   pdl_trigger();
   const int tid = threadIdx.x;
-  const uint32_t n = tile_count(tl);
   for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
     const uint32_t t = tile_at(tl, i);
     const int sx = (int)(t % tl.nsx), sy = (int)(t / tl.nsx);

@@ -56,9 +56,11 @@ __global__ void __launch_bounds__(kBlock, FLB_SC_MIN_BLOCKS) k_sc_scalar(const _
 template <class S, class C, class M, bool HW, bool ODD, bool FU>
 __global__ void __launch_bounds__(kListBlock, 2048 / kListBlock) k_sc_list(const __grid_constant__ KParams p,
                                                                            const TileList tl) {
+  // the list was built two kernels back (FS_1 waited for it), so it is read
+  // before waiting for FS_1, whose writes the cell updates need
+  const uint32_t n = tile_count(tl);
   pdl_wait();
   pdl_trigger();
-  const uint32_t n = tile_count(tl);
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t row = warp % kSTH, chunk = warp / kSTH, cpr = (blockDim.x >> 5) / kSTH;
   for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
