@@ -52,7 +52,7 @@ KERNEL_OF_PASS = {"stream_collide": "k_sc_list (free-surface stream-collide)", "
 # parities) from one ncu capture of the workload at steps 300-303
 # (profiles/dam_break_2048x512_launch_list.md); ncu flushes the caches before
 # each launch, so these are cold-start figures for an L2-resident working set
-TRAFFIC_NCU: dict = {"fs234": 7353088, "stream_collide": 9787008, "fs1": 13900672}
+TRAFFIC_NCU: dict = {"fs234": 7339520, "stream_collide": 9786880, "fs1": 13902464}
 
 
 def env_rank():

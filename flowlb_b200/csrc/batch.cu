@@ -332,7 +332,7 @@ flb_status btune(flb_batch b, uint32_t probe_steps) {
   };
   std::vector<Cand> cands;
   for (int threads : {512, 1024}) {
-    for (int cs : {2, 4, 8, 16}) {
+    for (int cs : {1, 2, 4, 8, 16}) {
       const int mx = max_clusters(b, cs, threads);
       if (mx <= 0) continue;
       const int per_sm = std::max(1, nsm / cs);
