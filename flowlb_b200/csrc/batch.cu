@@ -11,8 +11,9 @@
 //    global-memory exchange of populations between the cluster's CTAs);
 //  * the warps of a cluster share a case step by 32-cell row segments;
 //  * a case's parameters sit in shared memory for the duration of the case;
-//  * the cells are updated by the same sc_cell as the single-case kernels, so
-//    every case ends bit-identical to flb_step on its own handle.
+//  * the cells are updated with the loads, collision (collide_cell) and
+//    stores of the single-case kernels, so every case ends bit-identical to
+//    flb_step on its own handle.
 // With few clusters only a few cases are active at a time, so their
 // populations stay in the 126 MB L2 while they are stepped.  The cluster size
 // and the number of clusters are chosen by a short timed search at creation
@@ -20,6 +21,7 @@
 #include <cooperative_groups.h>
 
 #include <algorithm>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <numeric>
@@ -42,57 +44,163 @@ constexpr int kBatchMaxThreads = 1024;  // CTA sizes 256, 512 or 1024 (autotuned
 struct BatchCase {
   KParams kp;
   uint32_t nsegx;  // 32-cell row segments
+  // set on the device for the launch shape: a warp's walk over the row
+  // segments advances dy rows and ds segments per item
+  uint32_t dy, ds;
 };
 
-// One step of one case: the warps of the cluster take 32-cell row segments.
+// sc_cell for a batch case (single phase, FP32): the same loads, collision
+// and stores, with slot s addressed as s*N cells past the case's first
+// population instead of through the slot pointer table, which here sits in
+// shared memory and would cost a 64-bit shared load per population.
 template <bool HW, bool FU, bool ODD, bool WM>
-__device__ __noinline__ void batch_step(const KParams& p, uint32_t items, uint32_t nsegx, uint32_t wid, uint32_t nw,
-                                        uint32_t lane) {
-  for (uint32_t it = wid; it < items; it += nw) {
-    const uint32_t y = it / nsegx;
-    const uint32_t x = (it - y * nsegx) * 32u + lane;
-    if (x < p.nx) sc_cell<float, float, double, false, HW, WM, ODD, FU>(p, x, y);
+__device__ __forceinline__ void batch_cell(const KParams& p, uint32_t x, uint32_t y) {
+  const uint32_t nx = p.nx, N = p.N, idx = x + y * nx;
+  float* __restrict__ F = static_cast<float*>(p.f);
+  uint32_t nb[9];
+  neighbours(x, y, nx, p.ny, nb);
+  const uint8_t flag = p.flags[idx];
+  const uint32_t nbm = HW ? (uint32_t)p.nbmask[idx] : 0u;
+  // populations through L2 only: other CTAs wrote them last step, and no
+  // location is read twice in a step
+  float f[9];
+  f[0] = __ldcg(F + idx);
+#pragma unroll
+  for (int i = 1; i < 9; i += 2) {
+    const uint32_t a = (uint32_t)slot_a<ODD>(i) * N, b = (uint32_t)slot_b<ODD>(i) * N;
+    f[i] = __ldcg(F + ((HW && ((nbm >> i) & 1u)) ? b : a) + idx);
+    f[i + 1] = __ldcg(F + ((HW && ((nbm >> (i - 1)) & 1u)) ? a : b) + nb[i]);
+  }
+  if (flag & (kGas | kWall)) return;
+  collide_cell<float, double, false, WM, FU>(p, idx, x, y, flag, nbm, f);
+  // the addresses again, from shared memory and (x, y): cheaper than keeping
+  // them live through the collision under the 32-register budget
+  asm volatile("" ::: "memory");
+  float* G = static_cast<float*>(p.f);
+  const uint32_t M = p.N, nxs = p.nx, ids = x + y * nxs;
+  neighbours(x, y, nxs, p.ny, nb);
+  G[ids] = f[0];
+#pragma unroll
+  for (int i = 1; i < 9; i += 2) {
+    G[(uint32_t)slot_b<ODD>(i) * M + nb[i]] = f[i];
+    G[(uint32_t)slot_a<ODD>(i) * M + ids] = f[i + 1];
   }
 }
 
+// One step of one case: the warps of the cluster take 32-cell row segments,
+// warp k the segments k, k + nw, k + 2 nw, ... (nw warps in the cluster); a
+// warp starts at row y, segment s.  The case (in shared memory) is re-read per
+// item rather than held in registers.
+template <bool HW, bool FU, bool ODD, bool WM>
+__device__ __noinline__ void batch_step(const BatchCase& c, uint32_t y, uint32_t s, uint32_t lane) {
+  while (y < c.kp.ny) {
+    const uint32_t x = s * 32u + lane;
+    if (x < c.kp.nx) batch_cell<HW, FU, ODD, WM>(c.kp, x, y);
+    s += c.ds;
+    y += c.dy;
+    if (s >= c.nsegx) {
+      s -= c.nsegx;
+      y++;
+    }
+  }
+}
+
+// Team barrier (FLB_BATCH_TEAM): the CTAs of a team meet in global memory.
+// count: arrivals in the current round; gen: rounds completed.  One per team,
+// 128 bytes apart.
+struct TeamSync {
+  uint32_t count, gen, pad[30];
+};
+constexpr uint32_t kTeamSpinLimit = 1u << 21;  // polls (about 1 us each) before a wait gives up
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t* a) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(a) : "memory");
+  return v;
+}
+
+// All CTAs of the team have finished the step (and their writes are visible)
+// when this returns true.  Thread 0 arrives for the CTA; the last arrival
+// resets the count and opens the next round.  A wait longer than
+// kTeamSpinLimit polls, or an error raised elsewhere, sets *err and returns
+// false (the caller then leaves the kernel).
+__device__ __forceinline__ bool team_sync(TeamSync* ts, uint32_t n, uint32_t& gen, uint32_t* err, int& ok) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bool good = true;
+    __threadfence();
+    if (atomicAdd(&ts->count, 1u) == n - 1u) {
+      atomicExch(&ts->count, 0u);
+      __threadfence();
+      atomicAdd(&ts->gen, 1u);
+    } else {
+      uint32_t it = 0;
+      while (ld_acquire(&ts->gen) == gen) {
+        if (++it >= kTeamSpinLimit || ld_acquire(err) != 0u) {
+          good = false;
+          atomicOr(err, 1u);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    gen++;
+    ok = good;
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
 // *tdev: time step of the first step (its parity selects the slot pattern);
-// steps >= 1; wm_last: write density and velocity in the last step.
-template <bool HW, bool FU>
-__global__ void __launch_bounds__(kBatchMaxThreads, FLB_BATCH_MIN_BLOCKS) k_batch(const BatchCase* __restrict__ cases,
-                                                         const uint32_t* __restrict__ order,
-                                                         const uint32_t* __restrict__ start,
-                                                         const uint32_t* __restrict__ tdev, uint32_t steps,
-                                                         int wm_last) {
+// steps >= 1; wm_last: write density and velocity in the last step.  A group
+// of `group` consecutive CTAs steps one case at a time: a thread-block cluster
+// (TEAM false; cluster barrier between steps) or a team of co-resident CTAs of
+// a cooperative launch (TEAM true; team_sync between steps).
+template <bool HW, bool FU, bool TEAM>
+__global__ void __launch_bounds__(kBatchMaxThreads, FLB_BATCH_MIN_BLOCKS)
+    k_batch(const BatchCase* __restrict__ cases, const uint32_t* __restrict__ order, const uint32_t* __restrict__ start,
+            const uint32_t* __restrict__ tdev, uint32_t steps, int wm_last, uint32_t group, TeamSync* sync,
+            uint32_t* err) {
   __shared__ BatchCase sc;
+  __shared__ int ok;
   const uint32_t t0 = *tdev;
-  cg::cluster_group cl = cg::this_cluster();
-  const uint32_t cs = cl.num_blocks();
-  const uint32_t cid = blockIdx.x / cs;
-  const uint32_t rank = cl.block_rank();
+  const uint32_t cid = blockIdx.x / group, rank = blockIdx.x % group;
   const uint32_t warps = blockDim.x >> 5;
-  const uint32_t wid = rank * warps + (threadIdx.x >> 5), nw = cs * warps;
+  const uint32_t wid = rank * warps + (threadIdx.x >> 5), nw = group * warps;
   const uint32_t lane = threadIdx.x & 31u;
+  uint32_t gen = 0;
+  // before this CTA's first arrival no round of its team can complete
+  if (TEAM && threadIdx.x == 0) gen = ld_acquire(&sync[cid].gen);
   for (uint32_t k = start[cid]; k < start[cid + 1]; k++) {
     __syncthreads();  // the previous case's parameters are no longer read
     {
       const uint32_t* src = reinterpret_cast<const uint32_t*>(&cases[order[k]]);
       uint32_t* dst = reinterpret_cast<uint32_t*>(&sc);
-      for (uint32_t i = threadIdx.x; i < sizeof(BatchCase) / 4; i += blockDim.x) dst[i] = src[i];
+      for (uint32_t i = threadIdx.x; i < offsetof(BatchCase, dy) / 4; i += blockDim.x) dst[i] = src[i];
+      if (threadIdx.x == 0) {
+        const uint32_t n = cases[order[k]].nsegx;
+        sc.dy = nw / n;
+        sc.ds = nw % n;
+      }
     }
     __syncthreads();
-    const KParams& p = sc.kp;
-    const uint32_t nsegx = sc.nsegx, items = p.ny * nsegx;
+    const uint32_t nsegx = sc.nsegx, y0 = wid / nsegx, s0 = wid % nsegx;
     for (uint32_t s = 0; s < steps; s++) {
       const bool odd = ((t0 + s) & 1u) != 0;
       const bool wm = wm_last && s + 1 == steps;
       if (odd) {
-        if (wm) batch_step<HW, FU, true, true>(p, items, nsegx, wid, nw, lane);
-        else batch_step<HW, FU, true, false>(p, items, nsegx, wid, nw, lane);
+        if (wm) batch_step<HW, FU, true, true>(sc, y0, s0, lane);
+        else batch_step<HW, FU, true, false>(sc, y0, s0, lane);
       } else {
-        if (wm) batch_step<HW, FU, false, true>(p, items, nsegx, wid, nw, lane);
-        else batch_step<HW, FU, false, false>(p, items, nsegx, wid, nw, lane);
+        if (wm) batch_step<HW, FU, false, true>(sc, y0, s0, lane);
+        else batch_step<HW, FU, false, false>(sc, y0, s0, lane);
       }
-      cl.sync();
+      if constexpr (TEAM) {
+        if (!team_sync(&sync[cid], group, gen, err, ok)) return;
+      } else {
+        cg::this_cluster().sync();
+      }
     }
   }
 }
@@ -100,11 +208,16 @@ __global__ void __launch_bounds__(kBatchMaxThreads, FLB_BATCH_MIN_BLOCKS) k_batc
 // advances the device time-step counter after a batch launch
 __global__ void k_tadd(uint32_t* t, uint32_t n) { *t += n; }
 
-using BatchKernel = void (*)(const BatchCase*, const uint32_t*, const uint32_t*, const uint32_t*, uint32_t, int);
+using BatchKernel = void (*)(const BatchCase*, const uint32_t*, const uint32_t*, const uint32_t*, uint32_t, int,
+                             uint32_t, TeamSync*, uint32_t*);
 
-BatchKernel pick_kernel(bool hw, bool fu) {
-  if (hw) return fu ? k_batch<true, true> : k_batch<true, false>;
-  return fu ? k_batch<false, true> : k_batch<false, false>;
+BatchKernel pick_kernel(bool hw, bool fu, bool team) {
+  if (team) {
+    if (hw) return fu ? k_batch<true, true, true> : k_batch<true, false, true>;
+    return fu ? k_batch<false, true, true> : k_batch<false, false, true>;
+  }
+  if (hw) return fu ? k_batch<true, true, false> : k_batch<true, false, false>;
+  return fu ? k_batch<false, true, false> : k_batch<false, false, false>;
 }
 
 }  // namespace
@@ -132,15 +245,20 @@ struct flb_batch_s {
   BatchCase* d_cases = nullptr;
   uint32_t* d_order = nullptr;
   uint32_t* d_start = nullptr;
+  TeamSync* d_sync = nullptr;  // one per team (FLB_BATCH_TEAM)
+  uint32_t* d_err = nullptr;   // set when a team barrier gave up waiting
   std::vector<BatchCase> hcases;
-  // launch configuration
+  // launch configuration: `clusters` groups of `cluster` CTAs of `threads`
+  // threads, each group a thread-block cluster or (team) a team
   int cluster = 8, clusters = 0, threads = 512, tuned = 0;
+  bool team = false;
   uint64_t launches = 0;
   // the step graph (batch kernel + counter update) for one step count
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   uint32_t g_steps = 0;
   int g_wm = -1, g_cluster = 0, g_clusters = 0, g_threads = 0;
+  bool g_team = false;
   std::string err;
 };
 
@@ -183,8 +301,8 @@ void bdrop_graph(flb_batch b) {
 
 void bfree(flb_batch b) {
   bdrop_graph(b);
-  void* bufs[] = {b->d_f, b->d_rho, b->d_u, b->d_flags, b->d_geo, b->d_nbmask, b->d_tstep, b->d_cases, b->d_order,
-                  b->d_start};
+  void* bufs[] = {b->d_f,     b->d_rho,   b->d_u,     b->d_flags, b->d_geo, b->d_nbmask,
+                  b->d_tstep, b->d_cases, b->d_order, b->d_start, b->d_sync, b->d_err};
   for (void* p : bufs)
     if (p) cudaFree(p);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
@@ -200,6 +318,8 @@ flb_status binit(flb_batch b) {
     launch_init_ddf<float, float, double>(b->hcases[c].kp, b->stream, b->d_geo + o, b->hw);
   }
   FLB_BCUDA(b, cudaMemsetAsync(b->d_tstep, 0, 2 * sizeof(uint32_t), b->stream));
+  FLB_BCUDA(b, cudaMemsetAsync(b->d_sync, 0, b->n * sizeof(TeamSync), b->stream));
+  FLB_BCUDA(b, cudaMemsetAsync(b->d_err, 0, sizeof(uint32_t), b->stream));
   FLB_BCUDA(b, cudaGetLastError());
   FLB_BCUDA(b, cudaStreamSynchronize(b->stream));
   b->t = 0;
@@ -225,32 +345,46 @@ flb_status bassign(flb_batch b, int clusters) {
     order.insert(order.end(), l.begin(), l.end());
     start.push_back((uint32_t)order.size());
   }
+  // the new arrays are complete before the old ones go, so a failure leaves
+  // the previous assignment in place
+  uint32_t* d_start = nullptr;
+  FLB_BCUDA(b, cudaMalloc(&d_start, start.size() * sizeof(uint32_t)));
+  cudaError_t e = cudaMemcpy(d_start, start.data(), start.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(d_start);
+    return bcuda(b, e, "cudaMemcpy");
+  }
   bdrop_graph(b);  // the captured launch refers to the old arrays
-  if (b->d_start) cudaFree(b->d_start);
-  b->d_start = nullptr;
-  FLB_BCUDA(b, cudaMalloc(&b->d_start, start.size() * sizeof(uint32_t)));
   FLB_BCUDA(b, cudaMemcpy(b->d_order, order.data(), order.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
-  FLB_BCUDA(b, cudaMemcpy(b->d_start, start.data(), start.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  if (b->d_start) cudaFree(b->d_start);
+  b->d_start = d_start;
   b->clusters = clusters;
   return FLB_OK;
 }
 
 // One launch of the batch kernel for n steps on the stream (captured or not).
 flb_status bissue(flb_batch b, uint32_t n, int wm_last) {
-  BatchKernel kern = pick_kernel(b->hw, b->fu);
+  BatchKernel kern = pick_kernel(b->hw, b->fu, b->team);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(b->clusters * b->cluster));
   cfg.blockDim = dim3((unsigned)b->threads);
   cfg.stream = b->stream;
   cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = (unsigned)b->cluster;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
+  if (b->team) {
+    // every CTA resident at once: the team barriers wait for one another
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+  } else {
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)b->cluster;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+  }
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   FLB_BCUDA(b, cudaLaunchKernelEx(&cfg, kern, (const BatchCase*)b->d_cases, (const uint32_t*)b->d_order,
-                                  (const uint32_t*)b->d_start, (const uint32_t*)b->d_tstep, n, wm_last));
+                                  (const uint32_t*)b->d_start, (const uint32_t*)b->d_tstep, n, wm_last,
+                                  (uint32_t)b->cluster, b->d_sync, b->d_err));
   k_tadd<<<1, 1, 0, b->stream>>>(b->d_tstep, n);
   FLB_BCUDA(b, cudaGetLastError());
   return FLB_OK;
@@ -264,7 +398,7 @@ flb_status blaunch(flb_batch b, uint64_t steps, int wm_last) {
     const uint32_t n = (uint32_t)std::min<uint64_t>(steps - done, 1u << 31);
     const int wm = wm_last && done + n == steps;
     if (!b->gexec || b->g_steps != n || b->g_wm != wm || b->g_cluster != b->cluster ||
-        b->g_clusters != b->clusters || b->g_threads != b->threads) {
+        b->g_clusters != b->clusters || b->g_threads != b->threads || b->g_team != b->team) {
       bdrop_graph(b);
       FLB_BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
       flb_status s = bissue(b, n, wm);
@@ -282,6 +416,7 @@ flb_status blaunch(flb_batch b, uint64_t steps, int wm_last) {
       b->g_cluster = b->cluster;
       b->g_clusters = b->clusters;
       b->g_threads = b->threads;
+      b->g_team = b->team;
     }
     FLB_BCUDA(b, cudaGraphLaunch(b->gexec, b->stream));
     b->launches += 2;
@@ -293,7 +428,7 @@ flb_status blaunch(flb_batch b, uint64_t steps, int wm_last) {
 
 // Resident clusters of the given size (0 when the size cannot launch).
 int max_clusters(flb_batch b, int cs, int threads) {
-  BatchKernel kern = pick_kernel(b->hw, b->fu);
+  BatchKernel kern = pick_kernel(b->hw, b->fu, false);
   if (cs > 8) cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)cs);
@@ -313,12 +448,44 @@ int max_clusters(flb_batch b, int cs, int threads) {
   return n;
 }
 
-// Timed search over cluster sizes and cluster counts: probe steps of the whole
-// batch from the initial state for every candidate; the fastest wins.  The
-// counts include one sized so that the cases active at a time fit in about
-// half of the L2 (each cluster holds one case at a time): over thousands of
-// steps such a case is stepped from L2 after its first step.  The probe is long
-// enough (100 steps by default) for that reuse to show.
+// CTAs of the team kernel resident on the device at once (0 on failure).
+int max_team_ctas(flb_batch b, int threads) {
+  int nsm = 0, per_sm = 0;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick_kernel(b->hw, b->fu, true), threads, 0) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return nsm * per_sm;
+}
+
+// Groups of `group` CTAs that fit on the device at once for the mode.
+int max_groups(flb_batch b, bool team, int group, int threads) {
+  return team ? max_team_ctas(b, threads) / group : max_clusters(b, group, threads);
+}
+
+// Reads and clears the team barriers' error flag: FLB_ERR_CUDA when a wait
+// gave up (the populations of the cases then hold an unfinished step).
+flb_status bcheck(flb_batch b) {
+  uint32_t e = 0;
+  FLB_BCUDA(b, cudaMemcpyAsync(&e, b->d_err, sizeof(e), cudaMemcpyDeviceToHost, b->stream));
+  FLB_BCUDA(b, cudaStreamSynchronize(b->stream));
+  if (!e) return FLB_OK;
+  FLB_BCUDA(b, cudaMemsetAsync(b->d_sync, 0, b->n * sizeof(TeamSync), b->stream));
+  FLB_BCUDA(b, cudaMemsetAsync(b->d_err, 0, sizeof(uint32_t), b->stream));
+  FLB_BCUDA(b, cudaStreamSynchronize(b->stream));
+  return bfail(b, FLB_ERR_CUDA, "a team barrier gave up waiting; the batch state is undefined until reset");
+}
+
+// Timed search over launch shapes: probe steps of the whole batch from the
+// initial state for every candidate; the fastest wins.  Each group of CTAs
+// holds one case at a time, so the number of groups sets how many bytes of
+// cases are active at once: counts sized so that they fit in about half of
+// the L2 let a case be stepped from L2 after its first step (the probe, 100
+// steps by default, is long enough for that reuse to show).  Hardware
+// clusters give the cheapest barrier but pack into the GPCs unevenly at 8 or
+// 16 CTAs; teams take any number of CTAs and fill every SM.
 flb_status btune(flb_batch b, uint32_t probe_steps) {
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
@@ -328,42 +495,63 @@ flb_status btune(flb_batch b, uint32_t probe_steps) {
   const double case_bytes = (double)b->cells / b->n * (9.0 * 4.0 + 2.0);
   const int l2_fit = std::max(1, (int)(0.5 * (double)l2 / std::max(1.0, case_bytes)));
   struct Cand {
+    bool team;
     int cs, clusters, threads;
   };
   std::vector<Cand> cands;
+  auto add = [&](bool team, int cs, int k, int mx, int threads) {
+    const int cl = std::min(std::max(k, 1), std::min(mx, (int)b->n));
+    for (auto& c : cands)
+      if (c.team == team && c.cs == cs && c.clusters == cl && c.threads == threads) return;
+    cands.push_back({team, cs, cl, threads});
+  };
   for (int threads : {512, 1024}) {
-    for (int cs : {1, 2, 4, 8, 16}) {
+    for (int cs : {1, 4, 8, 16}) {
       const int mx = max_clusters(b, cs, threads);
       if (mx <= 0) continue;
       const int per_sm = std::max(1, nsm / cs);
-      for (int k : {l2_fit, per_sm / 2, per_sm, 2 * per_sm, mx}) {
-        const int cl = std::min(std::max(k, 1), std::min(mx, (int)b->n));
-        bool seen = false;
-        for (auto& c : cands) seen |= c.cs == cs && c.clusters == cl && c.threads == threads;
-        if (!seen) cands.push_back({cs, cl, threads});
-      }
+      for (int k : {l2_fit, per_sm, mx}) add(false, cs, k, mx, threads);
+    }
+    // teams: every resident CTA, split into l2_fit/2 .. 2 l2_fit teams (on a
+    // B200 the ensemble runs fastest with its active cases near l2_fit)
+    const int R = max_team_ctas(b, threads);
+    for (int teams : {l2_fit / 2, (3 * l2_fit) / 4, l2_fit, (5 * l2_fit) / 4, (3 * l2_fit) / 2, 2 * l2_fit}) {
+      teams = std::min(std::max(teams, 1), std::min(R, (int)b->n));
+      if (R <= 0 || teams <= 0) continue;
+      add(true, R / teams, teams, teams, threads);
     }
   }
-  if (cands.empty()) return bfail(b, FLB_ERR_UNSUPPORTED, "no thread-block cluster size can launch");
+  if (cands.empty()) return bfail(b, FLB_ERR_UNSUPPORTED, "no launch shape can run the batch");
   cudaEvent_t e0, e1;
   FLB_BCUDA(b, cudaEventCreate(&e0));
   FLB_BCUDA(b, cudaEventCreate(&e1));
   float best = 1e30f;
   Cand win = cands[0];
+  flb_status s = FLB_OK;
   for (const Cand& c : cands) {
+    b->team = c.team;
     b->cluster = c.cs;
     b->threads = c.threads;
-    flb_status s = bassign(b, c.clusters);
+    s = bassign(b, c.clusters);
     if (s == FLB_OK) s = binit(b);
     if (s == FLB_OK) s = blaunch(b, 2, 0);  // warm-up
-    if (s != FLB_OK) break;
-    cudaEventRecord(e0, b->stream);
-    s = blaunch(b, probe_steps, 0);
-    cudaEventRecord(e1, b->stream);
-    if (s != FLB_OK) break;
+    if (s == FLB_OK) {
+      cudaEventRecord(e0, b->stream);
+      s = blaunch(b, probe_steps, 0);
+      cudaEventRecord(e1, b->stream);
+    }
+    if (s != FLB_OK) {
+      // a shape that does not launch is skipped; an error that outlives the
+      // call ends the search
+      cudaGetLastError();
+      if (cudaStreamSynchronize(b->stream) != cudaSuccess) break;
+      s = FLB_OK;
+      continue;
+    }
     cudaEventSynchronize(e1);
     float ms = 0.0f;
     cudaEventElapsedTime(&ms, e0, e1);
+    if (bcheck(b) != FLB_OK) continue;  // a barrier that gave up: not a candidate
     if (ms < best) {
       best = ms;
       win = c;
@@ -371,10 +559,13 @@ flb_status btune(flb_batch b, uint32_t probe_steps) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (s != FLB_OK) return s;
   FLB_BCUDA(b, cudaGetLastError());
+  if (best == 1e30f) return bfail(b, FLB_ERR_CUDA, "no launch shape completed the probe steps");
+  b->team = win.team;
   b->cluster = win.cs;
   b->threads = win.threads;
-  flb_status s = bassign(b, win.clusters);
+  s = bassign(b, win.clusters);
   if (s != FLB_OK) return s;
   b->tuned = 1;
   return binit(b);
@@ -456,6 +647,7 @@ FLB_API flb_status flb_batch_create(const flb_case_desc* cases, uint32_t n, int 
       {(void**)&b->d_geo, M, true},                           {(void**)&b->d_nbmask, M, b->hw},
       {(void**)&b->d_tstep, 2 * sizeof(uint32_t), true},      {(void**)&b->d_cases, n * sizeof(BatchCase), true},
       {(void**)&b->d_order, n * sizeof(uint32_t), true},
+      {(void**)&b->d_sync, n * sizeof(TeamSync), true},       {(void**)&b->d_err, sizeof(uint32_t), true},
   };
   for (A& a : allocs) {
     if (!a.need) continue;
@@ -510,7 +702,7 @@ FLB_API flb_status flb_batch_sync(flb_batch b) {
   if (!b) return FLB_ERR_INVALID_ARGUMENT;
   BDevice g(b->device);
   FLB_BCUDA(b, cudaStreamSynchronize(b->stream));
-  return FLB_OK;
+  return bcheck(b);
 }
 
 FLB_API flb_status flb_batch_reset(flb_batch b) {
@@ -537,7 +729,7 @@ FLB_API flb_status flb_batch_read_field(flb_batch b, uint32_t i, int field, void
   return FLB_OK;
 }
 
-FLB_API flb_status flb_batch_info(flb_batch b, int64_t info[7]) {
+FLB_API flb_status flb_batch_info(flb_batch b, int64_t info[8]) {
   if (!b || !info) return FLB_ERR_INVALID_ARGUMENT;
   info[0] = b->n;
   info[1] = (int64_t)b->cells;
@@ -546,7 +738,40 @@ FLB_API flb_status flb_batch_info(flb_batch b, int64_t info[7]) {
   info[4] = b->clusters;
   info[5] = b->tuned;
   info[6] = b->threads;
+  info[7] = b->team ? FLB_BATCH_TEAM : FLB_BATCH_CLUSTER;
   return FLB_OK;
+}
+
+FLB_API flb_status flb_batch_set_launch(flb_batch b, int mode, int group, int groups, int threads) {
+  if (!b) return FLB_ERR_INVALID_ARGUMENT;
+  if (mode != FLB_BATCH_CLUSTER && mode != FLB_BATCH_TEAM)
+    return bfail(b, FLB_ERR_INVALID_ARGUMENT, "mode must be FLB_BATCH_CLUSTER or FLB_BATCH_TEAM");
+  const bool team = mode == FLB_BATCH_TEAM;
+  if (!team && group != 1 && group != 2 && group != 4 && group != 8 && group != 16)
+    return bfail(b, FLB_ERR_INVALID_ARGUMENT, "a cluster has 1, 2, 4, 8 or 16 CTAs");
+  if (team && group < 1) return bfail(b, FLB_ERR_INVALID_ARGUMENT, "a team has at least one CTA");
+  if (threads != 256 && threads != 512 && threads != 1024)
+    return bfail(b, FLB_ERR_INVALID_ARGUMENT, "threads per CTA must be 256, 512 or 1024");
+  if (groups < 1 || (uint32_t)groups > b->n)
+    return bfail(b, FLB_ERR_INVALID_ARGUMENT, "groups must be between 1 and the number of cases");
+  BDevice g(b->device);
+  FLB_BCUDA(b, cudaStreamSynchronize(b->stream));  // a running launch reads the assignment
+  const int mx = max_groups(b, team, group, threads);
+  if (groups > mx)
+    return bfail(b, FLB_ERR_UNSUPPORTED,
+                 "at most " + std::to_string(mx) + " groups of this shape fit on the device at once");
+  const int pc = b->cluster, pt = b->threads;
+  const bool pm = b->team;
+  b->team = team;
+  b->cluster = group;
+  b->threads = threads;
+  flb_status s = bassign(b, groups);
+  if (s != FLB_OK) {
+    b->team = pm;
+    b->cluster = pc;
+    b->threads = pt;
+  }
+  return s;
 }
 
 FLB_API flb_status flb_batch_destroy(flb_batch b) {

@@ -31,7 +31,7 @@ EXPORTS = [
     "flb_total_mass_noalloc", "flb_cell_counts", "flb_check_finite", "flb_run_pass", "flb_profile_steps", "flb_launch_count", "flb_save_checkpoint",
     "flb_load_checkpoint", "flb_last_error", "flb_status_string", "flb_version",
     "flb_batch_create", "flb_batch_step", "flb_batch_sync", "flb_batch_reset", "flb_batch_read_field",
-    "flb_batch_info", "flb_batch_destroy", "flb_batch_last_error",
+    "flb_batch_info", "flb_batch_set_launch", "flb_batch_destroy", "flb_batch_last_error",
     "flb_adjoint_desc_init", "flb_adjoint_create", "flb_adjoint_set_porosity", "flb_adjoint_set_force",
     "flb_adjoint_forward", "flb_adjoint_backward", "flb_adjoint_timing", "flb_adjoint_destroy",
     "flb_adjoint_last_error",
@@ -75,6 +75,7 @@ class SetupStruct(C.Structure):
 
 VTI_UINT8, VTI_FLOAT32, VTI_FLOAT64 = 0, 1, 2
 VIZ_UX, VIZ_UY, VIZ_MAGNITUDE, VIZ_PRESSURE = 0, 1, 2, 3
+BATCH_CLUSTER, BATCH_TEAM = 0, 1
 
 
 class VtiField(C.Structure):
@@ -138,6 +139,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "flb_batch_reset": (C.c_int, [H]),
         "flb_batch_read_field": (C.c_int, [H, C.c_uint32, C.c_int, C.c_void_p, C.c_int]),
         "flb_batch_info": (C.c_int, [H, C.POINTER(C.c_int64)]),
+        "flb_batch_set_launch": (C.c_int, [H, C.c_int, C.c_int, C.c_int, C.c_int]),
         "flb_batch_destroy": (C.c_int, [H]),
         "flb_batch_last_error": (C.c_char_p, [H]),
         "flb_adjoint_desc_init": (None, [C.POINTER(AdjointDesc)]),
@@ -515,9 +517,17 @@ class Batch:
         self._check(load_library().flb_batch_reset(self._h))
 
     def info(self) -> dict:
-        a = (C.c_int64 * 7)()
+        a = (C.c_int64 * 8)()
         self._check(load_library().flb_batch_info(self._h, a))
-        return dict(cases=a[0], cells=a[1], t=a[2], cluster=a[3], clusters=a[4], tuned=bool(a[5]), threads=a[6])
+        return dict(cases=a[0], cells=a[1], t=a[2], group=a[3], groups=a[4], tuned=bool(a[5]), threads=a[6],
+                    mode="team" if a[7] == BATCH_TEAM else "cluster")
+
+    def set_launch(self, mode: str, group: int, groups: int, threads: int):
+        """Launch shape for the following steps: ``mode`` "cluster" or "team",
+        CTAs per group, groups, threads per CTA (``info()`` of a tuned batch,
+        for instance); the state is kept."""
+        m = {"cluster": BATCH_CLUSTER, "team": BATCH_TEAM}[mode]
+        self._check(load_library().flb_batch_set_launch(self._h, m, int(group), int(groups), int(threads)))
 
     def read(self, i: int, field: int) -> np.ndarray:
         ny, nx = self.shapes[i]

@@ -212,10 +212,17 @@ FLB_API flb_status flb_load_checkpoint(flb_handle h, const char* path);
  * all; no inlet/outlet cells) advanced together: flb_batch_step(b, k) is one
  * graph launch of one persistent kernel that runs all k steps of every case.
  * Each case ends bit-identical to k flb_step calls on its own handle.
+ * A group of CTAs steps one case at a time; the steps of a case are separated
+ * by a barrier among the group: a thread-block cluster of 1, 2, 4, 8 or 16
+ * CTAs (FLB_BATCH_CLUSTER) or a team of any number of CTAs meeting in global
+ * memory, every CTA of the launch resident at once (FLB_BATCH_TEAM, a
+ * cooperative launch; a team barrier gives up after about two seconds, and
+ * flb_batch_sync then returns FLB_ERR_CUDA).
  * autotune: 0 uses 8-CTA clusters, one CTA per SM; 1 (100 probe steps) or a
- * probe step count > 1 times the candidate cluster sizes and counts on the
- * batch itself and keeps the fastest, then rebuilds the initial state.  The device, and the
- * stream if given, come from cases[0]. */
+ * probe step count > 1 times candidate modes, group sizes and counts on the
+ * batch itself and keeps the fastest, then rebuilds the initial state.  The
+ * device, and the stream if given, come from cases[0]. */
+enum { FLB_BATCH_CLUSTER = 0, FLB_BATCH_TEAM = 1 };
 typedef struct flb_batch_s* flb_batch;
 FLB_API flb_status flb_batch_create(const flb_case_desc* cases, uint32_t n, int autotune, flb_batch* out);
 FLB_API flb_status flb_batch_step(flb_batch b, uint64_t n);
@@ -224,8 +231,17 @@ FLB_API flb_status flb_batch_sync(flb_batch b);
 FLB_API flb_status flb_batch_reset(flb_batch b);
 /* FLB_FIELD_F, _RHO, _U or _FLAGS of case i (float, as a precision-32 handle) */
 FLB_API flb_status flb_batch_read_field(flb_batch b, uint32_t i, int field, void* dst, int on_device);
-/* info[0..6] = cases, cells, t, cluster size, clusters, autotuned, threads per CTA */
-FLB_API flb_status flb_batch_info(flb_batch b, int64_t info[7]);
+/* info[0..7] = cases, cells, t, CTAs per group, groups, autotuned, threads
+ * per CTA, mode (FLB_BATCH_CLUSTER or FLB_BATCH_TEAM) */
+FLB_API flb_status flb_batch_info(flb_batch b, int64_t info[8]);
+/* Sets the launch shape (info[7], [3], [4], [6] of an earlier tuned batch,
+ * for instance): mode; CTAs per group (1, 2, 4, 8 or 16 for a cluster, >= 1
+ * for a team); 1 <= groups <= the groups of that shape that fit on the device
+ * at once, and <= the number of cases; 256, 512 or 1024 threads per CTA.
+ * The state and t are kept (results do not depend on the shape).
+ * FLB_ERR_INVALID_ARGUMENT for a shape out of range, FLB_ERR_UNSUPPORTED for
+ * one that cannot launch. */
+FLB_API flb_status flb_batch_set_launch(flb_batch b, int mode, int group, int groups, int threads);
 FLB_API flb_status flb_batch_destroy(flb_batch b);
 FLB_API const char* flb_batch_last_error(flb_batch b);
 

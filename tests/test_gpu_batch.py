@@ -60,3 +60,39 @@ def test_batch_rejects_unsupported_cases():
     ens = _small_ensemble(2, 1)
     with pytest.raises(E.FlowLBError):
         E.Batch(ens, bounce_back=E.BB_HALFWAY, arithmetic=7)
+
+
+def test_batch_launch_shape_changes_keep_the_state():
+    """flb_batch_set_launch between launches, clusters and teams: the cases
+    still end equal to their own handles, whatever shape ran each part."""
+    ens = _small_ensemble(11, 7)
+    b = E.Batch(ens, autotune=0)
+    steps = 0
+    shapes = ((("cluster", 1, 5, 256), 3), (("team", 3, 4, 512), 6), (("cluster", 16, 1, 1024), 8),
+              (("team", 1, 11, 256), 1), (("team", 7, 2, 1024), 5), (("cluster", 4, 3, 1024), 1))
+    for shape, n in shapes:
+        b.set_launch(*shape)
+        info = b.info()
+        assert (info["mode"], info["group"], info["groups"], info["threads"]) == shape
+        b.step(n)
+        steps += n
+    b.sync()
+    assert b.info()["t"] == steps
+    for i, (flags, tau, gx, gy) in enumerate(ens):
+        s = E.Solver(flags, precision=32, tau=tau, fx=gx, fy=gy)
+        s.step(steps)
+        for fid, ref in ((E.FIELD_F, s.f), (E.FIELD_U, s.u)):
+            got = b.read(i, fid)
+            assert exact_equal(got, ref), f"case {i}: {first_mismatch(got, ref)}"
+        s.close()
+    for bad in (("cluster", 3, 1, 512), ("cluster", 8, 1, 384), ("cluster", 8, 0, 512), ("cluster", 8, 12, 512),
+                ("team", 0, 2, 512)):
+        with pytest.raises(E.FlowLBError) as ei:
+            b.set_launch(*bad)
+        assert ei.value.status == 1  # FLB_ERR_INVALID_ARGUMENT
+    with pytest.raises(E.FlowLBError) as ei:  # more CTAs than fit on the device at once
+        b.set_launch("team", 100000, 1, 1024)
+    assert ei.value.status == 4  # FLB_ERR_UNSUPPORTED
+    info = b.info()
+    assert (info["mode"], info["group"], info["groups"], info["threads"]) == ("cluster", 4, 3, 1024)
+    b.close()
