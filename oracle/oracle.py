@@ -7,7 +7,7 @@ as the checker, and by the CPU-baseline leg of ``bench.py``.  The engine in
 * ``Oracle``: the C restatement of the reference step (``liboracle.so``).
 * ``ref_host_init``: the reference's own host initialisation
   (``_ref/libflbref_host.so``, built from FlowLB ``src/initData.cpp``).
-* ``ref_cuda_run``: the reference's own CUDA kernels
+* ``ref_cuda_run`` / ``ref_cuda_time``: the reference's own CUDA kernels
   (``_ref/libflbref_cuda.so``, built from FlowLB ``src/cuda/*.cu`` with
   ``--fmad=false``); needs a GPU.
 """
@@ -249,6 +249,31 @@ def ref_cuda_run(state: dict, nx: int, ny: int, precision: int, free_surface: bo
     if rc != 0:
         raise RuntimeError(f"ref_cuda_run failed: {rc}")
     return s
+
+
+def ref_cuda_time(state: dict, nx: int, ny: int, precision: int, free_surface: bool, tau: float, fx: float,
+                  fy: float, warm: int, nsteps: int, t0: int = 0) -> tuple:
+    """Device time of the reference's own CUDA step sequence (16x16 blocks, one
+    launch per kernel and step, as its headless loop issues them): ``warm``
+    untimed steps from ``state`` at ``t0``, then ``nsteps`` timed with CUDA
+    events.  Returns (milliseconds, final state)."""
+    L = C.CDLL(os.path.join(REF_DIR, "libflbref_cuda.so"))
+    L.ref_cuda_time.argtypes = [C.c_int] * 7 + [C.c_double] * 3 + [C.c_uint64] * 3 + [C.c_void_p] * 8
+    dt = np.float32 if precision == 32 else np.float64
+    s = {k: np.ascontiguousarray(np.array(v, copy=True), dtype=(np.uint8 if k == "flags" else dt))
+         for k, v in state.items()}
+    N = nx * ny
+    for k in ("mass", "excess", "phi"):
+        if k not in s:
+            s[k] = np.zeros(N, dt)
+    ms = C.c_double()
+    rc = L.ref_cuda_time(precision, nx, ny, int(free_surface), 0, 0, 1, float(tau), float(fx), float(fy), int(t0),
+                         int(warm), int(nsteps), s["f"].ctypes.data, s["rho"].ctypes.data, s["u"].ctypes.data,
+                         s["flags"].ctypes.data, s["mass"].ctypes.data, s["excess"].ctypes.data,
+                         s["phi"].ctypes.data, C.byref(ms))
+    if rc != 0:
+        raise RuntimeError(f"ref_cuda_time failed: {rc}")
+    return float(ms.value), s
 
 
 def adjoint_run(flags: np.ndarray, porosity: np.ndarray, tau: float, gx: float, gy: float, steps: int,

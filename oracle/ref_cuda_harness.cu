@@ -25,7 +25,7 @@ namespace {
 template <typename P>
 int run_ref(int nx, int ny, int free_surface, int collision, int subgrid, int use_force, double tau, double fx,
             double fy, uint64_t t0, uint64_t nsteps, int kernel_id, void* f, void* rho, void* u, uint8_t* flags,
-            void* mass, void* excess, void* phi) {
+            void* mass, void* excess, void* phi, uint64_t warm = 0, double* ms = nullptr) {
   const unsigned int Nx = (unsigned)nx, Ny = (unsigned)ny, N = Nx * Ny;
   static float wf[9] = {4.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f,
                         1.0f / 36.0f, 1.0f / 36.0f, 1.0f / 36.0f, 1.0f / 36.0f};
@@ -61,7 +61,16 @@ int run_ref(int nx, int ny, int free_surface, int collision, int subgrid, int us
       default: break;
     }
   } else {
-    for (uint64_t k = 0; k < nsteps; k++) {
+    // timing (ms != nullptr): `warm` untimed steps, then CUDA events around
+    // the nsteps steps that follow
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    const uint64_t total = ms ? warm + nsteps : nsteps;
+    for (uint64_t k = 0; k < total; k++) {
+      if (ms && k == warm) {
+        cudaEventCreate(&e0);
+        cudaEventCreate(&e1);
+        cudaEventRecord(e0);
+      }
       const unsigned long t = (unsigned long)(t0 + k);
       if (free_surface) {
         FLB::d_FreeSurface2D_1<P, 9><<<grid, block>>>(d_f, d_rho, d_u, d_flags, d_mass, d_excess, d_phi, t);
@@ -72,6 +81,15 @@ int run_ref(int nx, int ny, int free_surface, int collision, int subgrid, int us
       } else {
         FLB::d_StreamCollide2D<P, 9><<<grid, block>>>(d_f, d_rho, d_u, d_flags, d_mass, t);
       }
+    }
+    if (ms && e0) {
+      cudaEventRecord(e1);
+      cudaEventSynchronize(e1);
+      float m = 0.0f;
+      cudaEventElapsedTime(&m, e0, e1);
+      *ms = m;
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
     }
   }
   cudaError_t err = cudaDeviceSynchronize();
@@ -116,5 +134,24 @@ extern "C" int ref_cuda_run(int precision, int nx, int ny, int free_surface, int
   if (precision == 64)
     return run_ref<double>(nx, ny, free_surface, collision, subgrid, use_force, tau, fx, fy, t0, nsteps, kernel_id,
                            f, rho, u, flags, mass, excess, phi);
+  return -1;
+}
+
+// Device time of the reference's headless step sequence: from the state in the
+// buffers, `warm` steps from t0, then nsteps more timed with CUDA events
+// (default stream, one launch per kernel and step as runCuda.cu issues them);
+// *ms receives the timed milliseconds and the buffers the final state.
+extern "C" int ref_cuda_time(int precision, int nx, int ny, int free_surface, int collision, int subgrid,
+                             int use_force, double tau, double fx, double fy, uint64_t t0, uint64_t warm,
+                             uint64_t nsteps, void* f, void* rho, void* u, uint8_t* flags, void* mass,
+                             void* excess, void* phi, double* ms) {
+  if (nx < 3 || ny < 3 || !ms || nsteps == 0) return -1;
+  *ms = 0.0;
+  if (precision == 32)
+    return run_ref<float>(nx, ny, free_surface, collision, subgrid, use_force, tau, fx, fy, t0, nsteps, -1, f, rho,
+                          u, flags, mass, excess, phi, warm, ms);
+  if (precision == 64)
+    return run_ref<double>(nx, ny, free_surface, collision, subgrid, use_force, tau, fx, fy, t0, nsteps, -1, f,
+                           rho, u, flags, mass, excess, phi, warm, ms);
   return -1;
 }

@@ -74,3 +74,89 @@ def test_free_surface_kernels_match_reference_along_a_trajectory(prec, mode):
             o.kernel(kid)
         o.t = o.t + 1
     print("cells decided by a race in the reference:", raced)
+
+
+def _engine_ms(solver, n):
+    import torch
+
+    st = torch.cuda.ExternalStream(solver.stream)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    solver.step(n)
+    b.record(st)
+    b.synchronize()
+    return a.elapsed_time(b)
+
+
+def _record(line):
+    """Prints a timing line; appends it as JSON to $FLB_TIMING_OUT when set."""
+    import json
+    import os
+
+    print(json.dumps(line))
+    path = os.environ.get("FLB_TIMING_OUT")
+    if path:
+        with open(path, "a") as fp:
+            fp.write(json.dumps(line) + "\n")
+
+
+def test_engine_outpaces_reference_kernels_single_phase_8192x2048():
+    """The engine in the reference's own modes (implicit walls, reference
+    arithmetic) against FlowLB's CUDA kernels on the same GPU, 8192x2048 plain
+    channel, FP32: equal populations after the same 220 steps, and a faster
+    step (device time of the last 200 steps of each)."""
+    import flowlb_b200.engine as E
+
+    c = cases.hbm_probe(8192, 2048)
+    o = O.Oracle(c.flags, O.OracleConfig(variant=O.F32_M32, tau=c.tau, fx=c.fx))
+    ref_ms, ref = O.ref_cuda_time(snapshot(o, False), c.nx, c.ny, 32, False, c.tau, c.fx, 0.0, warm=20, nsteps=200)
+    o.close()
+    s = E.Solver(c.flags, precision=32, mass_precision=32, tau=c.tau, fx=c.fx, bounce_back=E.BB_IMPLICIT,
+                 arithmetic=E.ARITH_REFERENCE, device=0)
+    s.step(20)
+    s.sync()
+    eng_ms = _engine_ms(s, 200)
+    assert exact_equal(s.f, ref["f"]), first_mismatch(s.f, ref["f"])
+    s.close()
+    # the engine's own defaults (half-way walls, fused arithmetic)
+    d = E.Solver(c.flags, precision=32, tau=c.tau, fx=c.fx, device=0)
+    d.step(20)
+    d.sync()
+    def_ms = _engine_ms(d, 200)
+    d.close()
+    mlups = lambda ms: c.cells * 200 / (ms * 1e-3) / 1e6  # noqa: E731
+    _record({"case": "single phase 8192x2048 FP32, 200 steps", "reference_kernels_mlups": round(mlups(ref_ms), 1),
+             "engine_reference_modes_mlups": round(mlups(eng_ms), 1), "engine_defaults_mlups": round(mlups(def_ms), 1),
+             "speedup_reference_modes": round(ref_ms / eng_ms, 2), "speedup_defaults": round(ref_ms / def_ms, 2)})
+    assert eng_ms < ref_ms
+
+
+def test_engine_outpaces_reference_kernels_dam_break_2048x512():
+    """The free-surface step in the reference's modes against FlowLB's five
+    CUDA kernels per step on the same GPU, 2048x512 dam break, FP32 (mass in
+    FP32 as in the reference): device time of 200 steps after 20."""
+    import flowlb_b200.engine as E
+
+    c = cases.dam_break(1)
+    o = O.Oracle(c.flags, O.OracleConfig(variant=O.F32_M32, free_surface=True, tau=c.tau, fy=c.fy))
+    ref_ms, _ = O.ref_cuda_time(snapshot(o, True), c.nx, c.ny, 32, True, c.tau, 0.0, c.fy, warm=20, nsteps=200)
+    o.close()
+    s = E.Solver(c.flags, free_surface=True, precision=32, mass_precision=32, tau=c.tau, fy=c.fy,
+                 bounce_back=E.BB_IMPLICIT, fs_mode=E.FS_REFERENCE, arithmetic=E.ARITH_REFERENCE, device=0)
+    s.step(20)
+    s.sync()
+    eng_ms = _engine_ms(s, 200)
+    s.close()
+    d = E.Solver(c.flags, free_surface=True, precision=32, mass_precision=64, tau=c.tau, fy=c.fy, u_max=0.25,
+                 device=0)
+    d.step(20)
+    d.sync()
+    def_ms = _engine_ms(d, 200)
+    d.close()
+    mlups = lambda ms: c.cells * 200 / (ms * 1e-3) / 1e6  # noqa: E731
+    _record({"case": "free-surface dam break 2048x512 FP32, 200 steps",
+             "reference_kernels_mlups": round(mlups(ref_ms), 1),
+             "engine_reference_modes_mlups": round(mlups(eng_ms), 1),
+             "engine_defaults_fp64_mass_mlups": round(mlups(def_ms), 1),
+             "speedup_reference_modes": round(ref_ms / eng_ms, 2), "speedup_defaults": round(ref_ms / def_ms, 2)})
+    assert eng_ms < ref_ms
