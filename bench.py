@@ -82,18 +82,47 @@ def measured_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """SM clocks and clock-event reasons sampled during the timed region.
+
+    NVML (read-only queries) polled every 2 ms from a thread when it can be
+    opened for the device, so even a timed region of a few hundred
+    milliseconds gets many samples; otherwise nvidia-smi every 200 ms."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits (nvml.h: nvmlClocksEventReason*)
+    NVML_REASONS = {"sw_power_cap": 0x4, "hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20,
+                    "hw_thermal_slowdown": 0x40}
 
-    def __init__(self, device: int):
+    def __init__(self, device: int, uuid: str | None = None):
         self.device = device
+        self.uuid = uuid
         self.lines: list[str] = []
+        self.samples: list[tuple] = []
         self.proc = None
+        self.nvml = None
+        self.stop = threading.Event()
+
+    def _open_nvml(self):
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = (pynvml.nvmlDeviceGetHandleByUUID(self.uuid) if self.uuid
+                 else pynvml.nvmlDeviceGetHandleByIndex(self.device))
+            pynvml.nvmlDeviceGetClockInfo(h, pynvml.NVML_CLOCK_SM)
+            return pynvml, h
+        except Exception:
+            return None
 
     def __enter__(self):
+        opened = self._open_nvml()
+        if opened is not None:
+            self.nvml = opened
+            self.thread = threading.Thread(target=self._poll, daemon=True)
+            self.thread.start()
+            return self
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
@@ -104,11 +133,30 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def _poll(self):
+        nv, h = self.nvml
+        while not self.stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.samples.append((float(sm), float(smax), int(bits)))
+            except Exception:
+                break
+            self.stop.wait(0.002)
+
     def _read(self):
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
     def __exit__(self, *exc):
+        self.stop.set()
+        if self.nvml is not None:
+            self.thread.join(timeout=5)
+            try:
+                self.nvml[0].nvmlShutdown()
+            except Exception:
+                pass
         if self.proc:
             self.proc.terminate()
             try:
@@ -118,23 +166,31 @@ class ClockSampler:
 
     def summary(self):
         sm, smax, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
-            parts = [p.strip() for p in line.split(",")]
-            if len(parts) < 9:
-                continue
-            try:
-                sm.append(float(parts[1]))
-                smax.append(float(parts[2]))
-            except ValueError:
-                continue
-            for name, val in zip(names, parts[5:9]):
-                if val.lower().startswith("active"):
-                    reasons.add(name)
+        if self.nvml is not None:
+            for a, b, bits in self.samples:
+                sm.append(a)
+                smax.append(b)
+                reasons.update(name for name, bit in self.NVML_REASONS.items() if bits & bit)
+            source = "nvml, 2 ms"
+        else:
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            for line in self.lines:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for name, val in zip(names, parts[5:9]):
+                    if val.lower().startswith("active"):
+                        reasons.add(name)
+            source = "nvidia-smi, 200 ms"
         if not sm:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "source": source}
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "sm_mhz_min": min(sm), "source": source}
 
 
 def algorithmic_bytes(counts: dict) -> dict:
@@ -153,6 +209,14 @@ def algorithmic_bytes(counts: dict) -> dict:
     active = counts["fluid"] + counts["interface"]
     return {"stream_collide": active * 86.0 + counts["interface"] * 9.0, "fs1": active * 93.0,
             "fs234": active * 39.0}
+
+
+def _gpu_uuid(torch, device: int):
+    """NVML's name ("GPU-<uuid>") of the CUDA device, or None."""
+    try:
+        return "GPU-" + str(torch.cuda.get_device_properties(device).uuid)
+    except Exception:
+        return None
 
 
 def run_ours(args, rank, local_rank, world):
@@ -191,7 +255,7 @@ def run_ours(args, rank, local_rank, world):
     launches0 = solver.launches
     barrier()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    with ClockSampler(local_rank) as clocks:
+    with ClockSampler(local_rank, _gpu_uuid(torch, local_rank)) as clocks:
         for a, b in ev:
             flush.zero_()
             torch.cuda.current_stream().synchronize()
