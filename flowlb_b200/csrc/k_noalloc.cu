@@ -1,10 +1,10 @@
 // k_noalloc.cu -- free-surface total mass for callers that cannot allocate.
 //
 // Some callers may not allocate device memory at the moment they need the
-// mass check: a host application stepping the solver from inside a CUDA
-// graph it is capturing (cudaMalloc is not allowed during capture), a
-// real-time loop whose device memory budget is fixed up front and audited, or
-// a plug-in that only ever receives pointers to buffers owned by someone else.
+// mass check: a real-time loop whose device memory budget is fixed up front
+// and audited, a loop that cannot afford the implicit device synchronisation
+// of cudaMalloc/cudaFree between steps, or a plug-in that only ever receives
+// pointers to buffers owned by someone else.
 // flb_total_mass needs a handle, whose creation allocates; this entry point
 // takes plain device pointers instead and keeps its scratch (one FP64 partial
 // sum per block of 256 cells) in a file-scope __device__ array of fixed size,

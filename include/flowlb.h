@@ -166,8 +166,9 @@ FLB_API flb_status flb_total_mass(flb_handle h, double* mass);
 
 /* Allocation-free free-surface total mass; no counterpart in the reference.
  * For callers that may not allocate device memory when they need the check
- * (inside their own stream capture, under a fixed audited memory budget, or
- * holding only pointers to someone else's buffers): it takes the device
+ * (under a fixed audited memory budget, in a loop that cannot take the
+ * implicit synchronisation of cudaMalloc/cudaFree, or holding only pointers
+ * to someone else's buffers): it takes the device
  * fields directly (mass and excess in FP64, flags as the solver keeps them,
  * nx*ny cells each), launches on `stream` and writes the same FP64 sum as
  * flb_total_mass to the device pointer `out` without waiting.  Its scratch is
