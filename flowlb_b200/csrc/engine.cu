@@ -12,6 +12,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -573,9 +574,16 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
       {(void**)&h->d_list[1][1], tiles * sizeof(uint32_t), h->fs},
       {(void**)&h->d_lcount, 4 * sizeof(uint32_t), h->fs},
   };
+  // Failure injection on the host: with FLB_FAIL_ALLOC_AT=k in the
+  // environment the k-th device allocation of this creation fails as
+  // cudaMalloc does when memory runs out (nothing is allocated for it), so the
+  // clean-up path can be exercised without exhausting a GPU.
+  long fail_at = 0;
+  if (const char* v = std::getenv("FLB_FAIL_ALLOC_AT")) fail_at = std::strtol(v, nullptr, 10);
+  long nalloc = 0;
   for (Alloc& a : allocs) {
     if (!a.need) continue;
-    cudaError_t e = cudaMalloc(a.p, a.bytes);
+    cudaError_t e = ++nalloc == fail_at ? cudaErrorMemoryAllocation : cudaMalloc(a.p, a.bytes);
     if (e != cudaSuccess) return bail(cuda_fail(h, e, "cudaMalloc"));
   }
   if (h->fs) {
