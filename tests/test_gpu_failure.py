@@ -5,6 +5,7 @@ into a case through flb_write_field, and an allocation failure is injected by
 the engine's host-side hook (FLB_FAIL_ALLOC_AT=k fails the k-th device
 allocation of a creation without attempting it).  The library must report
 each through its status codes, free what it allocated, and stay usable."""
+import gc
 import os
 
 import numpy as np
@@ -70,7 +71,22 @@ def test_injected_allocation_failure_frees_everything(require_gpu, fs, monkeypat
 
     c = cases.small_dam_break(512, 256) if fs else cases.plain_channel(512, 256)
     kw = dict(free_surface=fs, precision=32, tau=c.tau, fx=c.fx, fy=c.fy, device=0)
-    E.Solver(c.flags, **kw).close()  # the context and the module are loaded once, outside the count
+    # the context and every kernel this case launches (loaded lazily on first
+    # use) are loaded once, outside the measurement
+    w = E.Solver(c.flags, **kw)
+    w.step(8)
+    w.close()
+    # handles left by earlier tests in reference cycles are freed now, not
+    # by a collection in the middle of the measurement
+    gc.collect()
+    gc.disable()
+    try:
+        _allocation_failures(torch, c, kw, monkeypatch)
+    finally:
+        gc.enable()
+
+
+def _allocation_failures(torch, c, kw, monkeypatch):
     before = _free_bytes(torch)
     failures = 0
     for k in range(1, 40):
