@@ -225,3 +225,52 @@ def test_f16_stochastic_rounding_matches_recorded_instruction():
     got = np.array([L.orc_f16_rs_pair(int(x), int(y), int(z)) for x, y, z in zip(d["a"], d["b"], d["r"])],
                    np.uint32)
     np.testing.assert_array_equal(got, d["out"])
+
+
+def _random_free_surface_box(seed):
+    """A walled box with 1-3 solid blocks on the floor, a water column on one
+    side and a free drop of water above the floor, all seeded."""
+    rng = np.random.default_rng(seed)
+    nx, ny = int(rng.integers(40, 81)), int(rng.integers(32, 65))
+    g = np.full((ny, nx), cases.GAS, np.uint8)
+    for _ in range(int(rng.integers(1, 4))):
+        w, h = int(rng.integers(2, nx // 4)), int(rng.integers(2, ny // 3))
+        x0 = int(rng.integers(1, nx - w - 1))
+        g[1:1 + h, x0:x0 + w] = cases.WALL
+    cw, ch = int(rng.integers(4, nx // 2)), int(rng.integers(6, ny - 8))
+    col = g[1:1 + ch, 1:1 + cw]
+    col[col == cases.GAS] = cases.FLUID
+    r = int(rng.integers(2, 6))
+    cx, cy = int(rng.integers(cw + r + 3, nx - r - 2)), int(rng.integers(ny // 2, ny - r - 3))
+    yy, xx = np.mgrid[0:ny, 0:nx]
+    drop = ((xx - cx) ** 2 + (yy - cy) ** 2 <= r * r) & (g == cases.GAS)
+    g[drop] = cases.FLUID
+    g[0, :] = g[-1, :] = g[:, 0] = g[:, -1] = cases.WALL
+    tau = float(rng.uniform(0.52, 0.8))
+    return g, tau
+
+
+@pytest.mark.parametrize("seed", range(6))
+def test_oracle_free_surface_invariants_on_random_boxes(seed):
+    """Conservative free surface, FP64, half-way walls, gravity: on seeded
+    random geometries the total mass (fill plus pending excess) stays constant
+    to round-off, every non-solid cell is exactly one of fluid, interface or
+    gas, and no fluid cell touches a gas cell (the interface layer closes)."""
+    g, tau = _random_free_surface_box(seed)
+    o = O.Oracle(g, O.OracleConfig(variant=O.F64, free_surface=True, tau=tau, fy=-1e-4, bb=O.BB_HALFWAY,
+                                   fs_mode=O.FS_CONSERVATIVE, u_max=0.25))
+    m0 = o.total_mass()
+    ny, nx = g.shape
+    for _ in range(5):
+        o.step(40)
+        assert abs(o.total_mass() - m0) / m0 < 1e-12
+        fl = o.flags.reshape(ny, nx)
+        assert set(np.unique(fl)).issubset({cases.FLUID, cases.GAS, cases.INTERFACE, cases.WALL})
+        fluid = fl == cases.FLUID
+        gas = fl == cases.GAS
+        near_gas = np.zeros_like(gas)
+        for dy in (-1, 0, 1):
+            for dx in (-1, 0, 1):
+                near_gas |= np.roll(np.roll(gas, dy, 0), dx, 1)
+        assert not np.any(fluid & near_gas), np.argwhere(fluid & near_gas)[:5]
+    assert np.all(np.isfinite(o.rho))
