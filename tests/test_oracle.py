@@ -251,19 +251,27 @@ def _random_free_surface_box(seed):
 
 
 @pytest.mark.parametrize("seed", range(6))
-def test_oracle_free_surface_invariants_on_random_boxes(seed):
-    """Conservative free surface, FP64, half-way walls, gravity: on seeded
-    random geometries the total mass (fill plus pending excess) stays constant
-    to round-off, every non-solid cell is exactly one of fluid, interface or
-    gas, and no fluid cell touches a gas cell (the interface layer closes)."""
+@pytest.mark.parametrize("mode", [(O.FS_CONSERVATIVE, O.BB_HALFWAY), (O.FS_REFERENCE, O.BB_IMPLICIT),
+                                  (O.FS_REFERENCE, O.BB_HALFWAY)],
+                         ids=["conservative-halfway", "reference-implicit", "reference-halfway"])
+def test_oracle_free_surface_invariants_on_random_boxes(seed, mode):
+    """FP64 free surface with gravity on seeded random geometries: every
+    non-solid cell is exactly one of fluid, interface or gas, and no fluid cell
+    touches a gas cell (the interface layer closes), in the reference's rules
+    and in the conservative ones; with the conservative rules and half-way
+    walls the total mass (fill plus pending excess) also stays constant to
+    round-off (the reference's rules lose mass: about 5e-5 of it over these
+    200 steps with its implicit walls)."""
+    fs_mode, bb = mode
     g, tau = _random_free_surface_box(seed)
-    o = O.Oracle(g, O.OracleConfig(variant=O.F64, free_surface=True, tau=tau, fy=-1e-4, bb=O.BB_HALFWAY,
-                                   fs_mode=O.FS_CONSERVATIVE, u_max=0.25))
+    o = O.Oracle(g, O.OracleConfig(variant=O.F64, free_surface=True, tau=tau, fy=-1e-4, bb=bb, fs_mode=fs_mode,
+                                   u_max=0.25))
     m0 = o.total_mass()
     ny, nx = g.shape
     for _ in range(5):
         o.step(40)
-        assert abs(o.total_mass() - m0) / m0 < 1e-12
+        if fs_mode == O.FS_CONSERVATIVE:
+            assert abs(o.total_mass() - m0) / m0 < 1e-12
         fl = o.flags.reshape(ny, nx)
         assert set(np.unique(fl)).issubset({cases.FLUID, cases.GAS, cases.INTERFACE, cases.WALL})
         fluid = fl == cases.FLUID
