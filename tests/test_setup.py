@@ -454,3 +454,38 @@ def test_series_file(tmp_path):
     L = E.load_library()
     assert L.flb_write_vti_series(str(tmp_path).encode(), 3, 0.1) == 0
     assert (tmp_path / "loaderFiles.vti.series").read_bytes() == SO.series_text(3, 0.1)
+
+
+def _reformat(text, rng):
+    """The same file with whitespace inserted at random places (inside
+    keywords and numbers too), '#' comments after some lines, comment-only
+    lines between them and Windows line ends on some: every one of these is
+    removed by FlowLB's line rules before a line is read."""
+    out = []
+    for line in text.splitlines():
+        chars = list(line)
+        for _ in range(int(rng.integers(0, 4))):
+            chars.insert(int(rng.integers(0, len(chars) + 1)), str(rng.choice([" ", "  ", "\t"])))
+        line = "".join(chars)
+        if rng.random() < 0.3:
+            line += " # note = (1, 2, 3)"
+        if rng.random() < 0.2:
+            out.append("# a comment line")
+        out.append(line + ("\r" if rng.random() < 0.3 else ""))
+    return "\n".join(out) + "\n"
+
+
+@pytest.mark.parametrize("seed", range(8))
+def test_reader_ignores_formatting(tmp_path, seed):
+    """Seeded reformatting of valid input files (whitespace, comments, line
+    ends) gives the same lattice, flags, constants and loop bounds."""
+    base = _setup(tmp_path, GEO_OK, OPT_OK)
+    rng = np.random.default_rng(1000 + seed)
+    d = tmp_path / "fmt"
+    d.mkdir()
+    s = _setup(d, _reformat(GEO_OK, rng), _reformat(OPT_OK, rng))
+    assert (s.nx, s.ny) == (base.nx, base.ny)
+    assert (s.flags == base.flags).all() and (s.initial_flags == base.initial_flags).all()
+    for f in ("tau", "fx", "fy", "inlet_ux", "inlet_uy", "free_surface", "precision"):
+        assert getattr(s.desc, f) == getattr(base.desc, f), f
+    assert (s.time_steps, s.save_every, s.cuda_block) == (base.time_steps, base.save_every, base.cuda_block)
