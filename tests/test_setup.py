@@ -489,3 +489,23 @@ def test_reader_ignores_formatting(tmp_path, seed):
     for f in ("tau", "fx", "fy", "inlet_ux", "inlet_uy", "free_surface", "precision"):
         assert getattr(s.desc, f) == getattr(base.desc, f), f
     assert (s.time_steps, s.save_every, s.cuda_block) == (base.time_steps, base.save_every, base.cuda_block)
+
+
+def test_reader_comment_rule_removes_spaces_only(tmp_path):
+    """FlowLB skips a line when, after removing spaces (' ' only), it is
+    empty or starts with '#' (reader.cpp:720-723).  A comment indented by a
+    tab, or a blank line that holds only a carriage return, therefore reaches
+    the option parser as an empty option: the options reader rejects it as an
+    unknown option (reader.cpp:543-547), the geometry reader ignores it.  The
+    engine keeps both behaviours."""
+    for extra in ("\t# indented by a tab", "\r"):
+        opt = OPT_OK.replace("GRAPHICS_API = NONE", "GRAPHICS_API = NONE\n" + extra)
+        with pytest.raises(E.FlowLBError) as ei:
+            _setup(tmp_path, GEO_OK, opt)
+        assert ei.value.status == 1
+        assert "The option in the calculation's file in the line 5 doesn't exist" in str(ei.value)
+        geo = GEO_OK.replace("SIZE = 0.05", "SIZE = 0.05\n" + extra)
+        s = _setup(tmp_path, geo, OPT_OK)
+        assert (s.nx, s.ny) == (21, 11)
+    # indented by spaces, the same comment is skipped
+    _setup(tmp_path, GEO_OK, OPT_OK.replace("GRAPHICS_API = NONE", "GRAPHICS_API = NONE\n    # spaces"))
