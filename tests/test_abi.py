@@ -119,3 +119,28 @@ def test_null_handle_calls_fail_cleanly():
     assert L.flb_get_time(None, t) == 1
     assert L.flb_destroy(None) == 1
     assert L.flb_last_error(None) == b"null handle"
+
+
+@pytest.mark.parametrize("lang", ["c99", "c++17"])
+def test_header_builds_pedantic_and_links(lang):
+    """A host written in C or C++ (FlowLB itself is C++17) includes the header
+    with -Wall -Wextra -pedantic -Werror, links against libflowlb.so and calls
+    the device-free entry points."""
+    src = ('#include <string.h>\n#include "flowlb.h"\n'
+           "int main(void) {\n"
+           "  flb_case_desc d;\n"
+           "  flb_case_desc_init(&d);\n"
+           "  if (d.nx != 0 || d.flags) return 1;\n"
+           "  if (strcmp(flb_status_string(FLB_ERR_NONFINITE), \"non-finite populations\") != 0) return 2;\n"
+           "  if (!flb_version() || !flb_version()[0]) return 3;\n"
+           "  if (flb_create(0, 0) != FLB_ERR_INVALID_ARGUMENT) return 4;\n"
+           "  return 0;\n}\n")
+    libdir = os.path.join(ROOT, "flowlb_b200")
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "host.c" if lang == "c99" else "host.cpp")
+        exe = os.path.join(d, "host")
+        open(path, "w").write(src)
+        cc = ["gcc", "-std=c99"] if lang == "c99" else ["g++", "-std=c++17"]
+        subprocess.run(cc + ["-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(ROOT, "include"), path,
+                             "-L", libdir, "-lflowlb", f"-Wl,-rpath,{libdir}", "-o", exe], check=True)
+        assert subprocess.run([exe]).returncode == 0
