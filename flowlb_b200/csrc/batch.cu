@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <cstddef>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -111,7 +112,10 @@ __device__ __noinline__ void batch_step(const BatchCase& c, uint32_t y, uint32_t
 struct TeamSync {
   uint32_t count, gen, pad[30];
 };
-constexpr uint32_t kTeamSpinLimit = 1u << 21;  // polls (about 1 us each) before a wait gives up
+// polls (about 1 us each) before a wait gives up, unless flb_batch_set_wait_limit set another
+constexpr uint32_t kTeamSpinLimit = 1u << 21;
+// no CTA skips its arrival (see k_batch's skip_rank)
+constexpr uint32_t kNoSkip = 0xffffffffu;
 
 __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* a) {
   uint32_t v;
@@ -121,22 +125,25 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* a) {
 
 // All CTAs of the team have finished the step (and their writes are visible)
 // when this returns true.  Thread 0 arrives for the CTA; the last arrival
-// resets the count and opens the next round.  A wait longer than
-// kTeamSpinLimit polls, or an error raised elsewhere, sets *err and returns
-// false (the caller then leaves the kernel).
-__device__ __forceinline__ bool team_sync(TeamSync* ts, uint32_t n, uint32_t& gen, uint32_t* err, int& ok) {
+// resets the count and opens the next round.  A wait longer than `limit`
+// polls, or an error raised elsewhere, sets *err and returns false (the
+// caller then leaves the kernel).  arrive = false (failure injection only)
+// makes this CTA wait without arriving, so the round never completes and
+// every wait of the team runs out.
+__device__ __forceinline__ bool team_sync(TeamSync* ts, uint32_t n, uint32_t& gen, uint32_t* err, int& ok,
+                                          uint32_t limit, bool arrive) {
   __syncthreads();
   if (threadIdx.x == 0) {
     bool good = true;
     __threadfence();
-    if (atomicAdd(&ts->count, 1u) == n - 1u) {
+    if (arrive && atomicAdd(&ts->count, 1u) == n - 1u) {
       atomicExch(&ts->count, 0u);
       __threadfence();
       atomicAdd(&ts->gen, 1u);
     } else {
       uint32_t it = 0;
       while (ld_acquire(&ts->gen) == gen) {
-        if (++it >= kTeamSpinLimit || ld_acquire(err) != 0u) {
+        if (++it >= limit || ld_acquire(err) != 0u) {
           good = false;
           atomicOr(err, 1u);
           break;
@@ -156,12 +163,15 @@ __device__ __forceinline__ bool team_sync(TeamSync* ts, uint32_t n, uint32_t& ge
 // steps >= 1; wm_last: write density and velocity in the last step.  A group
 // of `group` consecutive CTAs steps one case at a time: a thread-block cluster
 // (TEAM false; cluster barrier between steps) or a team of co-resident CTAs of
-// a cooperative launch (TEAM true; team_sync between steps).
+// a cooperative launch (TEAM true; team_sync between steps, each wait bounded
+// by wait_limit polls).  skip_rank: in team mode, the CTA of each team with
+// this rank never arrives at its team's barriers (failure injection; kNoSkip
+// in normal operation); unused in cluster mode.
 template <bool HW, bool FU, bool TEAM>
 __global__ void __launch_bounds__(kBatchMaxThreads, FLB_BATCH_MIN_BLOCKS)
     k_batch(const BatchCase* __restrict__ cases, const uint32_t* __restrict__ order, const uint32_t* __restrict__ start,
             const uint32_t* __restrict__ tdev, uint32_t steps, int wm_last, uint32_t group, TeamSync* sync,
-            uint32_t* err) {
+            uint32_t* err, uint32_t wait_limit, uint32_t skip_rank) {
   __shared__ BatchCase sc;
   __shared__ int ok;
   const uint32_t t0 = *tdev;
@@ -197,7 +207,7 @@ __global__ void __launch_bounds__(kBatchMaxThreads, FLB_BATCH_MIN_BLOCKS)
         else batch_step<HW, FU, false, false>(sc, y0, s0, lane);
       }
       if constexpr (TEAM) {
-        if (!team_sync(&sync[cid], group, gen, err, ok)) return;
+        if (!team_sync(&sync[cid], group, gen, err, ok, wait_limit, rank != skip_rank)) return;
       } else {
         cg::this_cluster().sync();
       }
@@ -209,7 +219,7 @@ __global__ void __launch_bounds__(kBatchMaxThreads, FLB_BATCH_MIN_BLOCKS)
 __global__ void k_tadd(uint32_t* t, uint32_t n) { *t += n; }
 
 using BatchKernel = void (*)(const BatchCase*, const uint32_t*, const uint32_t*, const uint32_t*, uint32_t, int,
-                             uint32_t, TeamSync*, uint32_t*);
+                             uint32_t, TeamSync*, uint32_t*, uint32_t, uint32_t);
 
 BatchKernel pick_kernel(bool hw, bool fu, bool team) {
   if (team) {
@@ -247,6 +257,10 @@ struct flb_batch_s {
   uint32_t* d_start = nullptr;
   TeamSync* d_sync = nullptr;  // one per team (FLB_BATCH_TEAM)
   uint32_t* d_err = nullptr;   // set when a team barrier gave up waiting
+  uint32_t wait_limit = kTeamSpinLimit;  // polls before a team barrier wait gives up
+  // a team barrier gave up: populations and t no longer describe a finished
+  // step, so stepping is refused until flb_batch_reset
+  bool broken = false;
   std::vector<BatchCase> hcases;
   // launch configuration: `clusters` groups of `cluster` CTAs of `threads`
   // threads, each group a thread-block cluster or (team) a team
@@ -256,7 +270,7 @@ struct flb_batch_s {
   // the step graph (batch kernel + counter update) for one step count
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
-  uint32_t g_steps = 0;
+  uint32_t g_steps = 0, g_limit = 0, g_skip = 0;
   int g_wm = -1, g_cluster = 0, g_clusters = 0, g_threads = 0;
   bool g_team = false;
   std::string err;
@@ -323,6 +337,7 @@ flb_status binit(flb_batch b) {
   FLB_BCUDA(b, cudaGetLastError());
   FLB_BCUDA(b, cudaStreamSynchronize(b->stream));
   b->t = 0;
+  b->broken = false;
   return FLB_OK;
 }
 
@@ -362,8 +377,19 @@ flb_status bassign(flb_batch b, int clusters) {
   return FLB_OK;
 }
 
+// Failure injection for tests, read at every launch: with
+// FLB_BATCH_SKIP_ARRIVAL=1 in the environment the last CTA of every team never
+// arrives at its team's barriers, so each wait runs out after the wait limit
+// and the launch reports FLB_ERR_CUDA (team mode only; a hardware cluster
+// barrier has no bounded wait and is never skipped).
+uint32_t skip_rank_for(flb_batch b) {
+  const char* v = std::getenv("FLB_BATCH_SKIP_ARRIVAL");
+  if (!b->team || !v || std::strcmp(v, "1") != 0) return kNoSkip;
+  return (uint32_t)b->cluster - 1u;
+}
+
 // One launch of the batch kernel for n steps on the stream (captured or not).
-flb_status bissue(flb_batch b, uint32_t n, int wm_last) {
+flb_status bissue(flb_batch b, uint32_t n, int wm_last, uint32_t skip) {
   BatchKernel kern = pick_kernel(b->hw, b->fu, b->team);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(b->clusters * b->cluster));
@@ -384,7 +410,7 @@ flb_status bissue(flb_batch b, uint32_t n, int wm_last) {
   cfg.numAttrs = 1;
   FLB_BCUDA(b, cudaLaunchKernelEx(&cfg, kern, (const BatchCase*)b->d_cases, (const uint32_t*)b->d_order,
                                   (const uint32_t*)b->d_start, (const uint32_t*)b->d_tstep, n, wm_last,
-                                  (uint32_t)b->cluster, b->d_sync, b->d_err));
+                                  (uint32_t)b->cluster, b->d_sync, b->d_err, b->wait_limit, skip));
   k_tadd<<<1, 1, 0, b->stream>>>(b->d_tstep, n);
   FLB_BCUDA(b, cudaGetLastError());
   return FLB_OK;
@@ -394,14 +420,16 @@ flb_status bissue(flb_batch b, uint32_t n, int wm_last) {
 // same step count and configuration).
 flb_status blaunch(flb_batch b, uint64_t steps, int wm_last) {
   uint64_t done = 0;
+  const uint32_t skip = skip_rank_for(b);
   while (done < steps) {  // at most 2^31 steps per launch
     const uint32_t n = (uint32_t)std::min<uint64_t>(steps - done, 1u << 31);
     const int wm = wm_last && done + n == steps;
     if (!b->gexec || b->g_steps != n || b->g_wm != wm || b->g_cluster != b->cluster ||
-        b->g_clusters != b->clusters || b->g_threads != b->threads || b->g_team != b->team) {
+        b->g_clusters != b->clusters || b->g_threads != b->threads || b->g_team != b->team ||
+        b->g_limit != b->wait_limit || b->g_skip != skip) {
       bdrop_graph(b);
       FLB_BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-      flb_status s = bissue(b, n, wm);
+      flb_status s = bissue(b, n, wm, skip);
       cudaGraph_t g = nullptr;
       cudaError_t e = cudaStreamEndCapture(b->stream, &g);
       if (s != FLB_OK) {
@@ -417,6 +445,8 @@ flb_status blaunch(flb_batch b, uint64_t steps, int wm_last) {
       b->g_clusters = b->clusters;
       b->g_threads = b->threads;
       b->g_team = b->team;
+      b->g_limit = b->wait_limit;
+      b->g_skip = skip;
     }
     FLB_BCUDA(b, cudaGraphLaunch(b->gexec, b->stream));
     b->launches += 2;
@@ -466,12 +496,15 @@ int max_groups(flb_batch b, bool team, int group, int threads) {
 }
 
 // Reads and clears the team barriers' error flag: FLB_ERR_CUDA when a wait
-// gave up (the populations of the cases then hold an unfinished step).
+// gave up.  The populations of the cases then hold an unfinished step and t
+// (advanced when the launch was issued) no longer matches them, so the batch
+// refuses to step until flb_batch_reset.
 flb_status bcheck(flb_batch b) {
   uint32_t e = 0;
   FLB_BCUDA(b, cudaMemcpyAsync(&e, b->d_err, sizeof(e), cudaMemcpyDeviceToHost, b->stream));
   FLB_BCUDA(b, cudaStreamSynchronize(b->stream));
   if (!e) return FLB_OK;
+  b->broken = true;
   FLB_BCUDA(b, cudaMemsetAsync(b->d_sync, 0, b->n * sizeof(TeamSync), b->stream));
   FLB_BCUDA(b, cudaMemsetAsync(b->d_err, 0, sizeof(uint32_t), b->stream));
   FLB_BCUDA(b, cudaStreamSynchronize(b->stream));
@@ -693,6 +726,8 @@ FLB_API flb_status flb_batch_create(const flb_case_desc* cases, uint32_t n, int 
 
 FLB_API flb_status flb_batch_step(flb_batch b, uint64_t n) {
   if (!b) return FLB_ERR_INVALID_ARGUMENT;
+  if (b->broken)
+    return bfail(b, FLB_ERR_CUDA, "a team barrier gave up waiting in an earlier launch; call flb_batch_reset");
   if (n == 0) return FLB_OK;
   BDevice g(b->device);
   return blaunch(b, n, 1);
@@ -772,6 +807,12 @@ FLB_API flb_status flb_batch_set_launch(flb_batch b, int mode, int group, int gr
     b->threads = pt;
   }
   return s;
+}
+
+FLB_API flb_status flb_batch_set_wait_limit(flb_batch b, uint32_t polls) {
+  if (!b) return FLB_ERR_INVALID_ARGUMENT;
+  b->wait_limit = polls == 0 ? kTeamSpinLimit : polls;
+  return FLB_OK;
 }
 
 FLB_API flb_status flb_batch_destroy(flb_batch b) {

@@ -14,7 +14,6 @@
 // k_sum_partials (k_reduce.cu), so the result equals flb_total_mass bit for
 // bit on the same fields.
 #include <cstdio>
-#include <mutex>
 
 #include "../../include/flowlb.h"
 #include "common.cuh"
@@ -30,27 +29,18 @@ constexpr uint32_t kNoAllocMaxBlocks = FLB_NOALLOC_MAX_CELLS / kBlock;
 // different host threads) race on it.
 static __device__ __align__(256) double g_partial[kNoAllocMaxBlocks];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-double* g_addr[kMaxDevices] = {};
-
-// Device address of g_partial on the current device.  In host code the name
-// g_partial is only a host-side stand-in for the symbol, not a device address;
-// passing it to a kernel would fault (or, where the GPU can reach host memory,
-// silently use the wrong memory).  Looked up once per device.
+// Device address of g_partial in the current device's context.  In host code
+// the name g_partial is only a host-side stand-in for the symbol, not a device
+// address; passing it to a kernel would fault (or, where the GPU can reach
+// host memory, silently use the wrong memory).  Looked up on every call: the
+// lookup is a host-side query (no stream work), and an address kept from an
+// earlier call would be stale after the context was reset (cudaDeviceReset
+// reloads the module and its __device__ arrays).
 cudaError_t scratch_address(double** out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_partial);
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-  std::lock_guard<std::mutex> lock(g_mu);
-  if (!g_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_partial);
-    if (e != cudaSuccess) return e;
-    g_addr[dev] = static_cast<double*>(p);
-  }
-  *out = g_addr[dev];
+  *out = static_cast<double*>(p);
   return cudaSuccess;
 }
 

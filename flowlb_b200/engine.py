@@ -31,7 +31,8 @@ EXPORTS = [
     "flb_total_mass_noalloc", "flb_cell_counts", "flb_check_finite", "flb_run_pass", "flb_profile_steps", "flb_launch_count", "flb_save_checkpoint",
     "flb_load_checkpoint", "flb_last_error", "flb_status_string", "flb_version",
     "flb_batch_create", "flb_batch_step", "flb_batch_sync", "flb_batch_reset", "flb_batch_read_field",
-    "flb_batch_info", "flb_batch_set_launch", "flb_batch_destroy", "flb_batch_last_error",
+    "flb_batch_info", "flb_batch_set_launch", "flb_batch_set_wait_limit", "flb_batch_destroy",
+    "flb_batch_last_error",
     "flb_adjoint_desc_init", "flb_adjoint_create", "flb_adjoint_set_porosity", "flb_adjoint_set_force",
     "flb_adjoint_forward", "flb_adjoint_backward", "flb_adjoint_timing", "flb_adjoint_destroy",
     "flb_adjoint_last_error",
@@ -140,6 +141,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "flb_batch_read_field": (C.c_int, [H, C.c_uint32, C.c_int, C.c_void_p, C.c_int]),
         "flb_batch_info": (C.c_int, [H, C.POINTER(C.c_int64)]),
         "flb_batch_set_launch": (C.c_int, [H, C.c_int, C.c_int, C.c_int, C.c_int]),
+        "flb_batch_set_wait_limit": (C.c_int, [H, C.c_uint32]),
         "flb_batch_destroy": (C.c_int, [H]),
         "flb_batch_last_error": (C.c_char_p, [H]),
         "flb_adjoint_desc_init": (None, [C.POINTER(AdjointDesc)]),
@@ -528,6 +530,11 @@ class Batch:
         for instance); the state is kept."""
         m = {"cluster": BATCH_CLUSTER, "team": BATCH_TEAM}[mode]
         self._check(load_library().flb_batch_set_launch(self._h, m, int(group), int(groups), int(threads)))
+
+    def set_wait_limit(self, polls: int):
+        """Polls a team-mode CTA waits at its team's barrier before the launch
+        gives up (0: the default, 2^21)."""
+        self._check(load_library().flb_batch_set_wait_limit(self._h, int(polls)))
 
     def read(self, i: int, field: int) -> np.ndarray:
         ny, nx = self.shapes[i]

@@ -217,8 +217,9 @@ FLB_API flb_status flb_load_checkpoint(flb_handle h, const char* path);
  * by a barrier among the group: a thread-block cluster of 1, 2, 4, 8 or 16
  * CTAs (FLB_BATCH_CLUSTER) or a team of any number of CTAs meeting in global
  * memory, every CTA of the launch resident at once (FLB_BATCH_TEAM, a
- * cooperative launch; a team barrier gives up after about two seconds, and
- * flb_batch_sync then returns FLB_ERR_CUDA).
+ * cooperative launch; a team barrier gives up after about two seconds, or
+ * the limit of flb_batch_set_wait_limit, and flb_batch_sync then returns
+ * FLB_ERR_CUDA).
  * autotune: 0 uses 8-CTA clusters, one CTA per SM; 1 (100 probe steps) or a
  * probe step count > 1 times candidate modes, group sizes and counts on the
  * batch itself and keeps the fastest, then rebuilds the initial state.  The
@@ -243,6 +244,14 @@ FLB_API flb_status flb_batch_info(flb_batch b, int64_t info[8]);
  * FLB_ERR_INVALID_ARGUMENT for a shape out of range, FLB_ERR_UNSUPPORTED for
  * one that cannot launch. */
 FLB_API flb_status flb_batch_set_launch(flb_batch b, int mode, int group, int groups, int threads);
+/* Team mode: how many polls (about 1 us each) a CTA waits at its team's
+ * barrier before the launch gives up; 0 restores the default (2^21).  After
+ * a wait gave up, flb_batch_sync returns FLB_ERR_CUDA, the state and t are
+ * undefined, and flb_batch_step refuses with FLB_ERR_CUDA until
+ * flb_batch_reset.  With FLB_BATCH_SKIP_ARRIVAL=1 in the environment (failure
+ * injection for tests, read at every flb_batch_step) one CTA of every team
+ * never arrives, so every wait runs out. */
+FLB_API flb_status flb_batch_set_wait_limit(flb_batch b, uint32_t polls);
 FLB_API flb_status flb_batch_destroy(flb_batch b);
 FLB_API const char* flb_batch_last_error(flb_batch b);
 

@@ -23,7 +23,7 @@ The remaining examples (coche, pantalon, plenum) hold flags in an older
 encoding (values 0, 6 and 9) and options the current reader rejects; they are
 not used.
 
-Usage: python tests/golden/make_setup_fixtures.py [--ref /path/to/FlowLB]
+Usage: python tests/golden/make_setup_fixtures.py --ref /path/to/FlowLB   (or FLOWLB_REF=/path/to/FlowLB)
 """
 from __future__ import annotations
 
@@ -56,8 +56,11 @@ OVERRIDES = {
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("FLOWLB_REF"),
+                    help="FlowLB source tree (default: $FLOWLB_REF)")
     a = ap.parse_args()
+    if not a.ref:
+        ap.error("give the FlowLB source tree with --ref or FLOWLB_REF")
     for case, subs in OVERRIDES.items():
         src = os.path.join(a.ref, "test", "ejemplos", case)
         dst = os.path.join(HERE, "setup", case)

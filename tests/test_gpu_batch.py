@@ -96,3 +96,63 @@ def test_batch_launch_shape_changes_keep_the_state():
     info = b.info()
     assert (info["mode"], info["group"], info["groups"], info["threads"]) == ("cluster", 4, 3, 1024)
     b.close()
+
+
+def test_full_ensemble_matches_single_handles_at_5000_steps():
+    """The 512-case culvert ensemble at its full sizes (nx up to 1024, ny up
+    to 256) for its full 5,000 steps in the tuned launch shape: eight cases
+    (the largest, the smallest and six seeded picks) equal their own handles
+    bit for bit."""
+    ens = cases.ensemble()
+    b = E.Batch([(e.flags, e.tau, e.fx, 0.0) for e in ens], autotune=1)
+    b.step(5000)
+    b.sync()
+    assert b.info()["t"] == 5000
+    sizes = np.array([e.cells for e in ens])
+    rng = np.random.default_rng(5000)
+    picks = [int(sizes.argmax()), int(sizes.argmin())] + [int(k) for k in rng.choice(len(ens), 6, replace=False)]
+    for i in picks:
+        e = ens[i]
+        s = E.Solver(e.flags, precision=32, tau=e.tau, fx=e.fx)
+        s.step(5000)
+        for name, fid, ref in (("f", E.FIELD_F, s.f), ("rho", E.FIELD_RHO, s.rho), ("u", E.FIELD_U, s.u),
+                               ("flags", E.FIELD_FLAGS, s.flags)):
+            got = b.read(i, fid)
+            assert exact_equal(got, ref), f"case {i} {e.flags.shape} {name}: {first_mismatch(got, ref)}"
+        s.close()
+    b.close()
+
+
+def test_team_barrier_wait_runs_out_and_reset_recovers(monkeypatch):
+    """Failure detection of the team barrier, made on the host: with
+    FLB_BATCH_SKIP_ARRIVAL=1 one CTA of every team never arrives, so every
+    wait runs out after a short limit (4,096 polls) and the kernel leaves.
+    flb_batch_sync reports FLB_ERR_CUDA, stepping is refused until
+    flb_batch_reset, and after the reset the batch steps bit-equal to one
+    handle per case.  The reference has no failure handling here: its CUDA
+    error check exits the process (src/cuda/cudaUtils.cuh:17-26)."""
+    ens = _small_ensemble(6, 99)
+    b = E.Batch(ens, autotune=0)
+    b.set_launch("team", 2, 3, 256)
+    b.set_wait_limit(4096)
+    monkeypatch.setenv("FLB_BATCH_SKIP_ARRIVAL", "1")
+    b.step(9)
+    with pytest.raises(E.FlowLBError) as ei:
+        b.sync()
+    assert ei.value.status == 2  # FLB_ERR_CUDA
+    with pytest.raises(E.FlowLBError) as ei:
+        b.step(1)
+    assert ei.value.status == 2
+    monkeypatch.delenv("FLB_BATCH_SKIP_ARRIVAL")
+    b.reset()
+    b.set_wait_limit(0)
+    b.step(21)
+    b.sync()
+    assert b.info()["t"] == 21
+    for i, (flags, tau, gx, gy) in enumerate(ens):
+        s = E.Solver(flags, precision=32, tau=tau, fx=gx, fy=gy)
+        s.step(21)
+        got = b.read(i, E.FIELD_F)
+        assert exact_equal(got, s.f), f"case {i}: {first_mismatch(got, s.f)}"
+        s.close()
+    b.close()
