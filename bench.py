@@ -237,6 +237,8 @@ def run_ours(args, rank, local_rank, world):
     S = args.lattice_steps
     solver = E.Solver(case.flags, free_surface=True, precision=32, mass_precision=64, tau=case.tau, fy=case.fy,
                       bounce_back=E.BB_HALFWAY, fs_mode=E.FS_CONSERVATIVE, device=local_rank, u_max=U_MAX)
+    solver.set_step_mode({"auto": E.STEP_AUTO, "kernels": E.STEP_KERNELS,
+                          "persistent": E.STEP_PERSISTENT}[args.step_mode])
     stream = torch.cuda.ExternalStream(solver.stream, device=local_rank)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local_rank}")
 
@@ -518,6 +520,8 @@ def main():
     ap.add_argument("--ref-lattice-steps", type=int, default=40)
     ap.add_argument("--cpu-steps", type=int, default=2000)
     ap.add_argument("--batch-steps", type=int, default=1000, help="steps of the batch measurement (scaled to 5000)")
+    ap.add_argument("--step-mode", default="auto", choices=["auto", "kernels", "persistent"],
+                    help="free-surface step form (flb_set_step_mode)")
     ap.add_argument("--no-extra", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -138,7 +138,29 @@ struct ListBuild {
   uint32_t* other_counts;  // [2]: the other parity's lengths, zeroed by the build
 };
 
-__device__ __forceinline__ uint32_t tile_count(const TileList& tl) { return tl.all ? tl.ntiles : __ldcg(tl.count); }
+// What the persistent free-surface step (k_fsp.cu) needs besides the step
+// parameters: the lists and their lengths of both parities (read by the step
+// of that parity, built by the step before), the activity words, and its
+// grid barrier.
+struct FspArgs {
+  uint32_t* list[2][2];  // [parity][0: FS_1 and stream-collide, 1: flag pass]
+  uint32_t* lcount;      // [parity][2] list lengths
+  uint32_t* nz;
+  uint32_t* nz_prev;
+  uint32_t nsx, nsy;
+  int prev_unknown;      // the flag pass visits every super-tile (thin last super-tiles)
+  uint32_t* bar;         // grid barrier arrivals, zeroed before each launch
+  uint32_t* err;         // set when a barrier wait gave up
+  uint32_t steps;        // even: the run starts at an even t with flag buffer 0 current
+  uint32_t wait_limit;   // polls before a barrier wait gives up
+  uint32_t skip_cta;     // failure injection: this CTA never arrives (0xffffffff: none)
+};
+
+// A list holds at most ntiles entries; the length is clamped so that no state
+// (a launch that gave up part-way, for instance) can make a pass read past it.
+__device__ __forceinline__ uint32_t tile_count(const TileList& tl) {
+  return tl.all ? tl.ntiles : min(__ldcg(tl.count), tl.ntiles);
+}
 __device__ __forceinline__ uint32_t tile_at(const TileList& tl, uint32_t i) { return tl.all ? i : tl.list[i]; }
 
 template <class S>

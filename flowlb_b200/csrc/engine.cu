@@ -27,6 +27,10 @@ namespace {
 enum Variant { V_F64 = 0, V_F32 = 1, V_F16S = 2, V_F32M32 = 3 };
 
 constexpr int kGraphPairs = 16;  // steps per large graph = 2 * kGraphPairs
+// FLB_STEP_AUTO runs the free-surface step as one persistent kernel on grids of
+// up to this many super-tiles (where every pass is one latency-bound round)
+constexpr uint32_t kPersistAutoTiles = 4096;
+constexpr uint32_t kPersistWaitLimit = 1u << 22;  // barrier polls before the persistent step gives up
 
 struct GraphSlot {
   cudaGraph_t graph = nullptr;
@@ -62,6 +66,18 @@ struct flb_engine {
   bool lists_valid = false;       // lists of the current parity were built by the previous step
   bool thin_tiles = false;        // a last super-tile column or row narrower than the flag pass's reach
   uint32_t grid_sc = 0, grid_fs1 = 0, grid_fs234 = 0;
+  // persistent free-surface step (k_fsp.cu): requested mode, resolved path,
+  // resident grid, barrier count and error word
+  int step_mode = FLB_STEP_AUTO;
+  bool persist = false;
+  uint32_t grid_persist = 0;
+  uint32_t wait_limit = kPersistWaitLimit;
+  uint32_t g_skip = 0xffffffffu;  // failure injection the captured graphs were built with
+  uint32_t* d_bar = nullptr;
+  uint32_t* d_perr = nullptr;
+  // a barrier of the persistent step gave up: the state is undefined and
+  // stepping is refused until flb_reset
+  bool broken = false;
   KParams kp{};
   // device buffers
   void* d_f = nullptr;
@@ -142,6 +158,10 @@ struct Ops {
     h->grid_fs234 = (uint32_t)(nsm * fs_blocks_per_sm<S, C, M>(h->ntiles <= 4096u ? 1 : 2));
   }
   static void apply_recon(flb_engine* h, uint32_t odd) { launch_apply_recon<S, C, M>(h->kp, h->stream, odd); }
+  static cudaError_t persist(flb_engine* h, const KParams& p0, const KParams& p1, const FspArgs& a) {
+    return launch_fs_persist<S, C, M>(p0, p1, a, h->grid_persist, h->hw, h->fused, h->stream);
+  }
+  static int persist_blocks(flb_engine* h) { return fs_persist_blocks_per_sm<S, C, M>(h->hw, h->fused); }
   static void init_ddf(flb_engine* h) { launch_init_ddf<S, C, M>(h->kp, h->stream, h->d_geo, h->hw); }
   static void mass_partial(flb_engine* h, uint32_t odd) {
     launch_mass_partial<S, C, M>(h->kp, h->stream, odd, h->fs ? 1 : 0, h->hw, h->d_partial);
@@ -261,21 +281,78 @@ uint64_t issue_step(flb_engine* h, uint64_t t, bool write_macro) {
   return k;
 }
 
+// Failure injection for tests, read when the step graphs are built: with
+// FLB_PERSIST_SKIP_ARRIVAL=1 in the environment the last CTA of the persistent
+// step never arrives at its grid barriers, so each wait runs out after the
+// wait limit and the launch reports FLB_ERR_CUDA at the next flb_sync.
+uint32_t persist_skip_cta(flb_engine* h) {
+  const char* v = std::getenv("FLB_PERSIST_SKIP_ARRIVAL");
+  if (!v || std::strcmp(v, "1") != 0 || h->grid_persist == 0) return 0xffffffffu;
+  return h->grid_persist - 1u;
+}
+
+// Issues 2*pairs free-surface steps from an even t (flag buffer 0 current) as
+// one persistent launch.
+flb_status issue_persist(flb_engine* h, int pairs) {
+  const int saved = h->cur;
+  h->cur = 0;
+  refresh_params(h);
+  KParams p0 = h->kp;
+  h->cur = 1;
+  refresh_params(h);
+  KParams p1 = h->kp;
+  h->cur = saved;
+  refresh_params(h);
+  p0.trust_prev = 1;
+  p1.trust_prev = 1;
+  FspArgs a{};
+  for (int q = 0; q < 2; q++)
+    for (int k = 0; k < 2; k++) a.list[q][k] = h->d_list[q][k];
+  a.lcount = h->d_lcount;
+  a.nz = h->d_nz;
+  a.nz_prev = h->d_nz_prev;
+  a.nsx = h->nsx;
+  a.nsy = h->nsy;
+  a.prev_unknown = h->thin_tiles ? 1 : 0;
+  a.bar = h->d_bar;
+  a.err = h->d_perr;
+  a.steps = 2u * (uint32_t)pairs;
+  a.wait_limit = h->wait_limit;
+  a.skip_cta = h->g_skip;
+  cudaError_t e = cudaSuccess;
+  dispatch(h, [&](auto ops) { e = ops.persist(h, p0, p1, a); });
+  if (e != cudaSuccess) return cuda_fail(h, e, "persistent free-surface step launch");
+  return FLB_OK;
+}
+
 void destroy_graph(GraphSlot& g) {
   if (g.exec) cudaGraphExecDestroy(g.exec);
   if (g.graph) cudaGraphDestroy(g.graph);
   g = GraphSlot{};
 }
 
-// Captures 2*pairs steps starting at an even t with flag buffer 0 current.
+// Captures 2*pairs steps starting at an even t with flag buffer 0 current:
+// the passes of every step, or one persistent launch (free surface, h->persist).
 flb_status capture(flb_engine* h, GraphSlot& g, int pairs) {
   if (g.exec) return FLB_OK;
   const int saved_cur = h->cur;
   FLB_CUDA(h, cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
   uint64_t kernels = 0;
-  for (int s = 0; s < 2 * pairs; s++) kernels += issue_step(h, (uint64_t)s, false);
+  flb_status ps = FLB_OK;
+  if (h->fs && h->persist) {
+    ps = issue_persist(h, pairs);
+    kernels = 1;
+  } else {
+    for (int s = 0; s < 2 * pairs; s++) kernels += issue_step(h, (uint64_t)s, false);
+  }
   cudaGraph_t graph = nullptr;
   cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+  if (ps != FLB_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    h->cur = saved_cur;
+    refresh_params(h);
+    return ps;
+  }
   h->cur = saved_cur;
   refresh_params(h);
   if (e != cudaSuccess) return cuda_fail(h, e, "cudaStreamEndCapture");
@@ -291,6 +368,30 @@ flb_status capture(flb_engine* h, GraphSlot& g, int pairs) {
   return FLB_OK;
 }
 
+// Whether the free-surface steps replayed from graphs run as one persistent
+// launch (k_fsp.cu) or as four kernels per step.
+void resolve_persist(flb_engine* h) {
+  const bool can = h->fs && h->grid_persist > 0;
+  h->persist = can && (h->step_mode == FLB_STEP_PERSISTENT ||
+                       (h->step_mode == FLB_STEP_AUTO && h->ntiles <= kPersistAutoTiles));
+}
+
+// Reads (and clears) the persistent step's error word after the stream has
+// drained: a grid barrier that gave up leaves the state undefined.
+flb_status check_persist(flb_engine* h) {
+  if (!h->fs || !h->d_perr) return FLB_OK;
+  uint32_t e = 0;
+  FLB_CUDA(h, cudaMemcpyAsync(&e, h->d_perr, sizeof(e), cudaMemcpyDeviceToHost, h->stream));
+  FLB_CUDA(h, cudaStreamSynchronize(h->stream));
+  if (!e) return FLB_OK;
+  h->broken = true;
+  FLB_CUDA(h, cudaMemsetAsync(h->d_perr, 0, sizeof(uint32_t), h->stream));
+  FLB_CUDA(h, cudaStreamSynchronize(h->stream));
+  return fail(h, FLB_ERR_CUDA,
+              "a grid barrier of the persistent free-surface step gave up waiting; the state is undefined until "
+              "flb_reset");
+}
+
 void free_all(flb_engine* h) {
   destroy_graph(h->g_pair);
   destroy_graph(h->g_big);
@@ -299,7 +400,7 @@ void free_all(flb_engine* h) {
                   h->d_recon,      h->d_recon_mask,  h->d_rho_snap,    h->d_u_snap,      h->d_partial,
                   h->d_scalar,     h->d_counts,      h->d_nz,          h->d_nz_prev,     h->d_list[0][0],
                   h->d_list[0][1], h->d_list[1][0],  h->d_list[1][1],  h->d_lcount,     h->d_tstep,
-                  h->d_plain};
+                  h->d_plain,      h->d_bar,         h->d_perr};
   for (void* p : bufs)
     if (p) cudaFree(p);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
@@ -371,6 +472,7 @@ flb_status initialise(flb_engine* h) {
   refresh_plain(h);
   h->trust = true;  // flags[1] = flags[0] and the initial fields satisfy the skip invariants
   h->lists_valid = false;
+  h->broken = false;
   FLB_CUDA(h, cudaGetLastError());
   return FLB_OK;
 }
@@ -573,6 +675,8 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
       {(void**)&h->d_list[1][0], tiles * sizeof(uint32_t), h->fs},
       {(void**)&h->d_list[1][1], tiles * sizeof(uint32_t), h->fs},
       {(void**)&h->d_lcount, 4 * sizeof(uint32_t), h->fs},
+      {(void**)&h->d_bar, sizeof(uint32_t), h->fs},
+      {(void**)&h->d_perr, sizeof(uint32_t), h->fs},
   };
   // Failure injection on the host: with FLB_FAIL_ALLOC_AT=k in the
   // environment the k-th device allocation of this creation fails as
@@ -590,9 +694,17 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
     // list lengths start at zero
     cudaError_t e0 = cudaMemsetAsync(h->d_lcount, 0, 4 * sizeof(uint32_t), h->stream);
     if (e0 != cudaSuccess) return bail(cuda_fail(h, e0, "cudaMemsetAsync"));
+    e0 = cudaMemsetAsync(h->d_perr, 0, sizeof(uint32_t), h->stream);
+    if (e0 != cudaSuccess) return bail(cuda_fail(h, e0, "cudaMemsetAsync"));
     int nsm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device);
     dispatch(h, [&](auto ops) { ops.grids(h, nsm > 0 ? nsm : 1); });
+    // the persistent step needs every CTA resident at once (inlet/outlet cells
+    // need a density/velocity snapshot before each stream-collide: per-pass only)
+    int per_sm = 0;
+    dispatch(h, [&](auto ops) { per_sm = ops.persist_blocks(h); });
+    h->grid_persist = h->has_io || per_sm <= 0 ? 0u : (uint32_t)(nsm * per_sm);
+    resolve_persist(h);
   }
   fill_case_constants(desc, h->kp);
   cudaError_t e = cudaMemcpyAsync(h->d_geo, desc->flags, N, cudaMemcpyHostToDevice, h->stream);
@@ -636,8 +748,18 @@ FLB_API flb_status flb_destroy(flb_handle h) {
 
 FLB_API flb_status flb_step(flb_handle h, uint64_t n) {
   if (!h) return FLB_ERR_INVALID_ARGUMENT;
+  if (h->broken)
+    return fail(h, FLB_ERR_CUDA, "a grid barrier of the persistent step gave up in an earlier launch; call flb_reset");
   if (n == 0) return FLB_OK;
   DeviceGuard guard(h->device);
+  if (h->fs && h->persist) {
+    const uint32_t skip = persist_skip_cta(h);
+    if (skip != h->g_skip) {  // graphs carry the injection setting they were built with
+      destroy_graph(h->g_pair);
+      destroy_graph(h->g_big);
+      h->g_skip = skip;
+    }
+  }
   nvtxRangePushA("flb_step");
   uint64_t remaining = n;
   flb_status s = FLB_OK;
@@ -682,6 +804,46 @@ FLB_API flb_status flb_sync(flb_handle h) {
   if (!h) return FLB_ERR_INVALID_ARGUMENT;
   DeviceGuard guard(h->device);
   FLB_CUDA(h, cudaStreamSynchronize(h->stream));
+  return check_persist(h);
+}
+
+FLB_API flb_status flb_set_step_mode(flb_handle h, int mode) {
+  if (!h) return FLB_ERR_INVALID_ARGUMENT;
+  if (mode != FLB_STEP_AUTO && mode != FLB_STEP_KERNELS && mode != FLB_STEP_PERSISTENT)
+    return fail(h, FLB_ERR_INVALID_ARGUMENT, "mode must be FLB_STEP_AUTO, FLB_STEP_KERNELS or FLB_STEP_PERSISTENT");
+  if (mode == FLB_STEP_PERSISTENT && !(h->fs && h->grid_persist > 0))
+    return fail(h, FLB_ERR_UNSUPPORTED,
+                "the persistent step needs a free-surface case without inlet/outlet cells that can keep every CTA "
+                "resident");
+  DeviceGuard guard(h->device);
+  FLB_CUDA(h, cudaStreamSynchronize(h->stream));  // a running graph may be the one replaced
+  const bool before = h->persist;
+  h->step_mode = mode;
+  resolve_persist(h);
+  if (before != h->persist) {
+    destroy_graph(h->g_pair);
+    destroy_graph(h->g_big);
+  }
+  return FLB_OK;
+}
+
+FLB_API flb_status flb_get_step_mode(flb_handle h, int* mode, int* persistent) {
+  if (!h) return FLB_ERR_INVALID_ARGUMENT;
+  if (mode) *mode = h->step_mode;
+  if (persistent) *persistent = h->persist ? 1 : 0;
+  return FLB_OK;
+}
+
+FLB_API flb_status flb_set_wait_limit(flb_handle h, uint32_t polls) {
+  if (!h) return FLB_ERR_INVALID_ARGUMENT;
+  DeviceGuard guard(h->device);
+  FLB_CUDA(h, cudaStreamSynchronize(h->stream));
+  const uint32_t v = polls == 0 ? kPersistWaitLimit : polls;
+  if (v != h->wait_limit) {
+    h->wait_limit = v;
+    destroy_graph(h->g_pair);
+    destroy_graph(h->g_big);
+  }
   return FLB_OK;
 }
 
@@ -769,7 +931,7 @@ FLB_API flb_status flb_read_field(flb_handle h, int field, void* dst, int on_dev
     FLB_CUDA(h, cudaMemcpyAsync(dst, src, bytes, kind, h->stream));
   }
   FLB_CUDA(h, cudaStreamSynchronize(h->stream));
-  return FLB_OK;
+  return check_persist(h);
 }
 
 FLB_API flb_status flb_write_field(flb_handle h, int field, const void* src, int on_device) {

@@ -1,0 +1,507 @@
+// fs_cells.cuh -- per-cell and per-tile device code of the free-surface
+// passes: FS_1 (lbmKernel2D.cu:14-121) and FS_2, FS_3, FS_4 fused into one
+// shared-memory flag stencil (lbmKernel2D.cu:124-303), plus the super-tile
+// activity words the list build reads.  Shared by the per-pass kernels
+// (k_fs.cu) and the persistent free-surface step (k_fsp.cu).
+#pragma once
+
+#include "common.cuh"
+
+namespace flb {
+
+// ---- FS_1: mass exchange and gas reconstruction, lbmKernel2D.cu:14-121 -----
+template <class S, class C, class M, bool HW, bool ODD>
+__device__ __forceinline__ void fs1_cell(const KParams& p, uint32_t x, uint32_t y) {
+  const uint32_t nx = p.nx, N = p.N;
+  const uint32_t idx = x + y * nx;
+  const uint8_t* flags = p.flags;
+  const uint8_t flag = flags[idx];
+  if (flag & (kGas | kWall | kInlet)) return;
+  const bool cons = p.fs_cons != 0;
+  const uint8_t e = flag & kFGI;
+  if (cons && (!(e == kFluid || e == kInterface) || (flag & kMovingWall))) return;
+  uint32_t nb[9];
+  neighbours(x, y, nx, p.ny, nb);
+  C in[9], out[9];
+  load_in<S, C, HW, ODD>(p, idx, nb, HW ? p.nbmask[idx] : 0u, in);
+  out[0] = in[0];
+  load_out<S, C, ODD>(p, idx, nb, out);
+  M* Ms = static_cast<M*>(p.mass);
+  const M* Ex = static_cast<const M*>(p.excess);
+  const M* Ph = static_cast<const M*>(p.phi);
+  M m = Ms[idx];
+#pragma unroll
+  for (int i = 1; i < 9; i++) m += Ex[nb[i]];
+  if (e == kFluid) {
+    if (!cons) {
+#pragma unroll
+      for (int i = 1; i < 9; i += 2) {
+        m += in[i + 1] - out[i];
+        m += in[i] - out[i + 1];
+      }
+    } else {
+#pragma unroll
+      for (int i = 1; i < 9; i += 2) {
+        const uint8_t na = flags[nb[i]] & kFGI, nbb = flags[nb[i + 1]] & kFGI;
+        if (na == kFluid || na == kInterface) m += in[i + 1] - out[i];
+        if (nbb == kFluid || nbb == kInterface) m += in[i] - out[i + 1];
+      }
+    }
+  } else if (e == kInterface) {
+    C rho, ux, uy, rhoYL = 0.0f;
+    if (flag & (kInlet | kOutlet)) {
+      rho = static_cast<const C*>(p.rho)[idx];
+      ux = static_cast<const C*>(p.u)[idx];
+      uy = static_cast<const C*>(p.u)[idx + N];
+    } else {
+      rho = density(out);
+      velocity(out, rho, ux, uy);
+    }
+    M phiN[9];
+#pragma unroll
+    for (int i = 1; i < 9; i++) phiN[i] = Ph[nb[i]];
+    phiN[0] = cons ? Ph[idx] : fill_level<M, C>(m, rho);
+    const C rho2 = 0.5f / rho;
+    ux = ux + rho2 * p.fx;
+    uy = uy + rho2 * p.fy;
+    limit_u(p.u_max, ux, uy);
+    C feq[9];
+    equilibrium<C>(1.0f - rhoYL, ux, uy, feq);
+    uint8_t nF[9];
+#pragma unroll
+    for (int i = 1; i < 9; i++) nF[i] = flags[nb[i]] & kFGI;
+#pragma unroll
+    for (int i = 1; i < 9; i += 2) {
+      uint8_t ne = nF[i];
+      if (ne == kFluid) m += in[i + 1] - out[i];
+      else if (ne == kInterface) m += (in[i + 1] - out[i]) * 0.5f * (phiN[i] + phiN[0]);
+      ne = nF[i + 1];
+      if (ne == kFluid) m += in[i] - out[i + 1];
+      else if (ne == kInterface) m += (in[i] - out[i + 1]) * 0.5f * (phiN[i + 1] + phiN[0]);
+    }
+#pragma unroll
+    for (int i = 1; i < 9; i += 2) {
+      in[i] = feq[i] - out[i + 1] + feq[i + 1];
+      in[i + 1] = feq[i + 1] - out[i] + feq[i];
+    }
+    if (!cons) {
+      // reference gate (storeReconstructedGasf, cellCalculations.cuh:250-259):
+      // tests the neighbour the population travels toward.  Parked in recon so
+      // that neighbours reading their outgoing slots see the pre-pass values.
+      C* rec = static_cast<C*>(p.recon);
+      uint32_t mask = 0;
+#pragma unroll
+      for (int i = 1; i < 9; i += 2) {
+        if (nF[i] == kGas) { mask |= 1u << (i - 1); rec[(uint32_t)(i - 1) * N + idx] = in[i]; }
+        if (nF[i + 1] == kGas) { mask |= 1u << i; rec[(uint32_t)i * N + idx] = in[i + 1]; }
+      }
+      p.recon_mask[idx] = (uint8_t)mask;
+    } else {
+      // population arriving from a gas neighbour: its slot is read by no other
+      // cell in this pass (the gas cell does not run), so store in place
+      const float scale = p.f16_scale;
+#pragma unroll
+      for (int i = 1; i < 9; i += 2) {
+        if (nF[i + 1] == kGas) Codec<S, C>::st(slotp<S>(p, slot_a<ODD>(i)), idx, i, in[i], scale);
+        if (nF[i] == kGas) Codec<S, C>::st(slotp<S>(p, slot_b<ODD>(i)), nb[i], i + 1, in[i + 1], scale);
+      }
+    }
+  }
+  Ms[idx] = m;
+}
+
+// ---- FS_2 + FS_3 + FS_4 fused: lbmKernel2D.cu:124-303 ----------------------
+// The three reference passes are flag stencils of radius one, chained; a tile
+// of kTX x 8 cells stages the flags of its 3-cell halo in shared memory and
+// evaluates the chain there, so neighbour flags are never read while another
+// block rewrites them.  Reads p.flags, writes p.flags_out.
+// Tile width of the flag pass: 128 (a whole super-tile, 1024 threads) or 32
+// (a quarter, 256 threads).  Measured on a B200, dam break: 2048x512 (about
+// 300 active super-tiles) 31 vs 25 GLUPS in favour of 128; 8192x2048 (about
+// 4400) 53 vs 59 in favour of 32 (more resident warps).  launch_fs234 picks by
+// the grid's super-tile count (kWideTiles).
+constexpr int kTY = 8, kHalo = 3;
+constexpr uint32_t kWideTiles = 4096;
+#ifndef FLB_FS_WIDE_MIN_BLOCKS
+#define FLB_FS_WIDE_MIN_BLOCKS 2
+#endif
+// periodic index; halos of in-range tiles need one add or subtract, the
+// modulo is only reached on grids narrower than a tile
+__device__ __forceinline__ int wrapi(int v, int n) {
+  if (v < 0) v += n;
+  else if (v >= n) v -= n;
+  if ((unsigned)v >= (unsigned)n) v = ((v % n) + n) % n;
+  return v;
+}
+
+// ex / cont for a neighbour count of 1..8.  Counts 1, 2, 4 and 8 scale by an
+// exact power of two, which rounds exactly as the division does; only 3, 5, 6
+// and 7 divide (a double division is a long instruction sequence, and deep
+// fluid cells all have 8 neighbours).
+template <class M>
+__device__ __forceinline__ M div_count(M ex, int cont) {
+  if ((cont & (cont - 1)) == 0) return ex * (M)(1.0f / (float)cont);
+  return ex / (M)(float)cont;
+}
+
+// Bit-plane form of the stencil chain.  For each row of the tile and of its
+// 3-row halo, and each 32-cell word of the tile plus one word on either side,
+// a warp ballot turns 32 flag bytes into predicate masks (bit i = cell i of the
+// word).  FS_2's and FS_3's "any neighbour with property P" is then an 8-way
+// dilation of a mask (shifts and ORs across neighbouring words and rows), the
+// flag rewrites are bitwise logic on whole words, and FS_4's neighbour count
+// is a popcount of a 3x3 window; each cell finally reads its own bits.  The
+// words at the outer ends of a row lack a neighbour word, so their outermost
+// bits are wrong after each dilation; the three stages reach at most the third
+// bit from either end, and only the innermost 3 bits of those words (the halo)
+// are read.
+template <int TW>
+struct FlagMasks {
+  static constexpr int kW = TW / 32 + 2;      // words per row
+  static constexpr int kR = kTY + 2 * kHalo;  // rows
+  // from the flags after stream-collide (s0)
+  uint32_t a[kR][kW];      // (f & 5) == 5   IF
+  uint32_t gas[kR][kW];    // f & GAS
+  uint32_t gonly[kR][kW];  // (f & 6) == 2   gas, not interface
+  uint32_t gi[kR][kW];     // f & GAS_INTERFACE
+  uint32_t fl[kR][kW];     // FLUID set, INLET clear
+  uint32_t it[kR][kW];     // f & INTERFACE
+  uint32_t fb[kR][kW];     // f & FLUID
+  uint32_t sk[kR][kW];     // f & (WALL | MOVING_WALL | INLET)
+  // derived
+  uint32_t anyif[kR][kW];  // FS_2: a neighbour is IF
+  uint32_t ig1[kR][kW];    // after FS_2: (f & (GI | IG)) == IG
+  uint32_t p1[kR][kW];     // after FS_2: GAS bit
+  uint32_t p7[kR][kW];     // after FS_2: GAS_INTERFACE bit
+  uint32_t anyig[kR][kW];  // FS_3: a neighbour is IG (after FS_2)
+  uint32_t cnt[kR][kW];    // after FS_4's conversion: counted by FS_4's neighbour count
+};
+
+// 8-neighbourhood of bit i of word c, row r, of mask m (missing words read 0).
+template <int TW>
+__device__ __forceinline__ uint32_t dilate8(const uint32_t (&m)[FlagMasks<TW>::kR][FlagMasks<TW>::kW], int r,
+                                            int c) {
+  constexpr int kW = FlagMasks<TW>::kW;
+  uint32_t out = 0;
+#pragma unroll
+  for (int dr = -1; dr <= 1; dr++) {
+    const uint32_t w = m[r + dr][c];
+    const uint32_t l = c > 0 ? m[r + dr][c - 1] : 0u;
+    const uint32_t rt = c < kW - 1 ? m[r + dr][c + 1] : 0u;
+    const uint32_t sh = (w << 1) | (l >> 31) | (w >> 1) | (rt << 31);  // left and right neighbours
+    out |= dr ? (sh | w) : sh;
+  }
+  return out;
+}
+
+// Bits i-1, i, i+1 of row r around word c (c has words on both sides).
+template <int TW>
+__device__ __forceinline__ uint32_t window3(const uint32_t (&m)[FlagMasks<TW>::kR][FlagMasks<TW>::kW], int r, int c,
+                                            int i) {
+  const uint64_t v = ((uint64_t)m[r][c + 1] << 33) | ((uint64_t)m[r][c] << 1) | (uint64_t)(m[r][c - 1] >> 31);
+  return (uint32_t)(v >> i) & 7u;
+}
+
+template <int TW>
+__device__ __forceinline__ bool bit_at(const uint32_t (&m)[FlagMasks<TW>::kR][FlagMasks<TW>::kW], int r, int c,
+                                       int i) {
+  if (i < 0) {
+    c--;
+    i += 32;
+  } else if (i >= 32) {
+    c++;
+    i -= 32;
+  }
+  return (m[r][c] >> i) & 1u;
+}
+
+// One TW x 8 tile (tile coordinates tx, ty) with the TW*8 threads of the block;
+// every thread of the block must call it.  Returns whether this thread's cell
+// is fluid or interface after the pass.
+template <class S, class C, class M, bool ODD, int TW>
+__device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int tid, FlagMasks<TW>& sm) {
+  constexpr int kTX = TW, kW = FlagMasks<TW>::kW, kR = FlagMasks<TW>::kR;
+  constexpr int kWarps = TW * kTY / 32;
+  const int nx = (int)p.nx, ny = (int)p.ny;
+  const uint8_t* flags = p.flags;
+  // this thread's cell: its own values are loaded now, so that their latency
+  // overlaps the mask building and the stencil stages
+  const int gx = tx * kTX + tid % kTX, gy = ty * kTY + tid / kTX;
+  const bool in = gx < nx && gy < ny;
+  const uint32_t idx = in ? (uint32_t)gx + (uint32_t)gy * (uint32_t)nx : 0u;
+  M* Ms = static_cast<M*>(p.mass);
+  M* Exs = static_cast<M*>(p.excess);
+  const C* R = static_cast<const C*>(p.rho);
+  uint8_t old = 0, f0 = 0;
+  M m_old = M(0), ex_old = M(0);
+  C rho_own = C(0);
+  if (in) {
+    f0 = flags[idx];
+    old = p.flags_out[idx];
+    m_old = Ms[idx];
+    ex_old = Exs[idx];
+    rho_own = R[idx];
+  }
+  // masks of the flags after stream-collide: every flag byte a lane needs is
+  // loaded first, so the loads of all its row-words are in flight together
+  const int lane = tid & 31, warp = tid >> 5;
+  const int xw = tx * kTX - 32 + lane;  // word 0 starts one word left of the tile
+  constexpr int kRW = kR * kW, kIters = (kRW + kWarps - 1) / kWarps;
+  uint8_t fv[kIters];
+#pragma unroll
+  for (int k = 0; k < kIters; k++) {
+    const int rw = warp + k * kWarps;
+    const int r = rw / kW, c = rw % kW;
+    fv[k] = rw < kRW ? flags[wrapi(xw + 32 * c, nx) + wrapi(ty * kTY - kHalo + r, ny) * nx] : 0;
+  }
+#pragma unroll
+  for (int k = 0; k < kIters; k++) {
+    const int rw = warp + k * kWarps;  // the same for the whole warp
+    if (rw >= kRW) break;
+    const int r = rw / kW, c = rw % kW;
+    const uint8_t f = fv[k];
+    // ballots of the flag bits; the masks a row needs are formed from them:
+    // the outer halo rows only feed FS_2's IF dilation, the next rows also
+    // FS_2's rewrite, the inner ten rows everything (warp-uniform branches)
+    const uint32_t bF = __ballot_sync(0xffffffffu, (f & kFluid) != 0);
+    const uint32_t bI = __ballot_sync(0xffffffffu, (f & kInterface) != 0);
+    if (lane == 0) sm.a[r][c] = bF & bI;
+    if (r == 0 || r == kR - 1) continue;
+    const uint32_t bG = __ballot_sync(0xffffffffu, (f & kGas) != 0);
+    const uint32_t bGI = __ballot_sync(0xffffffffu, (f & kGasInterface) != 0);
+    if (lane == 0) {
+      sm.gas[r][c] = bG;
+      sm.gonly[r][c] = bG & ~bI;
+      sm.gi[r][c] = bGI;
+      sm.it[r][c] = bI;
+    }
+    if (r == 1 || r == kR - 2) continue;
+    const uint32_t bIn = __ballot_sync(0xffffffffu, (f & kInlet) != 0);
+    const uint32_t bSk = __ballot_sync(0xffffffffu, (f & (kWall | kMovingWall | kInlet)) != 0);
+    if (lane == 0) {
+      sm.fl[r][c] = bF & ~bIn;
+      sm.fb[r][c] = bF;
+      sm.sk[r][c] = bSk;
+    }
+  }
+  __syncthreads();
+  // FS_2 on rows 1 .. kR-2: next to an IF cell, IG -> I and G -> GI
+  if (tid < (kR - 2) * kW) {
+    const int r = 1 + tid / kW, c = tid % kW;
+    const uint32_t any_if = dilate8<TW>(sm.a, r, c);
+    const uint32_t p1 = sm.gas[r][c] & ~any_if;
+    const uint32_t p7 = sm.gi[r][c] | (any_if & sm.gonly[r][c]);
+    sm.anyif[r][c] = any_if;
+    sm.p1[r][c] = p1;
+    sm.p7[r][c] = p7;
+    sm.ig1[r][c] = p1 & sm.it[r][c] & ~p7;
+  }
+  __syncthreads();
+  // FS_3 on rows 2 .. kR-3: next to an IG cell, F / IF (not inlet) -> I; then
+  // FS_4's conversion and the mask of the neighbours FS_4 counts
+  if (tid < (kR - 4) * kW) {
+    const int r = 2 + tid / kW, c = tid % kW;
+    const uint32_t any_ig = dilate8<TW>(sm.ig1, r, c);
+    const uint32_t conv = sm.fl[r][c] & any_ig;
+    const uint32_t P0 = sm.fb[r][c] & ~conv, P1 = sm.p1[r][c], P2 = sm.it[r][c] | conv, P7 = sm.p7[r][c];
+    const uint32_t go = ~sm.sk[r][c];
+    const uint32_t to_plain = go & ((P0 & ~P1 & P2 & ~P7) | (~P0 & P1 & P2 & ~P7));  // IF, IG lose the I bit
+    const uint32_t from_gi = go & (~P0 & ~P1 & ~P2 & P7);                          // GI -> I
+    const uint32_t P2f = (P2 & ~to_plain) | from_gi, P7f = P7 & ~from_gi;
+    sm.anyig[r][c] = any_ig;
+    sm.cnt[r][c] = p.fs_cons ? ((P0 ^ P2f) & ~P1 & go) : ((P0 | P2f) ^ P7f);
+  }
+  __syncthreads();
+  if (!in) return false;
+  const int lx = tid % kTX, ly = tid / kTX;
+  const int r = kHalo + ly, c = 1 + lx / 32, i = lx % 32;
+  const bool any_if = (sm.anyif[r][c] >> i) & 1u, any_ig = (sm.anyig[r][c] >> i) & 1u;
+  // the byte chain of the reference passes, for this cell
+  uint8_t f1 = f0;
+  if (any_if) {
+    const uint8_t e = f1 & kIG;
+    if (e == kIG) f1 = (uint8_t)(f1 & ~kGas);
+    else if (e == kGas) f1 = (uint8_t)((f1 & ~kGas) | kGasInterface);
+  }
+  uint8_t f3 = f1;
+  {
+    const uint8_t e = f3 & (kInletFluid | kInterface);
+    if (e != kInletFluid && (e == kFluid || e == kIF) && any_ig) f3 = (uint8_t)((f3 & ~kIF) | kInterface);
+  }
+  uint8_t fin = f3;
+  if (!(fin & (kWall | kMovingWall | kInlet))) {
+    const uint8_t sw = fin & (kFGI | kGasInterface);
+    if (sw == kIF || sw == kIG) fin = (uint8_t)(fin & ~kInterface);
+    else if (sw == kGasInterface) fin = (uint8_t)((fin & ~kGasInterface) | kInterface);
+  }
+  const uint32_t N = p.N;
+  const bool live = (fin & (kWall | kMovingWall)) == 0 && ((fin & kFGI) == kFluid || (fin & kFGI) == kInterface);
+  // Write skipping.  flags_out still holds this cell's flag after the previous
+  // step's stream-collide ("old").  When the buffers come from consecutive
+  // full steps (trust_prev), values already in memory are not rewritten:
+  //  * the flag, when old equals the new flag;
+  //  * the fill level of a cell that is fluid (gas) both before and after this
+  //    pass: it was fluid (gas) after the previous step too, whose FS_4 left
+  //    phi = 1 (0);
+  //  * mass and excess of a gas cell when they do not change (deep gas holds
+  //    zeros; a gas cell with no fluid or interface neighbour keeps its mass,
+  //    lbmKernel2D.cu:296, so nothing else is assumed about them).
+  const bool trust = p.trust_prev != 0;
+  if (!trust || old != fin) p.flags_out[idx] = fin;
+  const C* U = static_cast<const C*>(p.u);
+  // FS_3 fields: a gas->interface cell starts from feq of the neighbour
+  // average (calculateAverageValuesNeighbors2D, accumulating in float)
+  if ((f1 & (kGasInterface | kIG)) == kGasInterface) {
+    uint32_t nb[9];
+    neighbours((uint32_t)gx, (uint32_t)gy, (uint32_t)nx, (uint32_t)ny, nb);
+    float count = 0.0f, lrho = 0.0f, lux = 0.0f, luy = 0.0f;
+    const int ddx[9] = {0, 1, -1, 0, 0, 1, -1, 1, -1};
+    const int ddy[9] = {0, 0, 0, 1, -1, 1, -1, -1, 1};
+#pragma unroll
+    for (int k = 1; k < 9; k++) {
+      // FLUID or INTERFACE set after FS_2 (FS_2 changes neither bit)
+      if (bit_at<TW>(sm.fb, r + ddy[k], c, i + ddx[k]) || bit_at<TW>(sm.it, r + ddy[k], c, i + ddx[k])) {
+        count += 1.0f;
+        lrho += R[nb[k]];
+        lux += U[nb[k]];
+        luy += U[nb[k] + N];
+      }
+    }
+    C rho = count > 0.0f ? lrho / count : 0.0f;
+    C ux = count > 0.0f ? lux / count : 0.0f;
+    C uy = count > 0.0f ? luy / count : 0.0f;
+    C feq[9];
+    const C rho2 = 0.5f / rho;
+    ux = ux + rho2 * p.fx;
+    uy = uy + rho2 * p.fy;
+    limit_u(p.u_max, ux, uy);
+    equilibrium(rho, ux, uy, feq);
+    store_post<S, C, ODD>(p, idx, nb, feq);
+  }
+  // FS_4 fields
+  if (f3 & (kWall | kMovingWall | kInlet)) return live;
+  const uint8_t sw4 = f3 & (kFGI | kGasInterface);
+  const uint8_t sw0 = f0 & (kFGI | kGasInterface);
+  const bool gas_stays = trust && sw4 == kGas && sw0 == kGas;
+  const bool keep_phi = gas_stays || (trust && sw4 == kFluid && sw0 == kFluid);
+  const C rho = sw4 == kGas ? C(0) : rho_own;  // the gas case does not use the density
+  M m = m_old;
+  M ex = 0.0f, ph = 0.0f;
+  switch (f3 & (kFGI | kGasInterface)) {
+    case 1:
+    case 5:
+      ex = m - rho;
+      m = rho;
+      ph = 1.0f;
+      break;
+    case 2:
+    case 6:
+      ex = m;
+      m = 0.0f;
+      ph = 0.0f;
+      break;
+    case 4:
+    case 128:
+      if (m > rho) {
+        ex = m - rho;
+        m = rho;
+      } else if (m < 0.0f) {
+        ex = m;
+        m = 0.0f;
+      } else {
+        ex = 0.0f;
+      }
+      ph = fill_level<M, C>(m, rho);
+      break;
+    default:
+      break;
+  }
+  // FS_4's count of fluid / interface neighbours after the conversion
+  const int cont = __popc(window3<TW>(sm.cnt, r - 1, c, i)) + __popc(window3<TW>(sm.cnt, r, c, i) & 5u) +
+                   __popc(window3<TW>(sm.cnt, r + 1, c, i));
+  m += cont > 0 ? 0.0f : ex;
+  ex = cont > 0 ? div_count(ex, cont) : M(0);
+  if (gas_stays) {
+    if (!same_bits(m, m_old)) Ms[idx] = m;
+    if (!same_bits(ex, ex_old)) Exs[idx] = ex;
+  } else {
+    Ms[idx] = m;
+    Exs[idx] = ex;
+  }
+  if (!keep_phi) static_cast<M*>(p.phi)[idx] = ph;
+  return live;
+}
+
+// Per super-tile activity word written by the flag pass: bit 0 = it holds a
+// fluid or interface cell; bits 1..8 = it holds one within kReach cells of
+// the edge or corner facing the neighbour in direction (dx, dy) (edge_bit).
+// The stencil chain of the flag pass reaches kReach = 3 cells, so a neighbour
+// needs the pass next step only if such a cell faces it.
+constexpr int kReach = 3;
+__host__ __device__ constexpr int edge_bit(int dx, int dy) {
+  return dy == 0 ? (dx > 0 ? 1 : 2) : dx == 0 ? (dy > 0 ? 3 : 4) : dy > 0 ? (dx > 0 ? 5 : 6) : (dx > 0 ? 7 : 8);
+}
+
+// Activity word of a live cell at (lx, ly) in a super-tile of wact x hact cells.
+__device__ __forceinline__ uint32_t activity(int lx, int ly, int wact, int hact) {
+  const bool r = lx >= wact - kReach, l = lx < kReach, u = ly >= hact - kReach, d = ly < kReach;
+  return 1u | ((uint32_t)r << edge_bit(1, 0)) | ((uint32_t)l << edge_bit(-1, 0)) | ((uint32_t)u << edge_bit(0, 1)) |
+         ((uint32_t)d << edge_bit(0, -1)) | ((uint32_t)(u && r) << edge_bit(1, 1)) |
+         ((uint32_t)(u && l) << edge_bit(-1, 1)) | ((uint32_t)(d && r) << edge_bit(1, -1)) |
+         ((uint32_t)(d && l) << edge_bit(-1, -1));
+}
+
+// Whether super-tile t is visited next step by stream-collide and FS_1 (sc:
+// it holds fluid or interface cells) and by the flag pass (fs: it does, or a
+// neighbour holds such a cell within reach of it, or it did a step earlier);
+// updates nz_prev[t].
+__device__ __forceinline__ void list_flags(const uint32_t* nz, uint32_t* nz_prev, uint32_t nsx, uint32_t nsy,
+                                           int prev_unknown, uint32_t t, bool& sc, bool& fs) {
+  const uint32_t sx = t % nsx, sy = t / nsx;
+  const uint32_t own = __ldcg(nz + t) & 1u;
+  bool near = false;
+#pragma unroll
+  for (int dy = -1; dy <= 1; dy++)
+#pragma unroll
+    for (int dx = -1; dx <= 1; dx++) {
+      if (!dx && !dy) continue;
+      const uint32_t xx = (sx + nsx + dx) % nsx, yy = (sy + nsy + dy) % nsy;
+      near |= (__ldcg(nz + xx + yy * nsx) >> edge_bit(-dx, -dy)) & 1u;  // its edge facing t
+    }
+  sc = own != 0;
+  fs = own || near || prev_unknown || nz_prev[t] != 0;
+  nz_prev[t] = own;
+}
+
+// The listed super-tiles: each block runs the tile pass on the tiles of a
+
+// The flag pass over one super-tile t (its kSTW / TW tiles in turn) with the
+// TW*kTY threads of the block; every thread of the block must call it.
+// Records the super-tile's activity word in nz[t].  wact_sm: one word per
+// warp of the block.
+template <class S, class C, class M, bool ODD, int TW>
+__device__ __forceinline__ void fs234_super_tile(const KParams& p, uint32_t t, uint32_t nsx, uint32_t* nz,
+                                                 FlagMasks<TW>& sm, uint32_t* wact_sm) {
+  constexpr int kTX = TW;
+  const int tid = threadIdx.x;
+  const int sx = (int)(t % nsx), sy = (int)(t / nsx);
+  const int wact = min((int)kSTW, (int)p.nx - sx * (int)kSTW), hact = min((int)kSTH, (int)p.ny - sy * (int)kSTH);
+  uint32_t act = 0;
+#pragma unroll 1
+  for (int j = 0; j < (int)(kSTW / kTX); j++) {
+    const int tx = sx * (int)(kSTW / kTX) + j;
+    if (tx * kTX < (int)p.nx && fs234_tile<S, C, M, ODD, TW>(p, tx, sy, tid, sm))
+      act |= activity(j * kTX + tid % kTX, tid / kTX, wact, hact);
+    __syncthreads();
+  }
+  act = __reduce_or_sync(0xffffffffu, act);
+  if ((tid & 31) == 0) wact_sm[tid >> 5] = act;
+  __syncthreads();
+  if (tid == 0) {
+    uint32_t m = 0;
+    for (int w = 0; w < TW * kTY / 32; w++) m |= wact_sm[w];
+    nz[t] = m;
+  }
+}
+
+}  // namespace flb

@@ -48,6 +48,14 @@ int launch_fs234(const KParams& kp, cudaStream_t st, uint32_t odd, const TileLis
 template <class S, class C, class M>
 int fs_blocks_per_sm(int which);  // 0: FS_1, 1: FS_2..4 on 128-wide tiles, 2: on 32-wide tiles
 
+// the free-surface step as one persistent cooperative kernel (k_fsp.cu):
+// a.steps steps per launch, `grid` CTAs of 1024 threads all resident at once
+template <class S, class C, class M>
+cudaError_t launch_fs_persist(const KParams& p0, const KParams& p1, const FspArgs& a, uint32_t grid, bool hw, bool fu,
+                              cudaStream_t st);
+template <class S, class C, class M>
+int fs_persist_blocks_per_sm(bool hw, bool fu);
+
 // headless visualisation (k_viz.cu), T = the arithmetic type of u / the mass type of phi
 template <class T>
 void launch_viz_uv(const void* u, float* out, uint32_t N, cudaStream_t st);

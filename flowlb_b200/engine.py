@@ -27,6 +27,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of memory", 4
 # Every symbol the header declares; tests check the library exports them all.
 EXPORTS = [
     "flb_case_desc_init", "flb_create", "flb_reset", "flb_destroy", "flb_step", "flb_sync", "flb_get_time",
+    "flb_set_step_mode", "flb_get_step_mode", "flb_set_wait_limit",
     "flb_set_stream", "flb_get_stream", "flb_field_info", "flb_read_field", "flb_write_field", "flb_total_mass",
     "flb_total_mass_noalloc", "flb_cell_counts", "flb_check_finite", "flb_run_pass", "flb_profile_steps", "flb_launch_count", "flb_save_checkpoint",
     "flb_load_checkpoint", "flb_last_error", "flb_status_string", "flb_version",
@@ -77,6 +78,7 @@ class SetupStruct(C.Structure):
 VTI_UINT8, VTI_FLOAT32, VTI_FLOAT64 = 0, 1, 2
 VIZ_UX, VIZ_UY, VIZ_MAGNITUDE, VIZ_PRESSURE = 0, 1, 2, 3
 BATCH_CLUSTER, BATCH_TEAM = 0, 1
+STEP_AUTO, STEP_KERNELS, STEP_PERSISTENT = 0, 1, 2
 
 
 class VtiField(C.Structure):
@@ -117,6 +119,9 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "flb_sync": (C.c_int, [H]),
         "flb_get_time": (C.c_int, [H, C.POINTER(C.c_uint64)]),
         "flb_set_stream": (C.c_int, [H, C.c_void_p]),
+        "flb_set_step_mode": (C.c_int, [H, C.c_int]),
+        "flb_get_step_mode": (C.c_int, [H, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+        "flb_set_wait_limit": (C.c_int, [H, C.c_uint32]),
         "flb_get_stream": (C.c_int, [H, C.POINTER(C.c_void_p)]),
         "flb_field_info": (C.c_int, [H, C.c_int, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
         "flb_read_field": (C.c_int, [H, C.c_int, C.c_void_p, C.c_int]),
@@ -289,6 +294,21 @@ class Solver:
         v = C.c_void_p()
         self._check(load_library().flb_get_stream(self._h, C.byref(v)))
         return int(v.value or 0)
+
+    def set_step_mode(self, mode: int):
+        """STEP_AUTO, STEP_KERNELS or STEP_PERSISTENT (flb_set_step_mode)."""
+        self._check(load_library().flb_set_step_mode(self._h, int(mode)))
+
+    @property
+    def persistent(self) -> bool:
+        """Whether graph-replayed free-surface steps run as one persistent kernel."""
+        m, p = C.c_int(), C.c_int()
+        self._check(load_library().flb_get_step_mode(self._h, C.byref(m), C.byref(p)))
+        return bool(p.value)
+
+    def set_wait_limit(self, polls: int):
+        """Grid-barrier polls of the persistent step before it gives up (0: default)."""
+        self._check(load_library().flb_set_wait_limit(self._h, int(polls)))
 
     def set_stream(self, stream: int | None):
         self._check(load_library().flb_set_stream(self._h, stream or None))

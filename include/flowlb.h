@@ -142,8 +142,33 @@ FLB_API flb_status flb_destroy(flb_handle h);
  * Replaces the loop bodies of runCuda.cu:473-490 and :506-527. */
 FLB_API flb_status flb_step(flb_handle h, uint64_t n);
 
+/* Waits for the handle's stream.  FLB_ERR_CUDA if a grid barrier of the
+ * persistent free-surface step gave up waiting (the state is then undefined
+ * and flb_step is refused until flb_reset). */
 FLB_API flb_status flb_sync(flb_handle h);
 FLB_API flb_status flb_get_time(flb_handle h, uint64_t* t);
+
+/* How the free-surface steps that flb_step replays from CUDA graphs run (no
+ * counterpart in the reference, whose host loop launches five kernels per
+ * step, runCuda.cu:506-527).  FLB_STEP_KERNELS: FS_1, stream-collide, the
+ * flag pass and the list build as four kernels per step.
+ * FLB_STEP_PERSISTENT: one cooperative kernel per graph (every CTA resident,
+ * one per SM) runs all its steps, the passes separated by grid barriers in
+ * global memory; a barrier wait gives up after a bounded number of polls
+ * (flb_set_wait_limit) and the next flb_sync or flb_read_field returns
+ * FLB_ERR_CUDA.  FLB_STEP_AUTO (default): persistent on grids of up to 4096
+ * 128x8 super-tiles, per-pass kernels above.  Both give identical results.
+ * The persistent form needs a free-surface case without inlet/outlet cells
+ * (FLB_ERR_UNSUPPORTED otherwise); single-phase cases ignore the mode.  With
+ * FLB_PERSIST_SKIP_ARRIVAL=1 in the environment (failure injection for
+ * tests) one CTA never arrives at the barriers, so every wait runs out. */
+enum { FLB_STEP_AUTO = 0, FLB_STEP_KERNELS = 1, FLB_STEP_PERSISTENT = 2 };
+FLB_API flb_status flb_set_step_mode(flb_handle h, int mode);
+/* mode as set; *persistent = 1 when graph-replayed steps run persistent */
+FLB_API flb_status flb_get_step_mode(flb_handle h, int* mode, int* persistent);
+/* Polls a CTA of the persistent step waits at a grid barrier before the
+ * launch gives up; 0 restores the default (2^22). */
+FLB_API flb_status flb_set_wait_limit(flb_handle h, uint32_t polls);
 FLB_API flb_status flb_set_stream(flb_handle h, void* stream);
 FLB_API flb_status flb_get_stream(flb_handle h, void** stream);
 
