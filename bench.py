@@ -23,8 +23,8 @@ Multi-GPU: the path does not shard (one GPU per case), so --gpus N runs N
 independent replicas, one per rank (weak scaling).
 
 --impl reference times the CPU restatement of the reference step (the oracle,
-OpenMP on the host cores, reference arithmetic) on a bounded sample of the
-same workload.
+OpenMP on all host cores, the reference's per-cell arithmetic) over the same
+window of lattice steps and in the same modes as the GPU arm.
 """
 from __future__ import annotations
 
@@ -53,6 +53,10 @@ KERNEL_OF_PASS = {"stream_collide": "k_sc_list (free-surface stream-collide)", "
 # (profiles/dam_break_2048x512_launch_list.md); ncu flushes the caches before
 # each launch, so these are cold-start figures for an L2-resident working set
 TRAFFIC_NCU: dict = {"fs234": 7339520, "stream_collide": 9786880, "fs1": 13902464}
+# the persistent step: one launch runs PERSIST_STEPS lattice steps of every pass
+KERNEL_PERSIST = "k_fs_persist (FS_1, stream-collide, FS_2..4 and list build, grid barriers)"
+PERSIST_STEPS = 32
+TRAFFIC_NCU_PERSIST = None
 
 
 def env_rank():
@@ -273,21 +277,60 @@ def run_ours(args, rank, local_rank, world):
     t_max = max_over_ranks(elapsed_ms, dist)
     value = world * N * S * args.steps / (t_max * 1e-3) / 1e6
 
-    # ---- dominant-kernel roofline: per-pass CUDA-event timing -------------
-    prof_steps = max(20, S // 4)
-    ca = solver.cell_counts()
-    passes = solver.profile_steps(prof_steps)
-    cb = solver.cell_counts()
-    counts_avg = {k: 0.5 * (ca[k] + cb[k]) for k in ca}
-    pbytes = algorithmic_bytes(counts_avg)
-    dom = max(passes, key=passes.get)
-    dom_ms = passes[dom] / prof_steps
+    # ---- dominant-kernel roofline ------------------------------------------
     peak, peak_kind = measured_peaks()
-    achieved = pbytes[dom] / (dom_ms * 1e-3) / 1e9
-    shares = {k: v / max(1e-12, sum(passes.values())) for k, v in passes.items()}
-    per_pass = {k: {"avg_launch_ms": round(passes[k] / prof_steps, 5),
-                    "achieved_gbs": round(pbytes[k] / (passes[k] / prof_steps * 1e-3) / 1e9, 1)} for k in passes}
+    prof_steps = max(32, S // 4)
+    step_ms = t_max / (args.steps * S)  # device time per lattice step of the timed region
+    if solver.persistent:
+        # one kernel runs every pass of the step (32 steps per launch): its
+        # launch time is the timed region's per-step time x 32, its bytes the
+        # passes' algorithmic bytes over the live-cell census; the phase
+        # shares come from the same kernel with a device-clock trace of its
+        # grid barriers (they sum to its step time, nothing is serialised)
+        ca = solver.cell_counts()
+        phases = solver.profile_phases(prof_steps)
+        cb = solver.cell_counts()
+        counts_avg = {k: 0.5 * (ca[k] + cb[k]) for k in ca}
+        pbytes = algorithmic_bytes(counts_avg)
+        launch_steps = PERSIST_STEPS
+        launch_bytes = sum(pbytes.values()) * launch_steps
+        dom_ms = step_ms * launch_steps
+        achieved = launch_bytes / (dom_ms * 1e-3) / 1e9
+        tot = max(1e-12, sum(phases.values()))
+        roofline = {"bound": "hbm", "kernel": KERNEL_PERSIST, "achieved": round(achieved, 1), "peak": peak,
+                    "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                    "traffic": TRAFFIC_NCU_PERSIST, "algorithmic_bytes_per_launch": int(launch_bytes),
+                    "lattice_steps_per_launch": launch_steps, "avg_launch_ms": round(dom_ms, 5),
+                    "phase_share": {k: round(v / tot, 3) for k, v in phases.items()},
+                    "phase_us_per_step": {k: round(v / prof_steps * 1e3, 2) for k, v in phases.items()},
+                    "bytes_per_step_by_pass": {k: int(v) for k, v in pbytes.items()}}
+    else:
+        # per-pass kernels: CUDA events around every pass (serialised: the
+        # launches of one step no longer overlap, so the shares are approximate)
+        ca = solver.cell_counts()
+        passes = solver.profile_steps(prof_steps)
+        cb = solver.cell_counts()
+        counts_avg = {k: 0.5 * (ca[k] + cb[k]) for k in ca}
+        pbytes = algorithmic_bytes(counts_avg)
+        dom = max(passes, key=passes.get)
+        dom_ms = passes[dom] / prof_steps
+        achieved = pbytes[dom] / (dom_ms * 1e-3) / 1e9
+        shares = {k: v / max(1e-12, sum(passes.values())) for k, v in passes.items()}
+        per_pass = {k: {"avg_launch_ms": round(passes[k] / prof_steps, 5),
+                        "achieved_gbs": round(pbytes[k] / (passes[k] / prof_steps * 1e-3) / 1e9, 1)}
+                    for k in passes}
+        roofline = {"bound": "hbm", "kernel": KERNEL_OF_PASS[dom], "achieved": round(achieved, 1), "peak": peak,
+                    "unit": "GB/s", "frac": round(achieved / peak, 4), "peak_source": peak_kind,
+                    "traffic": TRAFFIC_NCU.get(dom), "algorithmic_bytes_per_launch": int(pbytes[dom]),
+                    "avg_launch_ms": round(dom_ms, 5), "pass_share_serialised": {k: round(v, 3)
+                                                                                 for k, v in shares.items()},
+                    "passes": per_pass}
+    step_bytes = sum(pbytes.values())
+    roofline["whole_step"] = {"algorithmic_bytes": int(step_bytes), "us": round(step_ms * 1e3, 3),
+                              "achieved_gbs": round(step_bytes / (step_ms * 1e-3) / 1e9, 1),
+                              "frac": round(step_bytes / (step_ms * 1e-3) / 1e9 / peak, 4)}
 
+    persistent = solver.persistent
     # ---- end to end through the C ABI with host buffers -------------------
     host_flags = torch.from_numpy(np.ascontiguousarray(case.flags.ravel())).pin_memory()
     out_rho = torch.empty(N, dtype=torch.float32).pin_memory()
@@ -316,7 +359,7 @@ def run_ours(args, rank, local_rank, world):
     # ---- side measurements on rank 0 (FP16 storage, single-phase probe) ---
     extra = {}
     if rank == 0 and not args.no_extra:
-        extra = side_measurements(args, local_rank, E, cases, peak)
+        extra = side_measurements(args, local_rank, E, cases, peak, _gpu_uuid(torch, local_rank))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -332,6 +375,8 @@ def run_ours(args, rank, local_rank, world):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "nx": case.nx, "ny": case.ny, "cells": N,
                        "lattice_steps_per_step": S, "parallelism": f"replicas x{world}",
+                       "step_form": "persistent kernel" if persistent else "per-pass kernels",
+                       "timed_lattice_steps": [args.warmup * S, (args.warmup + args.steps) * S],
                        "l2": "working set ~70 MB < 126 MB L2: a 256 MB buffer is zeroed before every timed step "
                              "(outside the timed events)",
                        "cells_by_type_at_start": counts0, "cells_by_type_at_end": counts1,
@@ -339,12 +384,7 @@ def run_ours(args, rank, local_rank, world):
             "e2e": {"value": round(e2e_value, 1), "unit": "MLUPS", "h2d_bytes_per_step": int(N),
                     "d2h_bytes_per_step": int(N * (4 + 8 + 8 + 1))},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "hbm", "kernel": KERNEL_OF_PASS[dom],
-                         "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "peak_source": peak_kind,
-                         "traffic": TRAFFIC_NCU.get(dom), "algorithmic_bytes_per_launch": int(pbytes[dom]),
-                         "avg_launch_ms": round(dom_ms, 5), "pass_share": {k: round(v, 3) for k, v in shares.items()},
-                         "passes": per_pass},
+            "roofline": roofline,
             "clocks": clocks.summary(),
         }
         if cpu is not None:
@@ -365,27 +405,39 @@ def _timed(torch, solver, n):
     return a.elapsed_time(b)
 
 
-def side_measurements(args, device, E, cases, peak):
+def side_measurements(args, device, E, cases, peak, uuid):
+    """Each side measurement carries the SM clocks sampled while it ran."""
     import torch
 
     out = {}
+
+    def clocked(key, fn):
+        with ClockSampler(device, uuid) as clk:
+            r = fn()
+        if isinstance(r, dict):
+            r["clocks"] = clk.summary()
+        out[key] = r
+
     # plain single phase on 8192x2048 (working set ~1.2 GB): FP32 and FP16S
     p = cases.hbm_probe(8192, 2048)
-    for prec, key, bytes_per in ((32, "single_phase_fp32_8192x2048", 72.0),
-                                 (16, "single_phase_fp16s_8192x2048", 36.0)):
+
+    def single_phase(prec, bytes_per):
         s = E.Solver(p.flags, free_surface=False, precision=prec, tau=p.tau, fx=p.fx, bounce_back=E.BB_HALFWAY,
                      device=device)
         s.step(50)
         s.sync()
         n = 400
         ms = _timed(torch, s, n)
+        s.close()
         mlups = p.cells * n / (ms * 1e-3) / 1e6
         # bytes: the populations of every cell; flag and wall mask only where
         # the plain-fluid chunk map does not cover the cell (about 5 %)
         gbs = p.cells * bytes_per * n / (ms * 1e-3) / 1e9
-        out[key] = {"value": round(mlups, 1), "unit": "MLUPS", "achieved_gbs": round(gbs, 1),
-                    "frac_of_measured_hbm": round(gbs / peak, 4), "bytes_per_cell": bytes_per}
-        s.close()
+        return {"value": round(mlups, 1), "unit": "MLUPS", "achieved_gbs": round(gbs, 1),
+                "frac_of_measured_hbm": round(gbs / peak, 4), "bytes_per_cell": bytes_per}
+
+    clocked("single_phase_fp32_8192x2048", lambda: single_phase(32, 72.0))
+    clocked("single_phase_fp16s_8192x2048", lambda: single_phase(16, 36.0))
     out["fp16s_speedup_single_phase"] = round(out["single_phase_fp16s_8192x2048"]["value"] /
                                               out["single_phase_fp32_8192x2048"]["value"], 3)
     # FP16S accuracy: velocity L2 against FP64 on the 256x64 channel, 10,000 steps
@@ -403,59 +455,82 @@ def side_measurements(args, device, E, cases, peak):
     # the dam break at 8192x2048 (FP32 and FP16S)
     c = cases.dam_break(4)
     S = args.lattice_steps
-    for prec in (32, 16):
+
+    def dam_break_big(prec):
         s = E.Solver(c.flags, free_surface=True, precision=prec, mass_precision=64, tau=c.tau, fy=c.fy,
                      bounce_back=E.BB_HALFWAY, fs_mode=E.FS_CONSERVATIVE, device=device, u_max=U_MAX)
         s.step(S)
         s.sync()
         ms = _timed(torch, s, 2 * S)
-        out[f"dam_break_8192x2048_fp{prec if prec == 32 else '16s'}"] = {
-            "value": round(c.cells * 2 * S / (ms * 1e-3) / 1e6, 1), "unit": "MLUPS"}
+        form = "persistent kernel" if s.persistent else "per-pass kernels"
         s.close()
-    # batched ensemble: 512 cases in one launch per call vs a per-case loop
+        return {"value": round(c.cells * 2 * S / (ms * 1e-3) / 1e6, 1), "unit": "MLUPS", "step_form": form}
+
+    for prec in (32, 16):
+        clocked(f"dam_break_8192x2048_fp{prec if prec == 32 else '16s'}", lambda: dam_break_big(prec))
+    # storage-precision sweep of the 8192x2048 dam break (FP64 / FP32 / FP16S)
+    if args.sweep_steps > 0:
+        from flowlb_b200 import precision_sweep
+
+        clocked("precision_sweep_dam_break_8192x2048",
+                lambda: precision_sweep.run(4, args.sweep_steps, U_MAX, device))
+    # batched ensemble: 512 cases in one launch per call vs a per-case loop,
+    # both over the full step count
     ens = cases.ensemble()
     n_b = args.batch_steps
     spec = [(e.flags, e.tau, e.fx, 0.0) for e in ens]
     cells = sum(e.flags.size for e in ens)
-    b = E.Batch(spec, autotune=1, device=device)
-    b.step(2)
-    b.sync()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    b.step(n_b)
-    b.sync()
-    tb = time.perf_counter() - t0
-    info = b.info()
-    b.close()
-    sm = torch.cuda.Stream()
-    solvers = [E.Solver(e.flags, precision=32, tau=e.tau, fx=e.fx, stream=sm.cuda_stream, device=device)
-               for e in ens]
-    for s in solvers:
-        s.step(2)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for s in solvers:
-        s.step(n_b)
-    torch.cuda.synchronize()
-    tl = time.perf_counter() - t0
-    for s in solvers:
-        s.close()
-    scale = 5000.0 / n_b
-    out["batch_512_cases"] = {"cases_per_s": round(len(ens) / (tb * scale), 2), "unit": "cases/s (5000 steps)",
-                              "loop_cases_per_s": round(len(ens) / (tl * scale), 2),
-                              "speedup_vs_per_case_loop": round(tl / tb, 3), "glups": round(cells * n_b / tb / 1e9, 1),
-                              "steps_timed": n_b, "config": info}
+
+    def batch():
+        b = E.Batch(spec, autotune=1, device=device)
+        b.step(2)
+        b.sync()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        b.step(n_b)
+        b.sync()
+        tb = time.perf_counter() - t0
+        info = b.info()
+        b.close()
+        return {"cases_per_s": round(len(ens) / tb, 2), "unit": f"cases/s ({n_b} steps each)",
+                "glups": round(cells * n_b / tb / 1e9, 1), "steps_timed": n_b, "config": info, "wall_s": tb}
+
+    def loop():
+        sm = torch.cuda.Stream()
+        solvers = [E.Solver(e.flags, precision=32, tau=e.tau, fx=e.fx, stream=sm.cuda_stream, device=device)
+                   for e in ens]
+        for s in solvers:
+            s.step(2)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for s in solvers:
+            s.step(n_b)
+        torch.cuda.synchronize()
+        tl = time.perf_counter() - t0
+        for s in solvers:
+            s.close()
+        return {"cases_per_s": round(len(ens) / tl, 2), "wall_s": tl}
+
+    clocked("batch_512_cases", batch)
+    clocked("per_case_loop_512_cases", loop)
+    bt, lt = out["batch_512_cases"], out["per_case_loop_512_cases"]
+    bt["loop_cases_per_s"] = lt["cases_per_s"]
+    bt["speedup_vs_per_case_loop"] = round(lt["wall_s"] / bt["wall_s"], 3)
+
     # adjoint: backward (with checkpoint recomputation) over forward
-    pc = cases.porous_channel()
-    a = E.Adjoint(pc.flags, pc.porosity.astype(np.float64), tau=pc.tau, gx=pc.fx, precision=32, device=device)
-    a.forward()
-    a.backward()
-    a.forward()
-    a.backward()
-    f_ms, b_ms = a.timing()
-    a.close()
-    out["adjoint_1024x256_4096"] = {"forward_ms": round(f_ms, 2), "backward_ms": round(b_ms, 2),
-                                    "backward_over_forward": round(b_ms / f_ms, 3)}
+    def adjoint():
+        pc = cases.porous_channel()
+        a = E.Adjoint(pc.flags, pc.porosity.astype(np.float64), tau=pc.tau, gx=pc.fx, precision=32, device=device)
+        a.forward()
+        a.backward()
+        a.forward()
+        a.backward()
+        f_ms, b_ms = a.timing()
+        a.close()
+        return {"forward_ms": round(f_ms, 2), "backward_ms": round(b_ms, 2),
+                "backward_over_forward": round(b_ms / f_ms, 3)}
+
+    clocked("adjoint_1024x256_4096", adjoint)
     return out
 
 
@@ -479,7 +554,13 @@ def cpu_baseline(case, args):
 
 
 def run_reference(args, rank, world):
-    """CPU restatement of the reference step timed on the host cores."""
+    """The reference step restated on the CPU (the oracle, OpenMP on all host
+    cores), timed over the same window of lattice steps as the GPU arm:
+    W warm-up bench steps and K timed bench steps of S lattice steps each, on
+    the same case and in the same modes (half-way walls, conservative free
+    surface, limiter 0.25, FP32 populations + FP64 mass), with the reference's
+    per-cell expressions (reference arithmetic, as FlowLB's kernels evaluate
+    them, lbmKernel2D.cu:306-519).  Rank 0 alone runs and prints it."""
     if rank != 0:
         return
     from flowlb_b200 import cases
@@ -489,21 +570,25 @@ def run_reference(args, rank, world):
     threads = os.cpu_count() or 1
     o = O.Oracle(case.flags, O.OracleConfig(variant=O.F32, free_surface=True, bb=O.BB_HALFWAY,
                                             fs_mode=O.FS_CONSERVATIVE, tau=case.tau, fy=case.fy, threads=threads,
-                                            u_max=U_MAX))
-    S = args.ref_lattice_steps
+                                            u_max=U_MAX, arithmetic=O.ARITH_REFERENCE))
+    S = args.lattice_steps
     for _ in range(args.warmup):
         o.step(S)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         o.step(S)
     dt = time.perf_counter() - t0
+    o.close()
     value = case.cells * S * args.steps / dt / 1e6
-    sample = f"{case.nx}x{case.ny} dam break, {S} time steps per bench step"
+    sample = (f"{case.nx}x{case.ny} dam break, lattice steps {args.warmup * S}-{(args.warmup + args.steps) * S} "
+              f"timed in {args.steps} chunks of {S} (the GPU arm's window)")
     line = {"metric": METRIC, "value": round(value, 2), "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(dt * 1e3 / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
             "config": {"workload": WORKLOAD, "nx": case.nx, "ny": case.ny, "cells": case.cells,
-                       "lattice_steps_per_step": S, "parallelism": "host cores"},
+                       "lattice_steps_per_step": S, "parallelism": "host cores",
+                       "timed_lattice_steps": [args.warmup * S, (args.warmup + args.steps) * S],
+                       "arithmetic": "reference (FlowLB's per-cell expressions)"},
             "cpu_baseline": {"value": round(value, 2), "unit": "MLUPS", "cores": threads, "kind": "port",
                              "sample": sample},
             "e2e": {"value": round(value, 2), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -517,9 +602,10 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--lattice-steps", type=int, default=200, help="lattice time steps per bench step")
-    ap.add_argument("--ref-lattice-steps", type=int, default=40)
     ap.add_argument("--cpu-steps", type=int, default=2000)
-    ap.add_argument("--batch-steps", type=int, default=1000, help="steps of the batch measurement (scaled to 5000)")
+    ap.add_argument("--batch-steps", type=int, default=5000, help="steps of the batch and per-case-loop measurement")
+    ap.add_argument("--sweep-steps", type=int, default=50_000,
+                    help="steps of the 8192x2048 storage-precision sweep (0 skips it)")
     ap.add_argument("--step-mode", default="auto", choices=["auto", "kernels", "persistent"],
                     help="free-surface step form (flb_set_step_mode)")
     ap.add_argument("--no-extra", action="store_true")

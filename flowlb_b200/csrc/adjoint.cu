@@ -5,8 +5,8 @@
 // pull streaming with half-way walls; x periodic):
 //   f_i   = gathered f[i] from x - c_i (f[opp i] of the cell itself when that
 //           neighbour is a wall)
-//   rho   = sum f_i,  j = sum c_i f_i,  v = j / rho
-//   u     = (v + g/2) / (1 + s/2)                (Guo, F = rho (g - s u))
+//   rho   = sum f_i,  j = sum c_i f_i,  v = j (1 / rho)
+//   u     = (v + g/2) (1 / (1 + s/2))            (Guo, F = rho (g - s u))
 //   F     = rho (g - s u)
 //   feq_i = w_i rho (1 + 3 cu + 4.5 cu^2 - 1.5 u.u),    cu = c_i.u
 //   F_i   = w_i (3 (c_i.F - u.F) + 9 cu c_i.F)
@@ -95,18 +95,22 @@ __device__ __forceinline__ void gather(const AdjParams<T>& p, const T* __restric
   for (int i = 1; i < 9; i++) f[i] = ((sw >> (i - 1)) & 1u) ? fin[(uint32_t)opp(i) * N + idx] : fin[(uint32_t)i * N + nb.src[i]];
 }
 
-// Forward intermediates of one cell.
+// Forward intermediates of one cell.  The two divisions of the update are
+// taken once as reciprocals (ir = 1 / rho, id = 1 / d) and multiplied in, in
+// the forward and in the reverse step alike (an FP64 division is a long
+// instruction sequence; the reverse step would otherwise need ten).
 template <class T>
 struct Cell {
-  T rho, vx, vy, d, ux, uy, Fx, Fy, usq, uF;
+  T rho, ir, vx, vy, d, id, ux, uy, Fx, Fy, usq, uF;
 };
 
 // the rest of the intermediates from rho, v and s
 template <class T>
 __device__ __forceinline__ void cell_rest(const AdjParams<T>& p, Cell<T>& c, T s) {
   c.d = T(1) + T(0.5) * s;
-  c.ux = (c.vx + T(0.5) * p.gx) / c.d;
-  c.uy = (c.vy + T(0.5) * p.gy) / c.d;
+  c.id = T(1) / c.d;
+  c.ux = (c.vx + T(0.5) * p.gx) * c.id;
+  c.uy = (c.vy + T(0.5) * p.gy) * c.id;
   c.Fx = c.rho * (p.gx - s * c.ux);
   c.Fy = c.rho * (p.gy - s * c.uy);
   c.usq = c.ux * c.ux + c.uy * c.uy;
@@ -119,8 +123,9 @@ __device__ __forceinline__ Cell<T> cell_state(const AdjParams<T>& p, const T* f,
   c.rho = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
   const T jx = f[1] - f[2] + f[5] - f[6] + f[7] - f[8];
   const T jy = f[3] - f[4] + f[5] - f[6] - f[7] + f[8];
-  c.vx = jx / c.rho;
-  c.vy = jy / c.rho;
+  c.ir = T(1) / c.rho;
+  c.vx = jx * c.ir;
+  c.vy = jy * c.ir;
   cell_rest(p, c, s);
   return c;
 }
@@ -194,6 +199,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_por_bwd(const AdjParams<T> p, con
       const T s = p.s[idx];
       Cell<T> c;
       c.rho = mac[idx];
+      c.ir = T(1) / c.rho;
       c.vx = mac[N + idx];
       c.vy = mac[2 * N + idx];
       cell_rest(p, c, s);
@@ -258,14 +264,14 @@ __global__ void __launch_bounds__(kAdjBlock) k_por_bwd(const AdjParams<T> p, con
       uyb += -s * c.rho * Fyb;
       T sb = -c.rho * (Fxb * c.ux + Fyb * c.uy);
       T gxb = c.rho * Fxb, gyb = c.rho * Fyb;
-      // u = (v + g/2) / d
-      const T vxb = uxb / c.d, vyb = uyb / c.d;
-      sb += T(-0.5) * (uxb * c.ux + uyb * c.uy) / c.d;
-      gxb += T(0.5) * uxb / c.d;
-      gyb += T(0.5) * uyb / c.d;
-      // v = j / rho
-      const T jxb = vxb / c.rho, jyb = vyb / c.rho;
-      rhob += -(vxb * c.vx + vyb * c.vy) / c.rho;
+      // u = (v + g/2) id, id = 1 / d, d = 1 + s/2
+      const T vxb = uxb * c.id, vyb = uyb * c.id;
+      sb += T(-0.5) * (uxb * c.ux + uyb * c.uy) * c.id;
+      gxb += T(0.5) * uxb * c.id;
+      gyb += T(0.5) * uyb * c.id;
+      // v = j ir, ir = 1 / rho
+      const T jxb = vxb * c.ir, jyb = vyb * c.ir;
+      rhob += -(vxb * c.vx + vyb * c.vy) * c.ir;
       lam[idx] = fb[0] + rhob;
 #pragma unroll
       for (int i = 1; i < 9; i++) {

@@ -41,25 +41,52 @@ constexpr int kBatchMaxThreads = 1024;  // CTA sizes 256, 512 or 1024 (autotuned
 #ifndef FLB_BATCH_MIN_BLOCKS
 #define FLB_BATCH_MIN_BLOCKS 2  // two 1024-thread CTAs per SM: at most 32 registers
 #endif
+// the vector data path: CTAs of at most 512 threads, two per SM (64 registers)
+constexpr int kBatchVecMaxThreads = 512;
+constexpr uint32_t kVecCells = 4;  // cells per thread on the vector path
 
+// A case of the batch.  Its rows are stored kVecCells-aligned: row y starts at
+// cell y * sx, sx = nx rounded up to a multiple of 4, and the cells x >= nx of
+// a row are padding (flagged solid, never updated; their population slots are
+// scratch).  kp.N = sx * ny is the padded cell count (slot s at s * N).
 struct BatchCase {
   KParams kp;
-  uint32_t nsegx;  // 32-cell row segments
-  // set on the device for the launch shape: a warp's walk over the row
-  // segments advances dy rows and ds segments per item
-  uint32_t dy, ds;
+  uint32_t sx;  // row stride
+  // set on the device for the launch shape: row segments per row (32 cells,
+  // or 128 on the vector path), and a warp's walk over them advances dy rows
+  // and ds segments per item
+  uint32_t nseg, dy, ds;
 };
+
+// Neighbour cells of (x, y) in a case stored with row stride sx (periodic).
+__device__ __forceinline__ void neighbours_sx(uint32_t x, uint32_t y, uint32_t nx, uint32_t ny, uint32_t sx,
+                                              uint32_t* nb) {
+  const uint32_t yc = y * sx;
+  const uint32_t yu = (y + 1u == ny ? 0u : y + 1u) * sx;
+  const uint32_t yd = (y == 0u ? ny - 1u : y - 1u) * sx;
+  const uint32_t xr = x + 1u == nx ? 0u : x + 1u;
+  const uint32_t xl = x == 0u ? nx - 1u : x - 1u;
+  nb[0] = x + yc;
+  nb[1] = xr + yc;
+  nb[2] = xl + yc;
+  nb[3] = x + yu;
+  nb[4] = x + yd;
+  nb[5] = xr + yu;
+  nb[6] = xl + yd;
+  nb[7] = xr + yd;
+  nb[8] = xl + yu;
+}
 
 // sc_cell for a batch case (single phase, FP32): the same loads, collision
 // and stores, with slot s addressed as s*N cells past the case's first
 // population instead of through the slot pointer table, which here sits in
 // shared memory and would cost a 64-bit shared load per population.
 template <bool HW, bool FU, bool ODD, bool WM>
-__device__ __forceinline__ void batch_cell(const KParams& p, uint32_t x, uint32_t y) {
-  const uint32_t nx = p.nx, N = p.N, idx = x + y * nx;
+__device__ __forceinline__ void batch_cell(const KParams& p, uint32_t sx, uint32_t x, uint32_t y) {
+  const uint32_t N = p.N, idx = x + y * sx;
   float* __restrict__ F = static_cast<float*>(p.f);
   uint32_t nb[9];
-  neighbours(x, y, nx, p.ny, nb);
+  neighbours_sx(x, y, p.nx, p.ny, sx, nb);
   const uint8_t flag = p.flags[idx];
   const uint32_t nbm = HW ? (uint32_t)p.nbmask[idx] : 0u;
   // populations through L2 only: other CTAs wrote them last step, and no
@@ -78,8 +105,8 @@ __device__ __forceinline__ void batch_cell(const KParams& p, uint32_t x, uint32_
   // them live through the collision under the 32-register budget
   asm volatile("" ::: "memory");
   float* G = static_cast<float*>(p.f);
-  const uint32_t M = p.N, nxs = p.nx, ids = x + y * nxs;
-  neighbours(x, y, nxs, p.ny, nb);
+  const uint32_t M = p.N, ids = x + y * sx;
+  neighbours_sx(x, y, p.nx, p.ny, sx, nb);
   G[ids] = f[0];
 #pragma unroll
   for (int i = 1; i < 9; i += 2) {
@@ -88,19 +115,177 @@ __device__ __forceinline__ void batch_cell(const KParams& p, uint32_t x, uint32_
   }
 }
 
-// One step of one case: the warps of the cluster take 32-cell row segments,
-// warp k the segments k, k + nw, k + 2 nw, ... (nw warps in the cluster); a
-// warp starts at row y, segment s.  The case (in shared memory) is re-read per
-// item rather than held in registers.
+// The vector data path: kVecCells consecutive cells per thread (x0 .. x0+3 of
+// row y; x0 a multiple of 4), each population slot moved with one 16-byte
+// access (the padded row stride keeps them aligned), the slots of the x+1
+// neighbours shifted between lanes by shuffles, as the single-case vector
+// kernel (k_sc_vec) does.  The 32 lanes of a warp cover a 128-cell row
+// segment.  The group holding the row's last cell (x = nx - 1) takes that
+// cell's x+1 neighbour from x = 0 (periodic) and writes its outgoing
+// population there; padding cells are never updated.  Same loads, collision
+// and stores per cell as batch_cell, so the results are the same bit for bit.
 template <bool HW, bool FU, bool ODD, bool WM>
+__device__ __forceinline__ void batch_vec(const KParams& p, uint32_t sx, uint32_t x0, uint32_t y, uint32_t lane) {
+  constexpr int V = (int)kVecCells;
+  const uint32_t nx = p.nx, ny = p.ny, N = p.N;
+  float* F = static_cast<float*>(p.f);
+  const bool inrow = x0 < nx;
+  const uint32_t row = y * sx;
+  const uint32_t rowu = (y + 1u == ny ? 0u : y + 1u) * sx;
+  const uint32_t rowd = (y == 0u ? ny - 1u : y - 1u) * sx;
+  const bool last = inrow && x0 + (uint32_t)V >= nx;       // the group holding the row's last cell
+  const uint32_t kl = last ? nx - 1u - x0 : (uint32_t)V - 1u;  // that cell's position in the group
+  const bool tail = inrow && (lane == 31u || last);        // its x+1 neighbour is not in the next lane
+  const uint32_t xn = last ? 0u : x0 + (uint32_t)V;         // where that neighbour is
+  uint8_t fl[V] = {kWall, kWall, kWall, kWall};
+  uint8_t nbmv[V] = {0, 0, 0, 0};
+  float raw0[V], own[4][V], nbr[4][V], tmp[4][V];
+  if (inrow) {
+    const uchar4 fv = *reinterpret_cast<const uchar4*>(p.flags + row + x0);
+    fl[0] = fv.x; fl[1] = fv.y; fl[2] = fv.z; fl[3] = fv.w;
+    if (HW) {
+      const uchar4 mv = *reinterpret_cast<const uchar4*>(p.nbmask + row + x0);
+      nbmv[0] = mv.x; nbmv[1] = mv.y; nbmv[2] = mv.z; nbmv[3] = mv.w;
+    }
+    // populations through L2 only (other CTAs wrote them last step)
+    const float4 r0 = __ldcg(reinterpret_cast<const float4*>(F + row + x0));
+    raw0[0] = r0.x; raw0[1] = r0.y; raw0[2] = r0.z; raw0[3] = r0.w;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int i = 2 * q + 1;
+      const uint32_t r = (i == 1) ? row : (i == 7 ? rowd : rowu);
+      const float4 a = __ldcg(reinterpret_cast<const float4*>(F + (uint32_t)slot_a<ODD>(i) * N + row + x0));
+      const float4 b = __ldcg(reinterpret_cast<const float4*>(F + (uint32_t)slot_b<ODD>(i) * N + r + x0));
+      own[q][0] = a.x; own[q][1] = a.y; own[q][2] = a.z; own[q][3] = a.w;
+      tmp[q][0] = b.x; tmp[q][1] = b.y; tmp[q][2] = b.z; tmp[q][3] = b.w;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < V; k++) {
+      raw0[k] = 0.0f;
+#pragma unroll
+      for (int q = 0; q < 4; q++) own[q][k] = tmp[q][k] = 0.0f;
+    }
+  }
+  bool act[V];
+  bool any = false;
+#pragma unroll
+  for (int k = 0; k < V; k++) {
+    act[k] = !(fl[k] & (kGas | kWall));
+    any |= act[k];
+  }
+  // a warp with no cell to update leaves memory untouched
+  if (!__any_sync(0xffffffffu, any)) return;
+  // realign the x+1 slots (direction 3, +y, has no x shift)
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int i = 2 * q + 1;
+    if (i == 3) {
+#pragma unroll
+      for (int k = 0; k < V; k++) nbr[q][k] = tmp[q][k];
+    } else {
+      const uint32_t r = (i == 1) ? row : (i == 7 ? rowd : rowu);
+      const float from_next = __shfl_down_sync(0xffffffffu, tmp[q][0], 1);
+#pragma unroll
+      for (int k = 0; k < V - 1; k++) nbr[q][k] = tmp[q][k + 1];
+      nbr[q][V - 1] = from_next;
+      if (tail) {
+        const float w = __ldcg(F + (uint32_t)slot_b<ODD>(i) * N + r + xn);
+#pragma unroll
+        for (int k = 0; k < V; k++)
+          if ((uint32_t)k == kl) nbr[q][k] = w;
+      }
+    }
+  }
+  // per-cell collision; cells not updated keep their loaded values
+#pragma unroll
+  for (int k = 0; k < V; k++) {
+    if (!act[k]) continue;
+    const uint32_t x = x0 + (uint32_t)k, idx = row + x;
+    float f[9];
+    f[0] = raw0[k];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      f[2 * q + 1] = own[q][k];
+      f[2 * q + 2] = nbr[q][k];
+    }
+    const uint32_t nbm = nbmv[k];
+    if (HW && nbm) {
+      // half-way walls: reflected populations, scalar (wall-adjacent cells only)
+      uint32_t nb[9];
+      neighbours_sx(x, y, nx, ny, sx, nb);
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int i = 2 * q + 1;
+        if ((nbm >> i) & 1u) f[i] = __ldcg(F + (uint32_t)slot_b<ODD>(i) * N + idx);
+        if ((nbm >> (i - 1)) & 1u) f[i + 1] = __ldcg(F + (uint32_t)slot_a<ODD>(i) * N + nb[i]);
+      }
+    }
+    collide_cell<float, double, false, WM, FU>(p, idx, x, y, fl[k], nbm, f);
+    raw0[k] = f[0];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      nbr[q][k] = f[2 * q + 1];  // post f_i -> the x+1 (or +y) neighbour's slot b
+      own[q][k] = f[2 * q + 2];  // post f_{i+1} -> own slot a
+    }
+  }
+  // stores
+  if (inrow) {
+    *reinterpret_cast<float4*>(F + row + x0) = make_float4(raw0[0], raw0[1], raw0[2], raw0[3]);
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const int i = 2 * q + 1;
+      *reinterpret_cast<float4*>(F + (uint32_t)slot_a<ODD>(i) * N + row + x0) =
+          make_float4(own[q][0], own[q][1], own[q][2], own[q][3]);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int i = 2 * q + 1;
+    const uint32_t r = (i == 1) ? row : (i == 7 ? rowd : rowu);
+    float* dst = F + (uint32_t)slot_b<ODD>(i) * N + r;
+    if (i == 3) {
+      if (inrow) *reinterpret_cast<float4*>(dst + x0) = make_float4(nbr[q][0], nbr[q][1], nbr[q][2], nbr[q][3]);
+    } else {
+      const float from_prev = __shfl_up_sync(0xffffffffu, nbr[q][V - 1], 1);
+      if (inrow) {
+        // position x0 belongs to the previous lane's last cell (or, for lane 0,
+        // to the previous segment, which writes it itself)
+        if (lane != 0u) {
+          *reinterpret_cast<float4*>(dst + x0) = make_float4(from_prev, nbr[q][0], nbr[q][1], nbr[q][2]);
+        } else {
+#pragma unroll
+          for (int k = 0; k < V - 1; k++) dst[x0 + 1 + k] = nbr[q][k];
+        }
+        if (tail) {
+          float w = nbr[q][V - 1];
+#pragma unroll
+          for (int k = 0; k < V; k++)
+            if ((uint32_t)k == kl) w = nbr[q][k];
+          dst[xn] = w;
+        }
+      }
+    }
+  }
+}
+
+// One step of one case: the warps of the group take row segments (32 cells;
+// 128 on the vector path), warp k the segments k, k + nw, k + 2 nw, ... (nw
+// warps in the group); a warp starts at row y, segment s.  The case (in
+// shared memory) is re-read per item rather than held in registers.
+template <bool HW, bool FU, bool ODD, bool WM, bool VEC>
 __device__ __noinline__ void batch_step(const BatchCase& c, uint32_t y, uint32_t s, uint32_t lane) {
   while (y < c.kp.ny) {
-    const uint32_t x = s * 32u + lane;
-    if (x < c.kp.nx) batch_cell<HW, FU, ODD, WM>(c.kp, x, y);
+    if constexpr (VEC) {
+      batch_vec<HW, FU, ODD, WM>(c.kp, c.sx, s * (32u * kVecCells) + lane * kVecCells, y, lane);
+    } else {
+      const uint32_t x = s * 32u + lane;
+      if (x < c.kp.nx) batch_cell<HW, FU, ODD, WM>(c.kp, c.sx, x, y);
+    }
     s += c.ds;
     y += c.dy;
-    if (s >= c.nsegx) {
-      s -= c.nsegx;
+    if (s >= c.nseg) {
+      s -= c.nseg;
       y++;
     }
   }
@@ -167,8 +352,10 @@ __device__ __forceinline__ bool team_sync(TeamSync* ts, uint32_t n, uint32_t& ge
 // by wait_limit polls).  skip_rank: in team mode, the CTA of each team with
 // this rank never arrives at its team's barriers (failure injection; kNoSkip
 // in normal operation); unused in cluster mode.
-template <bool HW, bool FU, bool TEAM>
-__global__ void __launch_bounds__(kBatchMaxThreads, FLB_BATCH_MIN_BLOCKS)
+// VEC: the vector data path (kVecCells cells per thread, at most
+// kBatchVecMaxThreads threads per CTA).
+template <bool HW, bool FU, bool TEAM, bool VEC>
+__global__ void __launch_bounds__(VEC ? kBatchVecMaxThreads : kBatchMaxThreads, FLB_BATCH_MIN_BLOCKS)
     k_batch(const BatchCase* __restrict__ cases, const uint32_t* __restrict__ order, const uint32_t* __restrict__ start,
             const uint32_t* __restrict__ tdev, uint32_t steps, int wm_last, uint32_t group, TeamSync* sync,
             uint32_t* err, uint32_t wait_limit, uint32_t skip_rank) {
@@ -187,24 +374,26 @@ __global__ void __launch_bounds__(kBatchMaxThreads, FLB_BATCH_MIN_BLOCKS)
     {
       const uint32_t* src = reinterpret_cast<const uint32_t*>(&cases[order[k]]);
       uint32_t* dst = reinterpret_cast<uint32_t*>(&sc);
-      for (uint32_t i = threadIdx.x; i < offsetof(BatchCase, dy) / 4; i += blockDim.x) dst[i] = src[i];
+      for (uint32_t i = threadIdx.x; i < offsetof(BatchCase, nseg) / 4; i += blockDim.x) dst[i] = src[i];
       if (threadIdx.x == 0) {
-        const uint32_t n = cases[order[k]].nsegx;
+        const uint32_t seg = VEC ? 32u * kVecCells : 32u;
+        const uint32_t n = (cases[order[k]].kp.nx + seg - 1u) / seg;
+        sc.nseg = n;
         sc.dy = nw / n;
         sc.ds = nw % n;
       }
     }
     __syncthreads();
-    const uint32_t nsegx = sc.nsegx, y0 = wid / nsegx, s0 = wid % nsegx;
+    const uint32_t nsegx = sc.nseg, y0 = wid / nsegx, s0 = wid % nsegx;
     for (uint32_t s = 0; s < steps; s++) {
       const bool odd = ((t0 + s) & 1u) != 0;
       const bool wm = wm_last && s + 1 == steps;
       if (odd) {
-        if (wm) batch_step<HW, FU, true, true>(sc, y0, s0, lane);
-        else batch_step<HW, FU, true, false>(sc, y0, s0, lane);
+        if (wm) batch_step<HW, FU, true, true, VEC>(sc, y0, s0, lane);
+        else batch_step<HW, FU, true, false, VEC>(sc, y0, s0, lane);
       } else {
-        if (wm) batch_step<HW, FU, false, true>(sc, y0, s0, lane);
-        else batch_step<HW, FU, false, false>(sc, y0, s0, lane);
+        if (wm) batch_step<HW, FU, false, true, VEC>(sc, y0, s0, lane);
+        else batch_step<HW, FU, false, false, VEC>(sc, y0, s0, lane);
       }
       if constexpr (TEAM) {
         if (!team_sync(&sync[cid], group, gen, err, ok, wait_limit, rank != skip_rank)) return;
@@ -221,13 +410,17 @@ __global__ void k_tadd(uint32_t* t, uint32_t n) { *t += n; }
 using BatchKernel = void (*)(const BatchCase*, const uint32_t*, const uint32_t*, const uint32_t*, uint32_t, int,
                              uint32_t, TeamSync*, uint32_t*, uint32_t, uint32_t);
 
-BatchKernel pick_kernel(bool hw, bool fu, bool team) {
+template <bool VEC>
+BatchKernel pick_kernel_v(bool hw, bool fu, bool team) {
   if (team) {
-    if (hw) return fu ? k_batch<true, true, true> : k_batch<true, false, true>;
-    return fu ? k_batch<false, true, true> : k_batch<false, false, true>;
+    if (hw) return fu ? k_batch<true, true, true, VEC> : k_batch<true, false, true, VEC>;
+    return fu ? k_batch<false, true, true, VEC> : k_batch<false, false, true, VEC>;
   }
-  if (hw) return fu ? k_batch<true, true, false> : k_batch<true, false, false>;
-  return fu ? k_batch<false, true, false> : k_batch<false, false, false>;
+  if (hw) return fu ? k_batch<true, true, false, VEC> : k_batch<true, false, false, VEC>;
+  return fu ? k_batch<false, true, false, VEC> : k_batch<false, false, false, VEC>;
+}
+BatchKernel pick_kernel(bool hw, bool fu, bool team, bool vec) {
+  return vec ? pick_kernel_v<true>(hw, fu, team) : pick_kernel_v<false>(hw, fu, team);
 }
 
 }  // namespace
@@ -243,8 +436,13 @@ struct flb_batch_s {
   bool hw = false, fu = false;
   uint64_t t = 0;
   std::vector<uint32_t> nx, ny;
-  std::vector<size_t> off;  // first cell of each case in the concatenated cell arrays
-  size_t cells = 0;
+  std::vector<size_t> off;   // first cell of each case in the concatenated geometry (nx * ny cells each)
+  std::vector<size_t> poff;  // first cell of each case in the padded state arrays (sx * ny cells each)
+  std::vector<uint32_t> sx;  // padded row stride of each case (nx rounded up to a multiple of 4)
+  size_t cells = 0, pcells = 0, max_cells = 0;
+  // initialisation scratch for one case in the compact layout
+  float *d_sf = nullptr, *d_srho = nullptr, *d_su = nullptr;
+  uint8_t *d_sflags = nullptr, *d_snb = nullptr;
   float* d_f = nullptr;
   float* d_rho = nullptr;
   float* d_u = nullptr;
@@ -266,13 +464,14 @@ struct flb_batch_s {
   // threads, each group a thread-block cluster or (team) a team
   int cluster = 8, clusters = 0, threads = 512, tuned = 0;
   bool team = false;
+  bool vec = false;  // the vector data path (kVecCells cells per thread)
   uint64_t launches = 0;
   // the step graph (batch kernel + counter update) for one step count
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t gexec = nullptr;
   uint32_t g_steps = 0, g_limit = 0, g_skip = 0;
   int g_wm = -1, g_cluster = 0, g_clusters = 0, g_threads = 0;
-  bool g_team = false;
+  bool g_team = false, g_vec = false;
   std::string err;
 };
 
@@ -315,21 +514,52 @@ void bdrop_graph(flb_batch b) {
 
 void bfree(flb_batch b) {
   bdrop_graph(b);
-  void* bufs[] = {b->d_f,     b->d_rho,   b->d_u,     b->d_flags, b->d_geo, b->d_nbmask,
+  void* bufs[] = {b->d_sf,    b->d_srho,  b->d_su,    b->d_sflags, b->d_snb,
+                  b->d_f,     b->d_rho,   b->d_u,     b->d_flags, b->d_geo, b->d_nbmask,
                   b->d_tstep, b->d_cases, b->d_order, b->d_start, b->d_sync, b->d_err};
   for (void* p : bufs)
     if (p) cudaFree(p);
   if (b->own_stream && b->stream) cudaStreamDestroy(b->stream);
 }
 
-// Initial state of every case (the single-case initialisation, per case).
+// Copies `rows` rows of `width` bytes between the compact layout (pitch =
+// width) and a padded one (pitch = stride bytes).
+cudaError_t copy_rows(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, size_t rows,
+                      cudaMemcpyKind kind, cudaStream_t st) {
+  return cudaMemcpy2DAsync(dst, dpitch, src, spitch, width, rows, kind, st);
+}
+
+// Initial state of every case: the single-case initialisation in the compact
+// layout (scratch), copied row by row into the padded state; padding cells
+// are solid, with zero populations and no wall neighbours.
 flb_status binit(flb_batch b) {
   BDevice g(b->device);
+  const size_t P = b->pcells;
+  FLB_BCUDA(b, cudaMemsetAsync(b->d_f, 0, 9 * P * sizeof(float), b->stream));
+  FLB_BCUDA(b, cudaMemsetAsync(b->d_rho, 0, P * sizeof(float), b->stream));
+  FLB_BCUDA(b, cudaMemsetAsync(b->d_u, 0, 2 * P * sizeof(float), b->stream));
+  FLB_BCUDA(b, cudaMemsetAsync(b->d_flags, kWall, P, b->stream));
+  if (b->hw) FLB_BCUDA(b, cudaMemsetAsync(b->d_nbmask, 0, P, b->stream));
   for (uint32_t c = 0; c < b->n; c++) {
-    const size_t o = b->off[c];
-    launch_init_flags(b->d_geo + o, b->d_flags + o, b->nx[c], b->ny[c], 0, nullptr, nullptr, nullptr, 1, b->stream);
-    if (b->hw) launch_nbmask(b->d_geo + o, b->d_nbmask + o, b->nx[c], b->ny[c], b->stream);
-    launch_init_ddf<float, float, double>(b->hcases[c].kp, b->stream, b->d_geo + o, b->hw);
+    const size_t o = b->off[c], po = b->poff[c];
+    const uint32_t nx = b->nx[c], ny = b->ny[c], sx = b->sx[c];
+    const size_t N = (size_t)nx * ny;
+    KParams kp = b->hcases[c].kp;  // constants of the case, compact scratch pointers
+    kp.N = (uint32_t)N;
+    kp.f = b->d_sf;
+    for (int q = 0; q < 9; q++) kp.slot[q] = b->d_sf + (size_t)q * N;
+    kp.rho = b->d_srho;
+    kp.u = b->d_su;
+    FLB_BCUDA(b, cudaMemsetAsync(b->d_sf, 0, 9 * N * sizeof(float), b->stream));
+    launch_init_flags(b->d_geo + o, b->d_sflags, nx, ny, 0, nullptr, nullptr, nullptr, 1, b->stream);
+    if (b->hw) launch_nbmask(b->d_geo + o, b->d_snb, nx, ny, b->stream);
+    launch_init_ddf<float, float, double>(kp, b->stream, b->d_geo + o, b->hw);
+    const cudaMemcpyKind dd = cudaMemcpyDeviceToDevice;
+    FLB_BCUDA(b, copy_rows(b->d_f + 9 * po, sx * 4, b->d_sf, nx * 4, nx * 4, 9 * (size_t)ny, dd, b->stream));
+    FLB_BCUDA(b, copy_rows(b->d_rho + po, sx * 4, b->d_srho, nx * 4, nx * 4, ny, dd, b->stream));
+    FLB_BCUDA(b, copy_rows(b->d_u + 2 * po, sx * 4, b->d_su, nx * 4, nx * 4, 2 * (size_t)ny, dd, b->stream));
+    FLB_BCUDA(b, copy_rows(b->d_flags + po, sx, b->d_sflags, nx, nx, ny, dd, b->stream));
+    if (b->hw) FLB_BCUDA(b, copy_rows(b->d_nbmask + po, sx, b->d_snb, nx, nx, ny, dd, b->stream));
   }
   FLB_BCUDA(b, cudaMemsetAsync(b->d_tstep, 0, 2 * sizeof(uint32_t), b->stream));
   FLB_BCUDA(b, cudaMemsetAsync(b->d_sync, 0, b->n * sizeof(TeamSync), b->stream));
@@ -390,7 +620,7 @@ uint32_t skip_rank_for(flb_batch b) {
 
 // One launch of the batch kernel for n steps on the stream (captured or not).
 flb_status bissue(flb_batch b, uint32_t n, int wm_last, uint32_t skip) {
-  BatchKernel kern = pick_kernel(b->hw, b->fu, b->team);
+  BatchKernel kern = pick_kernel(b->hw, b->fu, b->team, b->vec);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)(b->clusters * b->cluster));
   cfg.blockDim = dim3((unsigned)b->threads);
@@ -425,7 +655,7 @@ flb_status blaunch(flb_batch b, uint64_t steps, int wm_last) {
     const uint32_t n = (uint32_t)std::min<uint64_t>(steps - done, 1u << 31);
     const int wm = wm_last && done + n == steps;
     if (!b->gexec || b->g_steps != n || b->g_wm != wm || b->g_cluster != b->cluster ||
-        b->g_clusters != b->clusters || b->g_threads != b->threads || b->g_team != b->team ||
+        b->g_clusters != b->clusters || b->g_threads != b->threads || b->g_team != b->team || b->g_vec != b->vec ||
         b->g_limit != b->wait_limit || b->g_skip != skip) {
       bdrop_graph(b);
       FLB_BCUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
@@ -445,6 +675,7 @@ flb_status blaunch(flb_batch b, uint64_t steps, int wm_last) {
       b->g_clusters = b->clusters;
       b->g_threads = b->threads;
       b->g_team = b->team;
+      b->g_vec = b->vec;
       b->g_limit = b->wait_limit;
       b->g_skip = skip;
     }
@@ -457,8 +688,9 @@ flb_status blaunch(flb_batch b, uint64_t steps, int wm_last) {
 }
 
 // Resident clusters of the given size (0 when the size cannot launch).
-int max_clusters(flb_batch b, int cs, int threads) {
-  BatchKernel kern = pick_kernel(b->hw, b->fu, false);
+int max_clusters(flb_batch b, int cs, int threads, bool vec) {
+  if (vec && threads > kBatchVecMaxThreads) return 0;
+  BatchKernel kern = pick_kernel(b->hw, b->fu, false, vec);
   if (cs > 8) cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3((unsigned)cs);
@@ -479,10 +711,11 @@ int max_clusters(flb_batch b, int cs, int threads) {
 }
 
 // CTAs of the team kernel resident on the device at once (0 on failure).
-int max_team_ctas(flb_batch b, int threads) {
+int max_team_ctas(flb_batch b, int threads, bool vec) {
+  if (vec && threads > kBatchVecMaxThreads) return 0;
   int nsm = 0, per_sm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick_kernel(b->hw, b->fu, true), threads, 0) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pick_kernel(b->hw, b->fu, true, vec), threads, 0) !=
       cudaSuccess) {
     cudaGetLastError();
     return 0;
@@ -491,8 +724,8 @@ int max_team_ctas(flb_batch b, int threads) {
 }
 
 // Groups of `group` CTAs that fit on the device at once for the mode.
-int max_groups(flb_batch b, bool team, int group, int threads) {
-  return team ? max_team_ctas(b, threads) / group : max_clusters(b, group, threads);
+int max_groups(flb_batch b, bool team, int group, int threads, bool vec) {
+  return team ? max_team_ctas(b, threads, vec) / group : max_clusters(b, group, threads, vec);
 }
 
 // Reads and clears the team barriers' error flag: FLB_ERR_CUDA when a wait
@@ -528,31 +761,42 @@ flb_status btune(flb_batch b, uint32_t probe_steps) {
   const double case_bytes = (double)b->cells / b->n * (9.0 * 4.0 + 2.0);
   const int l2_fit = std::max(1, (int)(0.5 * (double)l2 / std::max(1.0, case_bytes)));
   struct Cand {
-    bool team;
+    bool team, vec;
     int cs, clusters, threads;
   };
   std::vector<Cand> cands;
-  auto add = [&](bool team, int cs, int k, int mx, int threads) {
+  auto add = [&](bool team, bool vec, int cs, int k, int mx, int threads) {
     const int cl = std::min(std::max(k, 1), std::min(mx, (int)b->n));
     for (auto& c : cands)
-      if (c.team == team && c.cs == cs && c.clusters == cl && c.threads == threads) return;
-    cands.push_back({team, cs, cl, threads});
+      if (c.team == team && c.vec == vec && c.cs == cs && c.clusters == cl && c.threads == threads) return;
+    cands.push_back({team, vec, cs, cl, threads});
   };
-  for (int threads : {512, 1024}) {
-    for (int cs : {1, 4, 8, 16}) {
-      const int mx = max_clusters(b, cs, threads);
-      if (mx <= 0) continue;
-      const int per_sm = std::max(1, nsm / cs);
-      for (int k : {l2_fit, per_sm, mx}) add(false, cs, k, mx, threads);
-    }
-    // teams: every resident CTA, split into l2_fit/2 .. 2 l2_fit teams (on a
-    // B200 the ensemble runs fastest with its active cases near l2_fit)
-    const int R = max_team_ctas(b, threads);
+  // teams: every resident CTA, split into l2_fit/2 .. 2 l2_fit teams (on a
+  // B200 the ensemble runs fastest with its active cases near l2_fit)
+  auto add_teams = [&](bool vec, int threads) {
+    const int R = max_team_ctas(b, threads, vec);
     for (int teams : {l2_fit / 2, (3 * l2_fit) / 4, l2_fit, (5 * l2_fit) / 4, (3 * l2_fit) / 2, 2 * l2_fit}) {
       teams = std::min(std::max(teams, 1), std::min(R, (int)b->n));
       if (R <= 0 || teams <= 0) continue;
-      add(true, R / teams, teams, teams, threads);
+      add(true, vec, R / teams, teams, teams, threads);
     }
+  };
+  for (int threads : {512, 1024}) {
+    for (int cs : {1, 4, 8, 16}) {
+      const int mx = max_clusters(b, cs, threads, false);
+      if (mx <= 0) continue;
+      const int per_sm = std::max(1, nsm / cs);
+      for (int k : {l2_fit, per_sm, mx}) add(false, false, cs, k, mx, threads);
+    }
+    add_teams(false, threads);
+  }
+  // the vector data path: teams, and 8- and 16-CTA clusters at the L2-sized count
+  for (int threads : {256, 512}) {
+    for (int cs : {8, 16}) {
+      const int mx = max_clusters(b, cs, threads, true);
+      if (mx > 0) add(false, true, cs, l2_fit, mx, threads);
+    }
+    add_teams(true, threads);
   }
   if (cands.empty()) return bfail(b, FLB_ERR_UNSUPPORTED, "no launch shape can run the batch");
   cudaEvent_t e0, e1;
@@ -563,6 +807,7 @@ flb_status btune(flb_batch b, uint32_t probe_steps) {
   flb_status s = FLB_OK;
   for (const Cand& c : cands) {
     b->team = c.team;
+    b->vec = c.vec;
     b->cluster = c.cs;
     b->threads = c.threads;
     s = bassign(b, c.clusters);
@@ -596,6 +841,7 @@ flb_status btune(flb_batch b, uint32_t probe_steps) {
   FLB_BCUDA(b, cudaGetLastError());
   if (best == 1e30f) return bfail(b, FLB_ERR_CUDA, "no launch shape completed the probe steps");
   b->team = win.team;
+  b->vec = win.vec;
   b->cluster = win.cs;
   b->threads = win.threads;
   s = bassign(b, win.clusters);
@@ -650,11 +896,17 @@ FLB_API flb_status flb_batch_create(const flb_case_desc* cases, uint32_t n, int 
   b->nx.resize(n);
   b->ny.resize(n);
   b->off.resize(n);
+  b->poff.resize(n);
+  b->sx.resize(n);
   for (uint32_t c = 0; c < n; c++) {
     b->nx[c] = cases[c].nx;
     b->ny[c] = cases[c].ny;
+    b->sx[c] = (cases[c].nx + kVecCells - 1u) / kVecCells * kVecCells;
     b->off[c] = b->cells;
+    b->poff[c] = b->pcells;
     b->cells += (size_t)cases[c].nx * cases[c].ny;
+    b->pcells += (size_t)b->sx[c] * cases[c].ny;
+    b->max_cells = std::max(b->max_cells, (size_t)cases[c].nx * cases[c].ny);
   }
   auto bail = [&](flb_status s) {
     std::fprintf(stderr, "flb_batch_create: %s\n", b->err.c_str());
@@ -669,15 +921,18 @@ FLB_API flb_status flb_batch_create(const flb_case_desc* cases, uint32_t n, int 
     if (e != cudaSuccess) return bail(bcuda(b, e, "cudaStreamCreate"));
     b->own_stream = true;
   }
-  const size_t M = b->cells;
+  const size_t M = b->cells, P = b->pcells, S = b->max_cells;
   struct A {
     void** p;
     size_t bytes;
     bool need;
   } allocs[] = {
-      {(void**)&b->d_f, 9 * M * sizeof(float), true},         {(void**)&b->d_rho, M * sizeof(float), true},
-      {(void**)&b->d_u, 2 * M * sizeof(float), true},         {(void**)&b->d_flags, M, true},
-      {(void**)&b->d_geo, M, true},                           {(void**)&b->d_nbmask, M, b->hw},
+      {(void**)&b->d_f, 9 * P * sizeof(float), true},         {(void**)&b->d_rho, P * sizeof(float), true},
+      {(void**)&b->d_u, 2 * P * sizeof(float), true},         {(void**)&b->d_flags, P, true},
+      {(void**)&b->d_geo, M, true},                           {(void**)&b->d_nbmask, P, b->hw},
+      {(void**)&b->d_sf, 9 * S * sizeof(float), true},        {(void**)&b->d_srho, S * sizeof(float), true},
+      {(void**)&b->d_su, 2 * S * sizeof(float), true},        {(void**)&b->d_sflags, S, true},
+      {(void**)&b->d_snb, S, b->hw},
       {(void**)&b->d_tstep, 2 * sizeof(uint32_t), true},      {(void**)&b->d_cases, n * sizeof(BatchCase), true},
       {(void**)&b->d_order, n * sizeof(uint32_t), true},
       {(void**)&b->d_sync, n * sizeof(TeamSync), true},       {(void**)&b->d_err, sizeof(uint32_t), true},
@@ -689,21 +944,22 @@ FLB_API flb_status flb_batch_create(const flb_case_desc* cases, uint32_t n, int 
   }
   b->hcases.resize(n);
   for (uint32_t c = 0; c < n; c++) {
-    const size_t o = b->off[c], N = (size_t)b->nx[c] * b->ny[c];
+    const size_t o = b->off[c], po = b->poff[c], N = (size_t)b->nx[c] * b->ny[c];
+    const size_t NP = (size_t)b->sx[c] * b->ny[c];
     KParams& k = b->hcases[c].kp;
     fill_case_constants(&cases[c], k);
     k.nx = b->nx[c];
     k.ny = b->ny[c];
-    k.N = (uint32_t)N;
-    k.f = b->d_f + 9 * o;
-    for (int q = 0; q < 9; q++) k.slot[q] = b->d_f + 9 * o + (size_t)q * N;
-    k.rho = b->d_rho + o;
-    k.u = b->d_u + 2 * o;
-    k.flags = b->d_flags + o;
-    k.flags_out = b->d_flags + o;
-    k.nbmask = b->hw ? b->d_nbmask + o : nullptr;
+    k.N = (uint32_t)NP;
+    k.f = b->d_f + 9 * po;
+    for (int q = 0; q < 9; q++) k.slot[q] = b->d_f + 9 * po + (size_t)q * NP;
+    k.rho = b->d_rho + po;
+    k.u = b->d_u + 2 * po;
+    k.flags = b->d_flags + po;
+    k.flags_out = b->d_flags + po;
+    k.nbmask = b->hw ? b->d_nbmask + po : nullptr;
     k.tstep = b->d_tstep;
-    b->hcases[c].nsegx = (b->nx[c] + 31u) / 32u;
+    b->hcases[c].sx = b->sx[c];
     cudaError_t e = cudaMemcpyAsync(b->d_geo + o, cases[c].flags, N, cudaMemcpyHostToDevice, b->stream);
     if (e != cudaSuccess) return bail(bcuda(b, e, "cudaMemcpyAsync"));
   }
@@ -748,18 +1004,19 @@ FLB_API flb_status flb_batch_reset(flb_batch b) {
 FLB_API flb_status flb_batch_read_field(flb_batch b, uint32_t i, int field, void* dst, int on_device) {
   if (!b || !dst || i >= b->n) return FLB_ERR_INVALID_ARGUMENT;
   BDevice g(b->device);
-  const size_t o = b->off[i], N = (size_t)b->nx[i] * b->ny[i];
+  // the state is stored with padded rows; the copy drops the padding
+  const size_t po = b->poff[i], nx = b->nx[i], ny = b->ny[i], sx = b->sx[i];
   const void* src = nullptr;
-  size_t bytes = 0;
+  size_t es = 4, rows = 0;
   switch (field) {
-    case FLB_FIELD_F: src = b->d_f + 9 * o; bytes = 9 * N * sizeof(float); break;
-    case FLB_FIELD_RHO: src = b->d_rho + o; bytes = N * sizeof(float); break;
-    case FLB_FIELD_U: src = b->d_u + 2 * o; bytes = 2 * N * sizeof(float); break;
-    case FLB_FIELD_FLAGS: src = b->d_flags + o; bytes = N; break;
+    case FLB_FIELD_F: src = b->d_f + 9 * po; rows = 9 * ny; break;
+    case FLB_FIELD_RHO: src = b->d_rho + po; rows = ny; break;
+    case FLB_FIELD_U: src = b->d_u + 2 * po; rows = 2 * ny; break;
+    case FLB_FIELD_FLAGS: src = b->d_flags + po; rows = ny; es = 1; break;
     default: return bfail(b, FLB_ERR_INVALID_ARGUMENT, "the batch holds populations, density, velocity and flags");
   }
-  FLB_BCUDA(b, cudaMemcpyAsync(dst, src, bytes, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
-                               b->stream));
+  FLB_BCUDA(b, copy_rows(dst, nx * es, src, sx * es, nx * es, rows,
+                         on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, b->stream));
   FLB_BCUDA(b, cudaStreamSynchronize(b->stream));
   return FLB_OK;
 }
@@ -773,36 +1030,43 @@ FLB_API flb_status flb_batch_info(flb_batch b, int64_t info[8]) {
   info[4] = b->clusters;
   info[5] = b->tuned;
   info[6] = b->threads;
-  info[7] = b->team ? FLB_BATCH_TEAM : FLB_BATCH_CLUSTER;
+  info[7] = (b->team ? FLB_BATCH_TEAM : FLB_BATCH_CLUSTER) | (b->vec ? FLB_BATCH_VECTOR : 0);
   return FLB_OK;
 }
 
 FLB_API flb_status flb_batch_set_launch(flb_batch b, int mode, int group, int groups, int threads) {
   if (!b) return FLB_ERR_INVALID_ARGUMENT;
+  const bool vec = (mode & FLB_BATCH_VECTOR) != 0;
+  mode &= ~FLB_BATCH_VECTOR;
   if (mode != FLB_BATCH_CLUSTER && mode != FLB_BATCH_TEAM)
-    return bfail(b, FLB_ERR_INVALID_ARGUMENT, "mode must be FLB_BATCH_CLUSTER or FLB_BATCH_TEAM");
+    return bfail(b, FLB_ERR_INVALID_ARGUMENT,
+                 "mode must be FLB_BATCH_CLUSTER or FLB_BATCH_TEAM, optionally with FLB_BATCH_VECTOR");
   const bool team = mode == FLB_BATCH_TEAM;
   if (!team && group != 1 && group != 2 && group != 4 && group != 8 && group != 16)
     return bfail(b, FLB_ERR_INVALID_ARGUMENT, "a cluster has 1, 2, 4, 8 or 16 CTAs");
   if (team && group < 1) return bfail(b, FLB_ERR_INVALID_ARGUMENT, "a team has at least one CTA");
   if (threads != 256 && threads != 512 && threads != 1024)
     return bfail(b, FLB_ERR_INVALID_ARGUMENT, "threads per CTA must be 256, 512 or 1024");
+  if (vec && threads > kBatchVecMaxThreads)
+    return bfail(b, FLB_ERR_INVALID_ARGUMENT, "the vector data path takes 256 or 512 threads per CTA");
   if (groups < 1 || (uint32_t)groups > b->n)
     return bfail(b, FLB_ERR_INVALID_ARGUMENT, "groups must be between 1 and the number of cases");
   BDevice g(b->device);
   FLB_BCUDA(b, cudaStreamSynchronize(b->stream));  // a running launch reads the assignment
-  const int mx = max_groups(b, team, group, threads);
+  const int mx = max_groups(b, team, group, threads, vec);
   if (groups > mx)
     return bfail(b, FLB_ERR_UNSUPPORTED,
                  "at most " + std::to_string(mx) + " groups of this shape fit on the device at once");
   const int pc = b->cluster, pt = b->threads;
-  const bool pm = b->team;
+  const bool pm = b->team, pv = b->vec;
   b->team = team;
+  b->vec = vec;
   b->cluster = group;
   b->threads = threads;
   flb_status s = bassign(b, groups);
   if (s != FLB_OK) {
     b->team = pm;
+    b->vec = pv;
     b->cluster = pc;
     b->threads = pt;
   }

@@ -154,6 +154,7 @@ struct FspArgs {
   uint32_t steps;        // even: the run starts at an even t with flag buffer 0 current
   uint32_t wait_limit;   // polls before a barrier wait gives up
   uint32_t skip_cta;     // failure injection: this CTA never arrives (0xffffffff: none)
+  uint64_t* trace;       // null, or 4*steps+1 slots: CTA 0's exit time of each barrier (ns)
 };
 
 // A list holds at most ntiles entries; the length is clamped so that no state

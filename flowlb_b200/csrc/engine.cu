@@ -10,6 +10,7 @@
 #include <cuda_runtime.h>
 #include <nvtx3/nvToolsExt.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -292,8 +293,8 @@ uint32_t persist_skip_cta(flb_engine* h) {
 }
 
 // Issues 2*pairs free-surface steps from an even t (flag buffer 0 current) as
-// one persistent launch.
-flb_status issue_persist(flb_engine* h, int pairs) {
+// one persistent launch (trace: see FspArgs).
+flb_status issue_persist(flb_engine* h, int pairs, uint64_t* trace = nullptr) {
   const int saved = h->cur;
   h->cur = 0;
   refresh_params(h);
@@ -319,6 +320,7 @@ flb_status issue_persist(flb_engine* h, int pairs) {
   a.steps = 2u * (uint32_t)pairs;
   a.wait_limit = h->wait_limit;
   a.skip_cta = h->g_skip;
+  a.trace = trace;
   cudaError_t e = cudaSuccess;
   dispatch(h, [&](auto ops) { e = ops.persist(h, p0, p1, a); });
   if (e != cudaSuccess) return cuda_fail(h, e, "persistent free-surface step launch");
@@ -766,13 +768,16 @@ FLB_API flb_status flb_step(flb_handle h, uint64_t n) {
   while (remaining > 0 && s == FLB_OK) {
     // graphs cover pairs of steps from an even t; the last step of the call
     // runs on its own so that it writes density and velocity
+    // (free surface: every stream-collide writes density and velocity, so
+    // the graphs run to the end of the call)
     const uint64_t big = 2ull * kGraphPairs;
+    const uint64_t tail = h->fs ? 0u : 1u;
     if (h->fs && (!h->trust || !h->lists_valid)) {
       // first step after the state was written from outside: no write skipping
       h->launches += issue_step(h, h->t, remaining == 1);
       h->t += 1;
       remaining -= 1;
-    } else if ((h->t & 1u) == 0 && remaining > big) {
+    } else if ((h->t & 1u) == 0 && remaining >= big + tail) {
       s = capture(h, h->g_big, kGraphPairs);
       if (s != FLB_OK) break;
       cudaError_t e = cudaGraphLaunch(h->g_big.exec, h->stream);
@@ -780,7 +785,7 @@ FLB_API flb_status flb_step(flb_handle h, uint64_t n) {
       h->launches += h->g_big.kernels;
       h->t += big;
       remaining -= big;
-    } else if ((h->t & 1u) == 0 && remaining > 2) {
+    } else if ((h->t & 1u) == 0 && remaining >= 2 + tail) {
       s = capture(h, h->g_pair, 1);
       if (s != FLB_OK) break;
       cudaError_t e = cudaGraphLaunch(h->g_pair.exec, h->stream);
@@ -1167,6 +1172,46 @@ FLB_API flb_status flb_profile_steps(flb_handle h, uint64_t n, double pass_ms[3]
   }
   refresh_params(h);
   for (auto& e : ev) cudaEventDestroy(e);
+  return st;
+}
+
+FLB_API flb_status flb_profile_phases(flb_handle h, uint64_t n, double phase_ms[4]) {
+  if (!h || !phase_ms) return FLB_ERR_INVALID_ARGUMENT;
+  if (!h->fs || h->grid_persist == 0)
+    return fail(h, FLB_ERR_UNSUPPORTED, "phase timing needs the persistent free-surface step");
+  if (h->broken) return fail(h, FLB_ERR_CUDA, "call flb_reset first");
+  DeviceGuard guard(h->device);
+  for (int k = 0; k < 4; k++) phase_ms[k] = 0.0;
+  // steady state from an even t: per-pass steps until then
+  while (!h->trust || !h->lists_valid || (h->t & 1u)) {
+    h->launches += issue_step(h, h->t, false);
+    h->t += 1;
+  }
+  const uint64_t pairs_total = (n + 1) / 2;
+  const int per = kGraphPairs;
+  uint64_t* d_trace = nullptr;
+  const size_t slots = 8u * per + 1u;
+  FLB_CUDA(h, cudaMallocAsync((void**)&d_trace, slots * sizeof(uint64_t), h->stream));
+  std::vector<uint64_t> tr(slots);
+  flb_status st = FLB_OK;
+  for (uint64_t done = 0; done < pairs_total && st == FLB_OK; done += per) {
+    const int pairs = (int)std::min<uint64_t>((uint64_t)per, pairs_total - done);
+    st = issue_persist(h, pairs, d_trace);
+    if (st != FLB_OK) break;
+    h->launches += 1;
+    h->t += 2u * (uint64_t)pairs;
+    cudaError_t e = cudaMemcpyAsync(tr.data(), d_trace, (8u * pairs + 1u) * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                                    h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+      st = cuda_fail(h, e, "phase trace read-back");
+      break;
+    }
+    st = check_persist(h);
+    for (int b = 1; b <= 8 * pairs && st == FLB_OK; b++) phase_ms[(b - 1) % 4] += (double)(tr[b] - tr[b - 1]) * 1e-6;
+  }
+  cudaFreeAsync(d_trace, h->stream);
+  cudaStreamSynchronize(h->stream);
   return st;
 }
 

@@ -65,6 +65,22 @@ __device__ __forceinline__ bool grid_barrier(uint32_t* count, uint32_t target, u
   return ok != 0;
 }
 
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// The next grid barrier of the launch; with a.trace set, CTA 0 records the
+// time it leaves the barrier (a.trace[k] for the k-th barrier, a.trace[0] the
+// start of the launch), so the phases of the production kernel can be timed.
+__device__ __forceinline__ bool next_barrier(const FspArgs& a, uint32_t& nbar, int& ok) {
+  ++nbar;
+  const bool good = grid_barrier(a.bar, nbar * gridDim.x, a.err, a.wait_limit, blockIdx.x != a.skip_cta, ok);
+  if (a.trace && blockIdx.x == 0 && threadIdx.x == 0) a.trace[nbar] = global_ns();
+  return good;
+}
+
 // One time step with parity ODD (p: the step's parameters, its flag buffers
 // in the order of that parity).  Returns false when a barrier gave up.
 template <class S, class C, class M, bool HW, bool FU, bool ODD>
@@ -84,18 +100,18 @@ __device__ __forceinline__ bool fsp_step(const KParams& p, const FspArgs& a, Fla
     const uint32_t y = (t / a.nsx) * kSTH + row, x = (t % a.nsx) * kSTW + xo;
     if (y < p.ny && x < p.nx) fs1_cell<S, C, M, HW, ODD>(p, x, y);
   }
-  if (!grid_barrier(a.bar, ++nbar * G, a.err, a.wait_limit, blockIdx.x != a.skip_cta, ok)) return false;
+  if (!next_barrier(a, nbar, ok)) return false;
   // stream-collide
   for (uint32_t i = blockIdx.x; i < nsc; i += G) {
     const uint32_t t = __ldcg(lsc + i);
     const uint32_t y = (t / a.nsx) * kSTH + row, x = (t % a.nsx) * kSTW + xo;
     if (y < p.ny && x < p.nx) sc_cell<S, C, M, true, HW, true, ODD, FU>(p, x, y);
   }
-  if (!grid_barrier(a.bar, ++nbar * G, a.err, a.wait_limit, blockIdx.x != a.skip_cta, ok)) return false;
+  if (!next_barrier(a, nbar, ok)) return false;
   // FS_2..4: flag stencil, mass / excess / fill level, activity words
   for (uint32_t i = blockIdx.x; i < nfs; i += G)
     fs234_super_tile<S, C, M, ODD, 128>(p, __ldcg(lfs + i), a.nsx, a.nz, sm, wact_sm);
-  if (!grid_barrier(a.bar, ++nbar * G, a.err, a.wait_limit, blockIdx.x != a.skip_cta, ok)) return false;
+  if (!next_barrier(a, nbar, ok)) return false;
   // list build for the next step (k_build_lists spread over the grid): append
   // to the next parity's lengths, zeroed by the previous step's build; zero
   // this parity's, which every CTA read before the first barrier
@@ -125,7 +141,7 @@ __device__ __forceinline__ bool fsp_step(const KParams& p, const FspArgs& a, Fla
       if (fs && kfs < T) out_fs[kfs] = t;
     }
   }
-  return grid_barrier(a.bar, ++nbar * G, a.err, a.wait_limit, blockIdx.x != a.skip_cta, ok);
+  return next_barrier(a, nbar, ok);
 }
 
 // a.steps steps (even) from an even t with flag buffer 0 current: p0 holds the
@@ -143,6 +159,7 @@ __global__ void __launch_bounds__(kPBlock, 1) k_fs_persist(const __grid_constant
   if (threadIdx.x == 0) ok = __ldcg(a.err) == 0u ? 1 : 0;
   __syncthreads();
   if (!ok) return;
+  if (a.trace && blockIdx.x == 0 && threadIdx.x == 0) a.trace[0] = global_ns();
   uint32_t nbar = 0;
   for (uint32_t s = 0; s < a.steps; s += 2) {
     if (!fsp_step<S, C, M, HW, FU, false>(p0, a, sm, wact_sm, nbar, ok)) return;

@@ -29,7 +29,7 @@ EXPORTS = [
     "flb_case_desc_init", "flb_create", "flb_reset", "flb_destroy", "flb_step", "flb_sync", "flb_get_time",
     "flb_set_step_mode", "flb_get_step_mode", "flb_set_wait_limit",
     "flb_set_stream", "flb_get_stream", "flb_field_info", "flb_read_field", "flb_write_field", "flb_total_mass",
-    "flb_total_mass_noalloc", "flb_cell_counts", "flb_check_finite", "flb_run_pass", "flb_profile_steps", "flb_launch_count", "flb_save_checkpoint",
+    "flb_total_mass_noalloc", "flb_cell_counts", "flb_check_finite", "flb_run_pass", "flb_profile_steps", "flb_profile_phases", "flb_launch_count", "flb_save_checkpoint",
     "flb_load_checkpoint", "flb_last_error", "flb_status_string", "flb_version",
     "flb_batch_create", "flb_batch_step", "flb_batch_sync", "flb_batch_reset", "flb_batch_read_field",
     "flb_batch_info", "flb_batch_set_launch", "flb_batch_set_wait_limit", "flb_batch_destroy",
@@ -77,7 +77,7 @@ class SetupStruct(C.Structure):
 
 VTI_UINT8, VTI_FLOAT32, VTI_FLOAT64 = 0, 1, 2
 VIZ_UX, VIZ_UY, VIZ_MAGNITUDE, VIZ_PRESSURE = 0, 1, 2, 3
-BATCH_CLUSTER, BATCH_TEAM = 0, 1
+BATCH_CLUSTER, BATCH_TEAM, BATCH_VECTOR = 0, 1, 4
 STEP_AUTO, STEP_KERNELS, STEP_PERSISTENT = 0, 1, 2
 
 
@@ -133,6 +133,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "flb_check_finite": (C.c_int, [H]),
         "flb_run_pass": (C.c_int, [H, C.c_int]),
         "flb_profile_steps": (C.c_int, [H, C.c_uint64, C.POINTER(C.c_double)]),
+        "flb_profile_phases": (C.c_int, [H, C.c_uint64, C.POINTER(C.c_double)]),
         "flb_launch_count": (C.c_int, [H, C.POINTER(C.c_uint64)]),
         "flb_save_checkpoint": (C.c_int, [H, C.c_char_p]),
         "flb_load_checkpoint": (C.c_int, [H, C.c_char_p]),
@@ -374,6 +375,14 @@ class Solver:
         self._check(load_library().flb_profile_steps(self._h, int(n), arr))
         return dict(stream_collide=arr[0], fs1=arr[1], fs234=arr[2])
 
+    def profile_phases(self, n: int) -> dict:
+        """Runs n steps of the persistent free-surface step with its phases
+        timed on the device clock; summed ms per phase (they add up to the
+        step time of the production kernel)."""
+        arr = (C.c_double * 4)()
+        self._check(load_library().flb_profile_phases(self._h, int(n), arr))
+        return dict(fs1=arr[0], stream_collide=arr[1], fs234=arr[2], build=arr[3])
+
     def save_checkpoint(self, path: str):
         self._check(load_library().flb_save_checkpoint(self._h, path.encode()))
 
@@ -542,13 +551,14 @@ class Batch:
         a = (C.c_int64 * 8)()
         self._check(load_library().flb_batch_info(self._h, a))
         return dict(cases=a[0], cells=a[1], t=a[2], group=a[3], groups=a[4], tuned=bool(a[5]), threads=a[6],
-                    mode="team" if a[7] == BATCH_TEAM else "cluster")
+                    mode="team" if (a[7] & ~BATCH_VECTOR) == BATCH_TEAM else "cluster",
+                    vector=bool(a[7] & BATCH_VECTOR))
 
-    def set_launch(self, mode: str, group: int, groups: int, threads: int):
+    def set_launch(self, mode: str, group: int, groups: int, threads: int, vector: bool = False):
         """Launch shape for the following steps: ``mode`` "cluster" or "team",
         CTAs per group, groups, threads per CTA (``info()`` of a tuned batch,
-        for instance); the state is kept."""
-        m = {"cluster": BATCH_CLUSTER, "team": BATCH_TEAM}[mode]
+        for instance), and the vector data path; the state is kept."""
+        m = {"cluster": BATCH_CLUSTER, "team": BATCH_TEAM}[mode] | (BATCH_VECTOR if vector else 0)
         self._check(load_library().flb_batch_set_launch(self._h, m, int(group), int(groups), int(threads)))
 
     def set_wait_limit(self, polls: int):

@@ -223,6 +223,16 @@ FLB_API flb_status flb_run_pass(flb_handle h, int pass);
  * milliseconds: pass_ms[0] stream-collide, [1] FS_1, [2] FS_2..4.  Advances t. */
 FLB_API flb_status flb_profile_steps(flb_handle h, uint64_t n, double pass_ms[3]);
 
+/* Runs n time steps (rounded up to even, from the next even t in steady
+ * state) in the persistent free-surface form with a device clock read by one
+ * CTA as it leaves every grid barrier, and returns the summed time of each
+ * phase in milliseconds: phase_ms[0] FS_1, [1] stream-collide, [2] FS_2..4,
+ * [3] list build, each with the barrier that ends it.  Unlike
+ * flb_profile_steps nothing is serialised: the phases sum to the step time
+ * of the production kernel.  Advances t; FLB_ERR_UNSUPPORTED without a
+ * persistent form. */
+FLB_API flb_status flb_profile_phases(flb_handle h, uint64_t n, double phase_ms[4]);
+
 /* Kernels this handle has launched so far (graph replays count each kernel). */
 FLB_API flb_status flb_launch_count(flb_handle h, uint64_t* launches);
 
@@ -249,7 +259,7 @@ FLB_API flb_status flb_load_checkpoint(flb_handle h, const char* path);
  * probe step count > 1 times candidate modes, group sizes and counts on the
  * batch itself and keeps the fastest, then rebuilds the initial state.  The
  * device, and the stream if given, come from cases[0]. */
-enum { FLB_BATCH_CLUSTER = 0, FLB_BATCH_TEAM = 1 };
+enum { FLB_BATCH_CLUSTER = 0, FLB_BATCH_TEAM = 1, FLB_BATCH_VECTOR = 4 };
 typedef struct flb_batch_s* flb_batch;
 FLB_API flb_status flb_batch_create(const flb_case_desc* cases, uint32_t n, int autotune, flb_batch* out);
 FLB_API flb_status flb_batch_step(flb_batch b, uint64_t n);
@@ -259,12 +269,17 @@ FLB_API flb_status flb_batch_reset(flb_batch b);
 /* FLB_FIELD_F, _RHO, _U or _FLAGS of case i (float, as a precision-32 handle) */
 FLB_API flb_status flb_batch_read_field(flb_batch b, uint32_t i, int field, void* dst, int on_device);
 /* info[0..7] = cases, cells, t, CTAs per group, groups, autotuned, threads
- * per CTA, mode (FLB_BATCH_CLUSTER or FLB_BATCH_TEAM) */
+ * per CTA, mode (FLB_BATCH_CLUSTER or FLB_BATCH_TEAM, with FLB_BATCH_VECTOR
+ * set when the vector data path runs) */
 FLB_API flb_status flb_batch_info(flb_batch b, int64_t info[8]);
 /* Sets the launch shape (info[7], [3], [4], [6] of an earlier tuned batch,
- * for instance): mode; CTAs per group (1, 2, 4, 8 or 16 for a cluster, >= 1
- * for a team); 1 <= groups <= the groups of that shape that fit on the device
- * at once, and <= the number of cases; 256, 512 or 1024 threads per CTA.
+ * for instance): mode, with FLB_BATCH_VECTOR or'ed in for the vector data
+ * path (four cells per thread, 16-byte population accesses; the state is
+ * stored with rows padded to a multiple of four cells, so every case can take
+ * it); CTAs per group (1, 2, 4, 8 or 16 for a cluster, >= 1 for a team);
+ * 1 <= groups <= the groups of that shape that fit on the device at once, and
+ * <= the number of cases; 256, 512 or 1024 threads per CTA (256 or 512 on the
+ * vector path).
  * The state and t are kept (results do not depend on the shape).
  * FLB_ERR_INVALID_ARGUMENT for a shape out of range, FLB_ERR_UNSUPPORTED for
  * one that cannot launch. */

@@ -11,7 +11,8 @@
  * floating-point contraction off J and dJ/ds agree bit for bit.
  *
  * Model per fluid cell: pull streaming with half-way walls (x and y periodic,
- * walls given by flags), rho = sum f, v = j / rho, u = (v + g/2) / (1 + s/2),
+ * walls given by flags), rho = sum f, v = j (1 / rho), u = (v + g/2) (1 / d)
+ * with d = 1 + s/2 (each reciprocal taken once and multiplied in),
  * F = rho (g - s u), out_i = (1 - w) f_i + w feq_i + (1 - w/2) F_i with the
  * second-order feq and Guo's F_i.  J = (1/W) sum over the last W steps of
  * sum_y rho u_x at x = nx - 1.
@@ -52,7 +53,7 @@ static void agather(const adj_p* p, const double* fin, uint32_t x, uint32_t y, d
 }
 
 typedef struct {
-  double rho, vx, vy, d, ux, uy, Fx, Fy, usq, uF;
+  double rho, ir, vx, vy, d, id, ux, uy, Fx, Fy, usq, uF;
 } acell;
 
 static acell astate(const adj_p* p, const double* f, double s) {
@@ -60,11 +61,13 @@ static acell astate(const adj_p* p, const double* f, double s) {
   c.rho = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
   const double jx = f[1] - f[2] + f[5] - f[6] + f[7] - f[8];
   const double jy = f[3] - f[4] + f[5] - f[6] - f[7] + f[8];
-  c.vx = jx / c.rho;
-  c.vy = jy / c.rho;
+  c.ir = 1.0 / c.rho;
+  c.vx = jx * c.ir;
+  c.vy = jy * c.ir;
   c.d = 1.0 + 0.5 * s;
-  c.ux = (c.vx + 0.5 * p->gx) / c.d;
-  c.uy = (c.vy + 0.5 * p->gy) / c.d;
+  c.id = 1.0 / c.d;
+  c.ux = (c.vx + 0.5 * p->gx) * c.id;
+  c.uy = (c.vy + 0.5 * p->gy) * c.id;
   c.Fx = c.rho * (p->gx - s * c.ux);
   c.Fy = c.rho * (p->gy - s * c.uy);
   c.usq = c.ux * c.ux + c.uy * c.uy;
@@ -162,12 +165,12 @@ static void abackstep(const adj_p* p, const double* fin, const double* lam_next,
       uyb += -s * c.rho * Fyb;
       double sb = -c.rho * (Fxb * c.ux + Fyb * c.uy);
       double gxb = c.rho * Fxb, gyb = c.rho * Fyb;
-      const double vxb = uxb / c.d, vyb = uyb / c.d;
-      sb += -0.5 * (uxb * c.ux + uyb * c.uy) / c.d;
-      gxb += 0.5 * uxb / c.d;
-      gyb += 0.5 * uyb / c.d;
-      const double jxb = vxb / c.rho, jyb = vyb / c.rho;
-      rhob += -(vxb * c.vx + vyb * c.vy) / c.rho;
+      const double vxb = uxb * c.id, vyb = uyb * c.id;
+      sb += -0.5 * (uxb * c.ux + uyb * c.uy) * c.id;
+      gxb += 0.5 * uxb * c.id;
+      gyb += 0.5 * uyb * c.id;
+      const double jxb = vxb * c.ir, jyb = vyb * c.ir;
+      rhob += -(vxb * c.vx + vyb * c.vy) * c.ir;
       for (int i = 0; i < 9; i++) {
         const double v = fb[i] + rhob + jxb * (double)ACX[i] + jyb * (double)ACY[i];
         int b;

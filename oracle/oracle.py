@@ -251,13 +251,20 @@ def ref_cuda_run(state: dict, nx: int, ny: int, precision: int, free_surface: bo
     return s
 
 
+def ref_cuda_timing_available() -> bool:
+    return os.path.exists(os.path.join(REF_DIR, "libflbref_cuda_timing.so"))
+
+
 def ref_cuda_time(state: dict, nx: int, ny: int, precision: int, free_surface: bool, tau: float, fx: float,
-                  fy: float, warm: int, nsteps: int, t0: int = 0) -> tuple:
+                  fy: float, warm: int, nsteps: int, t0: int = 0, build: str = "parity") -> tuple:
     """Device time of the reference's own CUDA step sequence (16x16 blocks, one
     launch per kernel and step, as its headless loop issues them): ``warm``
     untimed steps from ``state`` at ``t0``, then ``nsteps`` timed with CUDA
-    events.  Returns (milliseconds, final state)."""
-    L = C.CDLL(os.path.join(REF_DIR, "libflbref_cuda.so"))
+    events.  ``build``: "parity" (the kernels as written, no floating-point
+    contraction: bit-comparable) or "timing" (FlowLB's own build flags with
+    the debug printf calls compiled out).  Returns (milliseconds, final state)."""
+    lib_name = {"parity": "libflbref_cuda.so", "timing": "libflbref_cuda_timing.so"}[build]
+    L = C.CDLL(os.path.join(REF_DIR, lib_name))
     L.ref_cuda_time.argtypes = [C.c_int] * 7 + [C.c_double] * 3 + [C.c_uint64] * 3 + [C.c_void_p] * 8
     dt = np.float32 if precision == 32 else np.float64
     s = {k: np.ascontiguousarray(np.array(v, copy=True), dtype=(np.uint8 if k == "flags" else dt))
@@ -274,6 +281,26 @@ def ref_cuda_time(state: dict, nx: int, ny: int, precision: int, free_surface: b
     if rc != 0:
         raise RuntimeError(f"ref_cuda_time failed: {rc}")
     return float(ms.value), s
+
+
+def ref_cuda_isoline(field: np.ndarray, nx: int, ny: int, precision: int, iso: float, width: int, height: int,
+                     bounds) -> np.ndarray:
+    """The reference's own iso-line kernel (d_CreateIsoSurfaceVector2D) on a
+    two-component field (2N values, reference layout) into a (height, width)
+    uint8 image.  Only camera bounds inside the lattice and finite values are
+    accepted (the kernel writes through a surface that traps out of range)."""
+    L = C.CDLL(os.path.join(REF_DIR, "libflbref_cuda.so"))
+    L.ref_cuda_isoline.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_float, C.c_uint, C.c_uint,
+                                   C.POINTER(C.c_uint), C.c_void_p]
+    dt = np.float32 if precision == 32 else np.float64
+    v = np.ascontiguousarray(field, dtype=dt)
+    assert v.size == 2 * nx * ny
+    b = (C.c_uint * 4)(*[int(k) for k in bounds])
+    img = np.zeros((height, width), np.uint8)
+    rc = L.ref_cuda_isoline(precision, nx, ny, v.ctypes.data, float(iso), width, height, b, img.ctypes.data)
+    if rc != 0:
+        raise RuntimeError(f"ref_cuda_isoline failed: {rc}")
+    return img
 
 
 def adjoint_run(flags: np.ndarray, porosity: np.ndarray, tau: float, gx: float, gy: float, steps: int,

@@ -12,12 +12,21 @@
 // (cudaInitData.cuh:90-125), 16x16 blocks and a ceil-divided grid
 // (cudaUtils.cu:89-105), and per step FS_1, StreamCollide, FS_2, FS_3, FS_4
 // (free surface) or StreamCollide alone (mono-fluid).
+//
+// It also runs the reference's headless-capable visualisation kernel
+// d_CreateIsoSurfaceVector2D (src/cuda/cudaIsosurface.cuh:33-199,
+// cudaIsosurface.cu:16-76; built from cudaIsosurface.cu in place) into a CUDA
+// array through a surface object, as the viewer's texture would receive it
+// (ref_cuda_isoline).
+#include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <vector>
 
 #include <cuda_runtime.h>
 
 #include "cudaInitData.cuh"
+#include "cudaIsosurface.cuh"
 #include "lbmKernel2D.cuh"
 
 namespace {
@@ -154,4 +163,73 @@ extern "C" int ref_cuda_time(int precision, int nx, int ny, int free_surface, in
     return run_ref<double>(nx, ny, free_surface, collision, subgrid, use_force, tau, fx, fy, t0, nsteps, -1, f,
                            rho, u, flags, mass, excess, phi, warm, ms);
   return -1;
+}
+
+// The reference's iso-line kernel on a two-component field v (host, 2N values
+// of the precision, v[c] and v[c + N]) into a width x height uint8 image
+// (host, row-major, row 0 = the surface's row 0): 16x16 blocks over the
+// lattice, as the viewer launches it.  Every pixel it writes lies inside the
+// image for camera bounds b0 < b1 <= nx, b2 < b3 <= ny and finite values (the
+// pixel mapping of drawLine, cudaIsosurface.cu:23-31, keeps both end points
+// of a segment inside and Bresenham stays between them); other inputs are
+// refused here (-2), because the kernel writes through a surface that traps
+// out of range.
+extern "C" int ref_cuda_isoline(int precision, int nx, int ny, const void* v, float iso, unsigned width,
+                                unsigned height, const unsigned bounds[4], uint8_t* img) {
+  if (nx < 3 || ny < 3 || width == 0 || height == 0 || !v || !img || !bounds) return -1;
+  if (!(bounds[0] < bounds[1] && bounds[1] <= (unsigned)nx && bounds[2] < bounds[3] && bounds[3] <= (unsigned)ny))
+    return -2;
+  if (!std::isfinite(iso)) return -2;
+  const unsigned Nx = (unsigned)nx, Ny = (unsigned)ny, N = Nx * Ny;
+  const size_t es = precision == 64 ? 8 : 4;
+  for (size_t k = 0; k < 2ull * N; k++) {
+    const double x = precision == 64 ? static_cast<const double*>(v)[k] : static_cast<const float*>(v)[k];
+    if (!std::isfinite(x)) return -2;
+  }
+  // __constant__ sizes of the kernels (d_Nx, d_Ny, d_N), as the solver set-up uploads them
+  static float wf[9] = {4.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f, 1.0f / 9.0f,
+                        1.0f / 36.0f, 1.0f / 36.0f, 1.0f / 36.0f, 1.0f / 36.0f};
+  static double wd[9] = {4.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0, 1.0 / 9.0,
+                         1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0, 1.0 / 36.0};
+  FLB::OptionsCalculation opts;
+  opts.graphicsAPI = FLB::API::NONE;
+  opts.typeProblem = FLB::TypeProblem::MONOFLUID;
+  opts.relaxationTime = 0.6;
+  opts.precision = precision == 64 ? 64 : 32;
+  FLB::Units units;
+  if (precision == 64) FLB::h_initConstantDataCuda2D<double>(opts, wd, Nx, Ny, N, units);
+  else FLB::h_initConstantDataCuda2D<float>(opts, wf, Nx, Ny, N, units);
+  void* d_v = nullptr;
+  cudaArray_t arr = nullptr;
+  cudaSurfaceObject_t surf = 0;
+  cudaError_t e = cudaMalloc(&d_v, 2ull * N * es);
+  if (e == cudaSuccess) e = cudaMemcpy(d_v, v, 2ull * N * es, cudaMemcpyHostToDevice);
+  cudaChannelFormatDesc cd = cudaCreateChannelDesc<unsigned char>();
+  if (e == cudaSuccess) e = cudaMallocArray(&arr, &cd, width, height, cudaArraySurfaceLoadStore);
+  std::vector<uint8_t> zero((size_t)width * height, 0);
+  if (e == cudaSuccess) e = cudaMemcpy2DToArray(arr, 0, 0, zero.data(), width, width, height, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    cudaResourceDesc rd;
+    std::memset(&rd, 0, sizeof(rd));
+    rd.resType = cudaResourceTypeArray;
+    rd.res.array.array = arr;
+    e = cudaCreateSurfaceObject(&surf, &rd);
+  }
+  if (e == cudaSuccess) {
+    dim3 block(16, 16);
+    dim3 grid((Nx + block.x - 1) / block.x, (Ny + block.y - 1) / block.y);
+    if (precision == 64)
+      FLB::d_CreateIsoSurfaceVector2D<double><<<grid, block>>>(static_cast<const double*>(d_v), surf, width, height,
+                                                               iso, bounds[0], bounds[1], bounds[2], bounds[3]);
+    else
+      FLB::d_CreateIsoSurfaceVector2D<float><<<grid, block>>>(static_cast<const float*>(d_v), surf, width, height,
+                                                              iso, bounds[0], bounds[1], bounds[2], bounds[3]);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy2DFromArray(img, width, arr, 0, 0, width, height, cudaMemcpyDeviceToHost);
+  if (surf) cudaDestroySurfaceObject(surf);
+  if (arr) cudaFreeArray(arr);
+  if (d_v) cudaFree(d_v);
+  return e == cudaSuccess ? 0 : (int)e;
 }

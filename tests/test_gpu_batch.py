@@ -56,6 +56,39 @@ def test_batch_matches_single_handles(bb, arith, autotune):
     b.close()
 
 
+@pytest.mark.parametrize("bb", [E.BB_HALFWAY, E.BB_IMPLICIT], ids=["halfway", "implicit"])
+@pytest.mark.parametrize("arith", [E.ARITH_FUSED, E.ARITH_REFERENCE], ids=["fused", "ref-arith"])
+@pytest.mark.parametrize("shape", [("team", 3, 7, 512), ("team", 1, 23, 256), ("cluster", 8, 2, 512)],
+                         ids=lambda v: f"{v[0]}{v[1]}x{v[2]}t{v[3]}")
+def test_batch_vector_path_matches_single_handles(bb, arith, shape):
+    """The vector data path (four cells per thread, rows padded to a multiple
+    of four cells) on widths of every residue mod 4, narrower than a group,
+    and wider than one 128-cell warp segment: every case equals its own
+    handle bit for bit, from both step parities."""
+    ens = _small_ensemble(23, 4321)
+    ens[0] = (cases.channel_with_block(3, 7, 1, 2, 2), 0.6, 1e-5, 0.0)
+    ens[1] = (cases.channel_with_block(131, 9, 60, 70, 4), 0.55, 2e-5, 0.0)
+    ens[2] = (cases.channel_with_block(258, 11, 100, 130, 6), 0.7, 1e-5, 0.0)
+    b = E.Batch(ens, bounce_back=bb, arithmetic=arith, autotune=0)
+    b.set_launch(*shape, vector=True)
+    assert b.info()["vector"]
+    for n in (1, 36, 29):
+        b.step(n)
+    b.sync()
+    for i, (flags, tau, gx, gy) in enumerate(ens):
+        s = E.Solver(flags, precision=32, tau=tau, fx=gx, fy=gy, bounce_back=bb, arithmetic=arith)
+        s.step(66)
+        for name, fid, ref in (("f", E.FIELD_F, s.f), ("rho", E.FIELD_RHO, s.rho), ("u", E.FIELD_U, s.u),
+                               ("flags", E.FIELD_FLAGS, s.flags)):
+            got = b.read(i, fid)
+            assert exact_equal(got, ref), f"case {i} {flags.shape} {name}: {first_mismatch(got, ref)}"
+        s.close()
+    with pytest.raises(E.FlowLBError) as ei:  # the vector path takes at most 512 threads per CTA
+        b.set_launch("team", 1, 2, 1024, vector=True)
+    assert ei.value.status == 1
+    b.close()
+
+
 def test_batch_rejects_unsupported_cases():
     ens = _small_ensemble(2, 1)
     with pytest.raises(E.FlowLBError):
@@ -68,12 +101,14 @@ def test_batch_launch_shape_changes_keep_the_state():
     ens = _small_ensemble(11, 7)
     b = E.Batch(ens, autotune=0)
     steps = 0
-    shapes = ((("cluster", 1, 5, 256), 3), (("team", 3, 4, 512), 6), (("cluster", 16, 1, 1024), 8),
-              (("team", 1, 11, 256), 1), (("team", 7, 2, 1024), 5), (("cluster", 4, 3, 1024), 1))
+    shapes = ((("cluster", 1, 5, 256), 3), (("team", 3, 4, 512, True), 6), (("cluster", 16, 1, 1024), 8),
+              (("team", 1, 11, 256), 1), (("cluster", 4, 2, 256, True), 2), (("team", 7, 2, 1024), 5),
+              (("cluster", 4, 3, 1024), 1))
     for shape, n in shapes:
         b.set_launch(*shape)
         info = b.info()
-        assert (info["mode"], info["group"], info["groups"], info["threads"]) == shape
+        assert (info["mode"], info["group"], info["groups"], info["threads"]) == shape[:4]
+        assert info["vector"] == (len(shape) > 4)
         b.step(n)
         steps += n
     b.sync()

@@ -100,17 +100,25 @@ def _record(line):
             fp.write(json.dumps(line) + "\n")
 
 
+TIMING_BUILD = "timing" if O.ref_cuda_timing_available() else "parity"
+
+
 def test_engine_outpaces_reference_kernels_single_phase_8192x2048():
     """The engine in the reference's own modes (implicit walls, reference
     arithmetic) against FlowLB's CUDA kernels on the same GPU, 8192x2048 plain
-    channel, FP32: equal populations after the same 220 steps, and a faster
-    step (device time of the last 200 steps of each)."""
+    channel, FP32: equal populations after the same 220 steps (against the
+    kernels as written, no contraction), and a faster step (device time of the
+    last 200 steps of each; the reference timed in its own build, debug
+    printf calls compiled out)."""
     import flowlb_b200.engine as E
 
     c = cases.hbm_probe(8192, 2048)
     o = O.Oracle(c.flags, O.OracleConfig(variant=O.F32_M32, tau=c.tau, fx=c.fx))
-    ref_ms, ref = O.ref_cuda_time(snapshot(o, False), c.nx, c.ny, 32, False, c.tau, c.fx, 0.0, warm=20, nsteps=200)
+    st0 = snapshot(o, False)
     o.close()
+    nofma_ms, ref = O.ref_cuda_time(st0, c.nx, c.ny, 32, False, c.tau, c.fx, 0.0, warm=20, nsteps=200)
+    ref_ms, _ = O.ref_cuda_time(st0, c.nx, c.ny, 32, False, c.tau, c.fx, 0.0, warm=20, nsteps=200,
+                                build=TIMING_BUILD)
     s = E.Solver(c.flags, precision=32, mass_precision=32, tau=c.tau, fx=c.fx, bounce_back=E.BB_IMPLICIT,
                  arithmetic=E.ARITH_REFERENCE, device=0)
     s.step(20)
@@ -125,7 +133,9 @@ def test_engine_outpaces_reference_kernels_single_phase_8192x2048():
     def_ms = _engine_ms(d, 200)
     d.close()
     mlups = lambda ms: c.cells * 200 / (ms * 1e-3) / 1e6  # noqa: E731
-    _record({"case": "single phase 8192x2048 FP32, 200 steps", "reference_kernels_mlups": round(mlups(ref_ms), 1),
+    _record({"case": "single phase 8192x2048 FP32, 200 steps", "reference_build": TIMING_BUILD,
+             "reference_kernels_mlups": round(mlups(ref_ms), 1),
+             "reference_kernels_no_contraction_mlups": round(mlups(nofma_ms), 1),
              "engine_reference_modes_mlups": round(mlups(eng_ms), 1), "engine_defaults_mlups": round(mlups(def_ms), 1),
              "speedup_reference_modes": round(ref_ms / eng_ms, 2), "speedup_defaults": round(ref_ms / def_ms, 2)})
     assert eng_ms < ref_ms
@@ -134,13 +144,17 @@ def test_engine_outpaces_reference_kernels_single_phase_8192x2048():
 def test_engine_outpaces_reference_kernels_dam_break_2048x512():
     """The free-surface step in the reference's modes against FlowLB's five
     CUDA kernels per step on the same GPU, 2048x512 dam break, FP32 (mass in
-    FP32 as in the reference): device time of 200 steps after 20."""
+    FP32 as in the reference): device time of 200 steps after 20 (the
+    reference in its own build, debug printf calls compiled out)."""
     import flowlb_b200.engine as E
 
     c = cases.dam_break(1)
     o = O.Oracle(c.flags, O.OracleConfig(variant=O.F32_M32, free_surface=True, tau=c.tau, fy=c.fy))
-    ref_ms, _ = O.ref_cuda_time(snapshot(o, True), c.nx, c.ny, 32, True, c.tau, 0.0, c.fy, warm=20, nsteps=200)
+    st0 = snapshot(o, True)
     o.close()
+    nofma_ms, _ = O.ref_cuda_time(st0, c.nx, c.ny, 32, True, c.tau, 0.0, c.fy, warm=20, nsteps=200)
+    ref_ms, _ = O.ref_cuda_time(st0, c.nx, c.ny, 32, True, c.tau, 0.0, c.fy, warm=20, nsteps=200,
+                                build=TIMING_BUILD)
     s = E.Solver(c.flags, free_surface=True, precision=32, mass_precision=32, tau=c.tau, fy=c.fy,
                  bounce_back=E.BB_IMPLICIT, fs_mode=E.FS_REFERENCE, arithmetic=E.ARITH_REFERENCE, device=0)
     s.step(20)
@@ -154,9 +168,47 @@ def test_engine_outpaces_reference_kernels_dam_break_2048x512():
     def_ms = _engine_ms(d, 200)
     d.close()
     mlups = lambda ms: c.cells * 200 / (ms * 1e-3) / 1e6  # noqa: E731
-    _record({"case": "free-surface dam break 2048x512 FP32, 200 steps",
+    _record({"case": "free-surface dam break 2048x512 FP32, 200 steps", "reference_build": TIMING_BUILD,
              "reference_kernels_mlups": round(mlups(ref_ms), 1),
+             "reference_kernels_no_contraction_mlups": round(mlups(nofma_ms), 1),
              "engine_reference_modes_mlups": round(mlups(eng_ms), 1),
              "engine_defaults_fp64_mass_mlups": round(mlups(def_ms), 1),
              "speedup_reference_modes": round(ref_ms / eng_ms, 2), "speedup_defaults": round(ref_ms / def_ms, 2)})
     assert eng_ms < ref_ms
+
+
+@pytest.mark.parametrize("prec", [32, 64])
+def test_isoline_matches_reference_kernel(prec):
+    """flb_viz_isoline against the reference's own d_CreateIsoSurfaceVector2D
+    (src/cuda/cudaIsosurface.cuh:33-199, cudaIsosurface.cu:16-76, compiled in
+    place) on the velocity magnitude of a free-surface state: whole domain,
+    camera windows and up- and down-scaled images.  The camera bounds stay
+    inside the lattice, where every pixel the reference writes lies inside
+    the image (its surface traps out of range).  The engine takes the
+    magnitude as sqrt(x*x + y*y) rounded per operation, the reference calls
+    hypotf: the two may differ in the last bit of a node value, which can move
+    a line end across a pixel boundary, so a few pixels may differ; the test
+    counts them and holds them to 0.5 % of the reference's line pixels."""
+    from flowlb_b200 import engine as E
+
+    c = cases.small_dam_break(160, 96)
+    s = E.Solver(c.flags, free_surface=True, precision=prec, mass_precision=64, tau=0.55, fy=-5e-4, u_max=0.25)
+    s.step(400)
+    u = s.u
+    speed = np.hypot(u[:s.N].astype(np.float64), u[s.N:].astype(np.float64))
+    assert np.isfinite(speed).all()
+    total_diff = total_line = 0
+    for frac in (0.25, 0.5):
+        iso = float(np.quantile(speed[speed > 0], frac))
+        for (w, h), b in (((160, 96), (0, 160, 0, 96)), ((480, 288), (0, 160, 0, 96)), ((64, 40), (0, 160, 0, 96)),
+                          ((300, 200), (20, 130, 10, 80)), ((97, 61), (40, 160, 0, 50))):
+            got = s.viz_isoline(E.FIELD_U, iso, w, h, b)
+            ref = O.ref_cuda_isoline(u, s.nx, s.ny, prec, iso, w, h, b)
+            line = int((ref != 0).sum())
+            diff = int((got != ref).sum())
+            assert line > 0
+            total_line += line
+            total_diff += diff
+            assert diff <= max(4, 0.005 * line), (iso, w, h, b, diff, line)
+    print(f"iso-line pixels differing from the reference kernel: {total_diff} of {total_line}")
+    s.close()

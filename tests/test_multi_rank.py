@@ -62,7 +62,7 @@ def test_reference_arm_under_torchrun_two_ranks():
     port = _free_port()
     cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", "--nproc-per-node", "2",
            "--master-addr", "127.0.0.1", "--master-port", str(port), "bench.py", "--impl", "reference", "--gpus",
-           "2", "--steps", "1", "--warmup", "1", "--ref-lattice-steps", "2"]
+           "2", "--steps", "1", "--warmup", "1", "--lattice-steps", "2"]
     r = subprocess.run(cmd, cwd=ROOT, capture_output=True, text=True, timeout=600)
     assert r.returncode == 0, r.stderr[-2000:]
     lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
