@@ -41,8 +41,12 @@ constexpr int kBatchMaxThreads = 1024;  // CTA sizes 256, 512 or 1024 (autotuned
 #ifndef FLB_BATCH_MIN_BLOCKS
 #define FLB_BATCH_MIN_BLOCKS 2  // two 1024-thread CTAs per SM: at most 32 registers
 #endif
-// the vector data path: CTAs of at most 512 threads, two per SM (64 registers)
+// the vector data path: CTAs of at most 512 threads, FLB_BATCH_VEC_MIN_BLOCKS
+// per SM (two: 64 registers)
 constexpr int kBatchVecMaxThreads = 512;
+#ifndef FLB_BATCH_VEC_MIN_BLOCKS
+#define FLB_BATCH_VEC_MIN_BLOCKS 2
+#endif
 constexpr uint32_t kVecCells = 4;  // cells per thread on the vector path
 
 // A case of the batch.  Its rows are stored kVecCells-aligned: row y starts at
@@ -273,15 +277,11 @@ __device__ __forceinline__ void batch_vec(const KParams& p, uint32_t sx, uint32_
 // 128 on the vector path), warp k the segments k, k + nw, k + 2 nw, ... (nw
 // warps in the group); a warp starts at row y, segment s.  The case (in
 // shared memory) is re-read per item rather than held in registers.
-template <bool HW, bool FU, bool ODD, bool WM, bool VEC>
-__device__ __noinline__ void batch_step(const BatchCase& c, uint32_t y, uint32_t s, uint32_t lane) {
+template <bool HW, bool FU, bool ODD, bool WM>
+__device__ __noinline__ void batch_step_cells(const BatchCase& c, uint32_t y, uint32_t s, uint32_t lane) {
   while (y < c.kp.ny) {
-    if constexpr (VEC) {
-      batch_vec<HW, FU, ODD, WM>(c.kp, c.sx, s * (32u * kVecCells) + lane * kVecCells, y, lane);
-    } else {
-      const uint32_t x = s * 32u + lane;
-      if (x < c.kp.nx) batch_cell<HW, FU, ODD, WM>(c.kp, c.sx, x, y);
-    }
+    const uint32_t x = s * 32u + lane;
+    if (x < c.kp.nx) batch_cell<HW, FU, ODD, WM>(c.kp, c.sx, x, y);
     s += c.ds;
     y += c.dy;
     if (s >= c.nseg) {
@@ -289,6 +289,23 @@ __device__ __noinline__ void batch_step(const BatchCase& c, uint32_t y, uint32_t
       y++;
     }
   }
+}
+template <bool HW, bool FU, bool ODD, bool WM>
+__device__ __noinline__ void batch_step_vec(const BatchCase& c, uint32_t y, uint32_t s, uint32_t lane) {
+  while (y < c.kp.ny) {
+    batch_vec<HW, FU, ODD, WM>(c.kp, c.sx, s * (32u * kVecCells) + lane * kVecCells, y, lane);
+    s += c.ds;
+    y += c.dy;
+    if (s >= c.nseg) {
+      s -= c.nseg;
+      y++;
+    }
+  }
+}
+template <bool HW, bool FU, bool ODD, bool WM, bool VEC>
+__device__ __forceinline__ void batch_step(const BatchCase& c, uint32_t y, uint32_t s, uint32_t lane) {
+  if constexpr (VEC) batch_step_vec<HW, FU, ODD, WM>(c, y, s, lane);
+  else batch_step_cells<HW, FU, ODD, WM>(c, y, s, lane);
 }
 
 // Team barrier (FLB_BATCH_TEAM): the CTAs of a team meet in global memory.
@@ -355,7 +372,8 @@ __device__ __forceinline__ bool team_sync(TeamSync* ts, uint32_t n, uint32_t& ge
 // VEC: the vector data path (kVecCells cells per thread, at most
 // kBatchVecMaxThreads threads per CTA).
 template <bool HW, bool FU, bool TEAM, bool VEC>
-__global__ void __launch_bounds__(VEC ? kBatchVecMaxThreads : kBatchMaxThreads, FLB_BATCH_MIN_BLOCKS)
+__global__ void __launch_bounds__(VEC ? kBatchVecMaxThreads : kBatchMaxThreads,
+                                  VEC ? FLB_BATCH_VEC_MIN_BLOCKS : FLB_BATCH_MIN_BLOCKS)
     k_batch(const BatchCase* __restrict__ cases, const uint32_t* __restrict__ order, const uint32_t* __restrict__ start,
             const uint32_t* __restrict__ tdev, uint32_t steps, int wm_last, uint32_t group, TeamSync* sync,
             uint32_t* err, uint32_t wait_limit, uint32_t skip_rank) {

@@ -29,8 +29,13 @@ enum Variant { V_F64 = 0, V_F32 = 1, V_F16S = 2, V_F32M32 = 3 };
 
 constexpr int kGraphPairs = 16;  // steps per large graph = 2 * kGraphPairs
 // FLB_STEP_AUTO runs the free-surface step as one persistent kernel on grids of
-// up to this many super-tiles (where every pass is one latency-bound round)
-constexpr uint32_t kPersistAutoTiles = 4096;
+// up to this many super-tiles.  Measured on a B200 (2048x512 dam break, 1024
+// super-tiles): 34.8 us per step persistent against 29.3 us for the PDL-chained
+// per-pass kernels.  FS_1 needs 64 registers, so the persistent kernel keeps
+// 1024 threads per SM where the per-pass stream-collide and flag kernels keep
+// 2048, and each of its four grid barriers per step costs about 1.5 us; AUTO
+// therefore runs the per-pass kernels everywhere (0 super-tiles).
+constexpr uint32_t kPersistAutoTiles = 0;
 constexpr uint32_t kPersistWaitLimit = 1u << 22;  // barrier polls before the persistent step gives up
 
 struct GraphSlot {

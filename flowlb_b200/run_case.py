@@ -46,6 +46,8 @@ def main(argv=None):
     ap.add_argument("--profile", action="store_true", help="per-pass CUDA-event times")
     ap.add_argument("--u-max", type=float, default=0.0, help="velocity limiter (0 = off)")
     ap.add_argument("--arithmetic", default="fused", choices=["fused", "reference"])
+    ap.add_argument("--step-mode", default="auto", choices=["auto", "kernels", "persistent"],
+                    help="free-surface step form (flb_set_step_mode)")
     ap.add_argument("--files", default="", help="folder with Geometry.txt and OptionsCalc.txt")
     ap.add_argument("--out", default="", help="where --files writes results_<k>/ (default: the folder itself)")
     a = ap.parse_args(argv)
@@ -65,10 +67,13 @@ def main(argv=None):
                  fs_mode=E.FS_CONSERVATIVE if a.fs_mode == "conservative" else E.FS_REFERENCE,
                  kernel_variant=a.kernel_variant, u_max=a.u_max,
                  arithmetic=E.ARITH_FUSED if a.arithmetic == "fused" else E.ARITH_REFERENCE)
+    if case.free_surface:
+        s.set_step_mode({"auto": E.STEP_AUTO, "kernels": E.STEP_KERNELS, "persistent": E.STEP_PERSISTENT}[a.step_mode])
     m0 = s.total_mass()
     s.step(a.warmup)
     s.sync()
-    out = {"case": case.name, "cells": case.cells, "precision": a.precision, "steps": a.steps}
+    out = {"case": case.name, "cells": case.cells, "precision": a.precision, "steps": a.steps,
+           "step_form": "persistent kernel" if case.free_surface and s.persistent else "per-pass kernels"}
     if a.profile:
         passes = s.profile_steps(a.steps)
         total = sum(passes.values())

@@ -156,8 +156,10 @@ FLB_API flb_status flb_get_time(flb_handle h, uint64_t* t);
  * one per SM) runs all its steps, the passes separated by grid barriers in
  * global memory; a barrier wait gives up after a bounded number of polls
  * (flb_set_wait_limit) and the next flb_sync or flb_read_field returns
- * FLB_ERR_CUDA.  FLB_STEP_AUTO (default): persistent on grids of up to 4096
- * 128x8 super-tiles, per-pass kernels above.  Both give identical results.
+ * FLB_ERR_CUDA.  FLB_STEP_AUTO (default): the per-pass kernels, measured
+ * faster on a B200 (the persistent kernel holds 1024 threads per SM, the
+ * per-pass stream-collide and flag kernels 2048).  Both give identical
+ * results.
  * The persistent form needs a free-surface case without inlet/outlet cells
  * (FLB_ERR_UNSUPPORTED otherwise); single-phase cases ignore the mode.  With
  * FLB_PERSIST_SKIP_ARRIVAL=1 in the environment (failure injection for
