@@ -82,9 +82,9 @@ __device__ __forceinline__ bool same_bits(double a, double b) {
 __device__ __forceinline__ bool same_bits(float a, float b) { return __float_as_uint(a) == __float_as_uint(b); }
 
 // Free-surface steps work on super-tiles of kSTW x kSTH cells.  Only the
-// super-tiles a pass can change are visited: the flag pass records which
-// super-tiles hold fluid or interface cells, a small kernel compacts them into
-// lists (k_build_lists), and the next step's passes loop over the lists in a
+// super-tiles a pass can change are visited: the flag pass, as it finishes a
+// super-tile, appends to the next step's lists the super-tiles that step must
+// visit (NextLists), and the next step's passes loop over the lists in a
 // persistent grid.  all = 1 visits every super-tile (first step after the
 // state was set from outside).
 constexpr uint32_t kSTW = 128, kSTH = 8;
@@ -127,16 +127,35 @@ inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, c
   return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
-// What the list build of a step needs (k_build_lists).
-struct ListBuild {
-  uint32_t* nz_prev;
-  uint32_t nsx, nsy;
-  int prev_unknown;
+// Where the flag pass of the step at t appends the super-tiles of step t+1:
+// FS_1 and stream-collide visit those holding fluid or interface cells
+// (list_sc); the flag pass also visits a neighbour of such a super-tile when
+// one of those cells lies within the stencil chain's reach of their shared
+// edge or corner, and, once more, those that held such cells a step earlier
+// (list_fs; bits marks the super-tiles already in it, so each is listed once).
+// The lengths and the marks start at zero: FS_1 of the same step clears them
+// (ListClear), after the previous step's passes have finished reading that
+// parity's lists.
+struct NextLists {
   uint32_t* list_sc;
   uint32_t* list_fs;
-  uint32_t* counts;        // [2]: lengths of list_sc and list_fs, zero on entry
-  uint32_t* other_counts;  // [2]: the other parity's lengths, zeroed by the build
+  uint32_t* counts;  // [2]: lengths of list_sc and list_fs
+  uint32_t* bits;    // (ntiles + 31) / 32 words
+  uint32_t nsx, nsy;
 };
+struct ListClear {
+  uint32_t* counts;  // [2]
+  uint32_t* bits;
+  uint32_t nwords;
+};
+
+// FS_1's first block clears the lengths and marks the flag pass of the same
+// step appends to (called after pdl_wait).
+__device__ __forceinline__ void clear_next_lists(const ListClear& lc) {
+  if (blockIdx.x != 0 || !lc.counts) return;
+  if (threadIdx.x < 2) lc.counts[threadIdx.x] = 0u;
+  for (uint32_t i = threadIdx.x; i < lc.nwords; i += blockDim.x) lc.bits[i] = 0u;
+}
 
 // What the persistent free-surface step (k_fsp.cu) needs besides the step
 // parameters: the lists and their lengths of both parities (read by the step
@@ -145,16 +164,17 @@ struct ListBuild {
 struct FspArgs {
   uint32_t* list[2][2];  // [parity][0: FS_1 and stream-collide, 1: flag pass]
   uint32_t* lcount;      // [parity][2] list lengths
+  uint32_t* lbits;       // [parity][nwords] marks of the flag-pass lists
+  uint32_t nwords;
   uint32_t* nz;
-  uint32_t* nz_prev;
   uint32_t nsx, nsy;
-  int prev_unknown;      // the flag pass visits every super-tile (thin last super-tiles)
+  int fs_all;            // the flag pass visits every super-tile (thin last super-tiles)
   uint32_t* bar;         // grid barrier arrivals, zeroed before each launch
   uint32_t* err;         // set when a barrier wait gave up
   uint32_t steps;        // even: the run starts at an even t with flag buffer 0 current
   uint32_t wait_limit;   // polls before a barrier wait gives up
   uint32_t skip_cta;     // failure injection: this CTA never arrives (0xffffffff: none)
-  uint64_t* trace;       // null, or 4*steps+1 slots: CTA 0's exit time of each barrier (ns)
+  uint64_t* trace;       // null, or 3*steps+1 slots: CTA 0's exit time of each barrier (ns)
 };
 
 // A list holds at most ntiles entries; the length is clamped so that no state

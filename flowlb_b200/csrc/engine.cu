@@ -65,11 +65,15 @@ struct flb_engine {
   bool trust = false;
   // free surface: super-tile activity bitmaps and the lists of the next step
   uint32_t nsx = 0, nsy = 0, ntiles = 0;
-  uint32_t* d_nz = nullptr;       // super-tile holds fluid/interface after the last flag pass
-  uint32_t* d_nz_prev = nullptr;  // the same one step earlier
+  uint32_t* d_nz = nullptr;       // super-tile activity words of the last flag pass that visited each
+  uint32_t* d_lbits = nullptr;    // [step parity][nwords]: marks of the flag-pass lists
+  uint32_t nwords = 0;
   uint32_t* d_list[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [step parity][0 FS_1/SC, 1 flag pass]
   uint32_t* d_lcount = nullptr;   // [step parity][2] list lengths
   bool lists_valid = false;       // lists of the current parity were built by the previous step
+  // the previous step visited every super-tile: this step's flag pass must
+  // too (the activity words of two steps back are unknown)
+  bool fs_all_next = false;
   bool thin_tiles = false;        // a last super-tile column or row narrower than the flag pass's reach
   uint32_t grid_sc = 0, grid_fs1 = 0, grid_fs234 = 0;
   // persistent free-surface step (k_fsp.cu): requested mode, resolved path,
@@ -152,11 +156,11 @@ struct Ops {
   static void sc_list(flb_engine* h, uint32_t odd, const TileList& tl) {
     launch_sc_list<S, C, M>(h->kp, h->stream, odd, h->hw, tl, h->grid_sc, h->fused);
   }
-  static void fs1(flb_engine* h, uint32_t odd, const TileList& tl) {
-    launch_fs1<S, C, M>(h->kp, h->stream, odd, h->hw, tl, h->grid_fs1);
+  static void fs1(flb_engine* h, uint32_t odd, const TileList& tl, const ListClear& lc) {
+    launch_fs1<S, C, M>(h->kp, h->stream, odd, h->hw, tl, h->grid_fs1, lc);
   }
-  static int fs234(flb_engine* h, uint32_t odd, const TileList& tl, const ListBuild& lb) {
-    return launch_fs234<S, C, M>(h->kp, h->stream, odd, tl, h->grid_fs234, h->d_nz, lb);
+  static int fs234(flb_engine* h, uint32_t odd, const TileList& tl, const NextLists& nl) {
+    return launch_fs234<S, C, M>(h->kp, h->stream, odd, tl, h->grid_fs234, h->d_nz, nl);
   }
   static void grids(flb_engine* h, int nsm) {
     h->grid_sc = (uint32_t)(nsm * sc_list_blocks_per_sm<S, C, M>());
@@ -236,23 +240,29 @@ struct FsLists {
   bool all;
 };
 
+// A live cell can reach past a super-tile narrower than 3 cells into the one
+// beyond it; such grids visit every super-tile in the flag pass.
 FsLists fs_lists(flb_engine* h, uint64_t t) {
   const int lp = (int)(t & 1u);
   FsLists L;
   L.all = !h->lists_valid;
+  const bool fs_all = L.all || h->fs_all_next || h->thin_tiles;
   L.sc = TileList{h->d_list[lp][0], h->d_lcount + 2 * lp, h->ntiles, h->nsx, L.all ? 1 : 0};
-  L.fs = TileList{h->d_list[lp][1], h->d_lcount + 2 * lp + 1, h->ntiles, h->nsx, L.all ? 1 : 0};
+  L.fs = TileList{h->d_list[lp][1], h->d_lcount + 2 * lp + 1, h->ntiles, h->nsx, fs_all ? 1 : 0};
   L.next_count = h->d_lcount + 2 * (lp ^ 1);
   return L;
 }
 
-// The list build of the step at t: the lists of t+1 and their lengths.
-ListBuild list_build(flb_engine* h, uint64_t t, const FsLists& L) {
+// The next step's lists, which the flag pass of the step at t appends to
+// and FS_1 of that step clears.
+NextLists next_lists(flb_engine* h, uint64_t t) {
   const int np = (int)((t + 1) & 1u);
-  // a live cell can reach past a super-tile narrower than 3 cells into the
-  // one beyond it; such grids visit every super-tile in the flag pass
-  return ListBuild{h->d_nz_prev, h->nsx, h->nsy, (L.all || h->thin_tiles) ? 1 : 0, h->d_list[np][0],
-                   h->d_list[np][1], L.next_count, h->d_lcount + 2 * (1 - np)};
+  return NextLists{h->d_list[np][0], h->d_list[np][1], h->d_lcount + 2 * np, h->d_lbits + (size_t)np * h->nwords,
+                   h->nsx, h->nsy};
+}
+ListClear list_clear(flb_engine* h, uint64_t t) {
+  const NextLists nl = next_lists(h, t);
+  return ListClear{nl.counts, nl.bits, h->nwords};
 }
 
 // Issues the passes of one time step at t on the stream.
@@ -267,17 +277,14 @@ uint64_t issue_step(flb_engine* h, uint64_t t, bool write_macro) {
   if (h->fs) {
     h->kp.trust_prev = h->trust ? 1 : 0;
     const FsLists L = fs_lists(h, t);
-    const ListBuild lb = list_build(h, t, L);
-    // the first step after the state was written from outside: the list
-    // lengths may be stale, and each build appends to zeroed ones
-    if (L.all) cudaMemsetAsync(h->d_lcount, 0, 4 * sizeof(uint32_t), h->stream);
     dispatch(h, [&](auto ops) {
-      ops.fs1(h, odd, L.sc);
+      ops.fs1(h, odd, L.sc, list_clear(h, t));
       ops.sc_list(h, odd, L.sc);
-      k = 2 + (uint64_t)ops.fs234(h, odd, L.fs, lb);
+      k = 2 + (uint64_t)ops.fs234(h, odd, L.fs, next_lists(h, t));
     });
     h->cur ^= 1;
     h->trust = true;
+    h->fs_all_next = L.all;
     h->lists_valid = true;
     refresh_params(h);
   } else {
@@ -315,11 +322,12 @@ flb_status issue_persist(flb_engine* h, int pairs, uint64_t* trace = nullptr) {
   for (int q = 0; q < 2; q++)
     for (int k = 0; k < 2; k++) a.list[q][k] = h->d_list[q][k];
   a.lcount = h->d_lcount;
+  a.lbits = h->d_lbits;
+  a.nwords = h->nwords;
   a.nz = h->d_nz;
-  a.nz_prev = h->d_nz_prev;
   a.nsx = h->nsx;
   a.nsy = h->nsy;
-  a.prev_unknown = h->thin_tiles ? 1 : 0;
+  a.fs_all = h->thin_tiles ? 1 : 0;
   a.bar = h->d_bar;
   a.err = h->d_perr;
   a.steps = 2u * (uint32_t)pairs;
@@ -405,7 +413,7 @@ void free_all(flb_engine* h) {
   void* bufs[] = {h->d_f,          h->d_rho,         h->d_u,           h->d_flags[0],    h->d_flags[1],
                   h->d_geo,        h->d_nbmask,      h->d_mass,        h->d_excess,      h->d_phi,
                   h->d_recon,      h->d_recon_mask,  h->d_rho_snap,    h->d_u_snap,      h->d_partial,
-                  h->d_scalar,     h->d_counts,      h->d_nz,          h->d_nz_prev,     h->d_list[0][0],
+                  h->d_scalar,     h->d_counts,      h->d_nz,          h->d_lbits,       h->d_list[0][0],
                   h->d_list[0][1], h->d_list[1][0],  h->d_list[1][1],  h->d_lcount,     h->d_tstep,
                   h->d_plain,      h->d_bar,         h->d_perr};
   for (void* p : bufs)
@@ -479,6 +487,7 @@ flb_status initialise(flb_engine* h) {
   refresh_plain(h);
   h->trust = true;  // flags[1] = flags[0] and the initial fields satisfy the skip invariants
   h->lists_valid = false;
+  h->fs_all_next = false;
   h->broken = false;
   FLB_CUDA(h, cudaGetLastError());
   return FLB_OK;
@@ -654,6 +663,7 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
   h->nsy = (h->ny + kSTH - 1) / kSTH;
   h->thin_tiles = (h->nx % kSTW != 0 && h->nx % kSTW < 3) || (h->ny % kSTH != 0 && h->ny % kSTH < 3);
   h->ntiles = h->nsx * h->nsy;
+  h->nwords = (h->ntiles + 31u) / 32u;
   const uint64_t tiles = h->ntiles;
   Alloc allocs[] = {
       {&h->d_f, 9 * N * h->s_size, true},
@@ -676,7 +686,7 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
       {(void**)&h->d_tstep, 2 * sizeof(uint32_t), true},
       {(void**)&h->d_plain, (((size_t)N + 3) / 4 + 31) / 32 * sizeof(uint32_t), !h->fs},
       {(void**)&h->d_nz, tiles * sizeof(uint32_t), h->fs},
-      {(void**)&h->d_nz_prev, tiles * sizeof(uint32_t), h->fs},
+      {(void**)&h->d_lbits, 2 * (size_t)((tiles + 31) / 32) * sizeof(uint32_t), h->fs},
       {(void**)&h->d_list[0][0], tiles * sizeof(uint32_t), h->fs},
       {(void**)&h->d_list[0][1], tiles * sizeof(uint32_t), h->fs},
       {(void**)&h->d_list[1][0], tiles * sizeof(uint32_t), h->fs},
@@ -777,7 +787,7 @@ FLB_API flb_status flb_step(flb_handle h, uint64_t n) {
     // the graphs run to the end of the call)
     const uint64_t big = 2ull * kGraphPairs;
     const uint64_t tail = h->fs ? 0u : 1u;
-    if (h->fs && (!h->trust || !h->lists_valid)) {
+    if (h->fs && (!h->trust || !h->lists_valid || h->fs_all_next)) {
       // first step after the state was written from outside: no write skipping
       h->launches += issue_step(h, h->t, remaining == 1);
       h->t += 1;
@@ -1105,11 +1115,10 @@ FLB_API flb_status flb_run_pass(flb_handle h, int pass) {
       if (h->fs) ops.sc_list(h, odd, all);
       else ops.sc(h, odd, true);
     } else if (pass == 1) {
-      ops.fs1(h, odd, all);
+      ops.fs1(h, odd, all, list_clear(h, h->t));
     } else {
-      // the lists it builds go unused: lists_valid is false
-      cudaMemsetAsync(h->d_lcount, 0, 4 * sizeof(uint32_t), h->stream);
-      k = (uint64_t)ops.fs234(h, odd, all, list_build(h, h->t, fs_lists(h, h->t)));
+      // the lists it appends to go unused: lists_valid is false
+      k = (uint64_t)ops.fs234(h, odd, all, next_lists(h, h->t));
     }
     if (pass == 1 && recon) ops.apply_recon(h, odd);
   });
@@ -1140,19 +1149,18 @@ FLB_API flb_status flb_profile_steps(flb_handle h, uint64_t n, double pass_ms[3]
     if (h->fs) {
       h->kp.trust_prev = h->trust ? 1 : 0;
       const FsLists L = fs_lists(h, h->t);
-      const ListBuild lb = list_build(h, h->t, L);
-      if (L.all) cudaMemsetAsync(h->d_lcount, 0, 4 * sizeof(uint32_t), h->stream);
       cudaEventRecord(ev[0], h->stream);
-      dispatch(h, [&](auto ops) { ops.fs1(h, odd, L.sc); });
+      dispatch(h, [&](auto ops) { ops.fs1(h, odd, L.sc, list_clear(h, h->t)); });
       cudaEventRecord(ev[1], h->stream);
       dispatch(h, [&](auto ops) { ops.sc_list(h, odd, L.sc); });
       cudaEventRecord(ev[2], h->stream);
       int kf = 0;
-      dispatch(h, [&](auto ops) { kf = ops.fs234(h, odd, L.fs, lb); });
+      dispatch(h, [&](auto ops) { kf = ops.fs234(h, odd, L.fs, next_lists(h, h->t)); });
       cudaEventRecord(ev[3], h->stream);
       h->launches += 2 + (uint64_t)kf;
       h->cur ^= 1;
       h->trust = true;
+      h->fs_all_next = L.all;
       h->lists_valid = true;
     } else {
       cudaEventRecord(ev[1], h->stream);
@@ -1180,22 +1188,22 @@ FLB_API flb_status flb_profile_steps(flb_handle h, uint64_t n, double pass_ms[3]
   return st;
 }
 
-FLB_API flb_status flb_profile_phases(flb_handle h, uint64_t n, double phase_ms[4]) {
+FLB_API flb_status flb_profile_phases(flb_handle h, uint64_t n, double phase_ms[3]) {
   if (!h || !phase_ms) return FLB_ERR_INVALID_ARGUMENT;
   if (!h->fs || h->grid_persist == 0)
     return fail(h, FLB_ERR_UNSUPPORTED, "phase timing needs the persistent free-surface step");
   if (h->broken) return fail(h, FLB_ERR_CUDA, "call flb_reset first");
   DeviceGuard guard(h->device);
-  for (int k = 0; k < 4; k++) phase_ms[k] = 0.0;
+  for (int k = 0; k < 3; k++) phase_ms[k] = 0.0;
   // steady state from an even t: per-pass steps until then
-  while (!h->trust || !h->lists_valid || (h->t & 1u)) {
+  while (!h->trust || !h->lists_valid || h->fs_all_next || (h->t & 1u)) {
     h->launches += issue_step(h, h->t, false);
     h->t += 1;
   }
   const uint64_t pairs_total = (n + 1) / 2;
   const int per = kGraphPairs;
   uint64_t* d_trace = nullptr;
-  const size_t slots = 8u * per + 1u;
+  const size_t slots = 6u * per + 1u;
   FLB_CUDA(h, cudaMallocAsync((void**)&d_trace, slots * sizeof(uint64_t), h->stream));
   std::vector<uint64_t> tr(slots);
   flb_status st = FLB_OK;
@@ -1205,7 +1213,7 @@ FLB_API flb_status flb_profile_phases(flb_handle h, uint64_t n, double phase_ms[
     if (st != FLB_OK) break;
     h->launches += 1;
     h->t += 2u * (uint64_t)pairs;
-    cudaError_t e = cudaMemcpyAsync(tr.data(), d_trace, (8u * pairs + 1u) * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+    cudaError_t e = cudaMemcpyAsync(tr.data(), d_trace, (6u * pairs + 1u) * sizeof(uint64_t), cudaMemcpyDeviceToHost,
                                     h->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
     if (e != cudaSuccess) {
@@ -1213,7 +1221,7 @@ FLB_API flb_status flb_profile_phases(flb_handle h, uint64_t n, double phase_ms[
       break;
     }
     st = check_persist(h);
-    for (int b = 1; b <= 8 * pairs && st == FLB_OK; b++) phase_ms[(b - 1) % 4] += (double)(tr[b] - tr[b - 1]) * 1e-6;
+    for (int b = 1; b <= 6 * pairs && st == FLB_OK; b++) phase_ms[(b - 1) % 3] += (double)(tr[b] - tr[b - 1]) * 1e-6;
   }
   cudaFreeAsync(d_trace, h->stream);
   cudaStreamSynchronize(h->stream);

@@ -451,37 +451,57 @@ __device__ __forceinline__ uint32_t activity(int lx, int ly, int wact, int hact)
          ((uint32_t)(d && l) << edge_bit(-1, -1));
 }
 
-// Whether super-tile t is visited next step by stream-collide and FS_1 (sc:
-// it holds fluid or interface cells) and by the flag pass (fs: it does, or a
-// neighbour holds such a cell within reach of it, or it did a step earlier);
-// updates nz_prev[t].
-__device__ __forceinline__ void list_flags(const uint32_t* nz, uint32_t* nz_prev, uint32_t nsx, uint32_t nsy,
-                                           int prev_unknown, uint32_t t, bool& sc, bool& fs) {
-  const uint32_t sx = t % nsx, sy = t / nsx;
-  const uint32_t own = __ldcg(nz + t) & 1u;
-  bool near = false;
-#pragma unroll
-  for (int dy = -1; dy <= 1; dy++)
-#pragma unroll
-    for (int dx = -1; dx <= 1; dx++) {
-      if (!dx && !dy) continue;
-      const uint32_t xx = (sx + nsx + dx) % nsx, yy = (sy + nsy + dy) % nsy;
-      near |= (__ldcg(nz + xx + yy * nsx) >> edge_bit(-dx, -dy)) & 1u;  // its edge facing t
-    }
-  sc = own != 0;
-  fs = own || near || prev_unknown || nz_prev[t] != 0;
-  nz_prev[t] = own;
+// Appends super-tile t to the next step's lists (NextLists), with warp 0 of
+// the block (every lane calls it): t itself when it holds fluid or interface
+// cells now (m bit 0: both lists) or held some after the previous step (old
+// bit 0: the flag-pass list), and the neighbour in the direction of every set
+// edge bit of m (the flag-pass list).  A super-tile is added to the flag-pass
+// list once (the first to set its mark adds it).  The lengths never pass the
+// super-tile count, whatever the state of the marks.
+__device__ __forceinline__ void append_next(const NextLists& nl, uint32_t t, uint32_t m, uint32_t old,
+                                            uint32_t lane) {
+  constexpr uint32_t kNone = 0xffffffffu;
+  const uint32_t T = nl.nsx * nl.nsy;
+  uint32_t cand = kNone;
+  if (lane == 0) {
+    if ((m | old) & 1u) cand = t;
+  } else if (lane <= 8u && ((m >> lane) & 1u)) {
+    // edge_bit: 1 +x, 2 -x, 3 +y, 4 -y, 5 +x+y, 6 -x+y, 7 +x-y, 8 -x-y
+    const int dx = (lane == 1 || lane == 5 || lane == 7) ? 1 : (lane == 2 || lane == 6 || lane == 8) ? -1 : 0;
+    const int dy = (lane == 3 || lane == 5 || lane == 6) ? 1 : (lane == 4 || lane == 7 || lane == 8) ? -1 : 0;
+    const uint32_t sx = t % nl.nsx, sy = t / nl.nsx;
+    const uint32_t xx = dx > 0 ? (sx + 1u == nl.nsx ? 0u : sx + 1u) : dx < 0 ? (sx == 0u ? nl.nsx - 1u : sx - 1u) : sx;
+    const uint32_t yy = dy > 0 ? (sy + 1u == nl.nsy ? 0u : sy + 1u) : dy < 0 ? (sy == 0u ? nl.nsy - 1u : sy - 1u) : sy;
+    cand = xx + yy * nl.nsx;
+  }
+  bool add_fs = false;
+  if (cand != kNone) {
+    const uint32_t bit = 1u << (cand & 31u);
+    add_fs = (atomicOr(nl.bits + (cand >> 5), bit) & bit) == 0u;
+  }
+  const uint32_t bfs = __ballot_sync(0xffffffffu, add_fs);
+  const bool add_sc = lane == 0 && (m & 1u);
+  uint32_t base_fs = 0, base_sc = 0;
+  if (lane == 0) {
+    if (bfs) base_fs = atomicAdd(nl.counts + 1, (uint32_t)__popc(bfs));
+    if (add_sc) base_sc = atomicAdd(nl.counts, 1u);
+  }
+  base_fs = __shfl_sync(0xffffffffu, base_fs, 0);
+  if (add_fs) {
+    const uint32_t k = base_fs + __popc(bfs & ((1u << lane) - 1u));
+    if (k < T) nl.list_fs[k] = cand;
+  }
+  if (add_sc && base_sc < T) nl.list_sc[base_sc] = t;
 }
-
-// The listed super-tiles: each block runs the tile pass on the tiles of a
 
 // The flag pass over one super-tile t (its kSTW / TW tiles in turn) with the
 // TW*kTY threads of the block; every thread of the block must call it.
-// Records the super-tile's activity word in nz[t].  wact_sm: one word per
-// warp of the block.
+// Records the super-tile's activity word in nz[t] (whose previous value, the
+// word of the last step, it reads first) and appends to the next step's
+// lists.  wact_sm: one word per warp of the block.
 template <class S, class C, class M, bool ODD, int TW>
 __device__ __forceinline__ void fs234_super_tile(const KParams& p, uint32_t t, uint32_t nsx, uint32_t* nz,
-                                                 FlagMasks<TW>& sm, uint32_t* wact_sm) {
+                                                 const NextLists& nl, FlagMasks<TW>& sm, uint32_t* wact_sm) {
   constexpr int kTX = TW;
   const int tid = threadIdx.x;
   const int sx = (int)(t % nsx), sy = (int)(t / nsx);
@@ -497,10 +517,12 @@ __device__ __forceinline__ void fs234_super_tile(const KParams& p, uint32_t t, u
   act = __reduce_or_sync(0xffffffffu, act);
   if ((tid & 31) == 0) wact_sm[tid >> 5] = act;
   __syncthreads();
-  if (tid == 0) {
+  if (tid < 32) {
     uint32_t m = 0;
     for (int w = 0; w < TW * kTY / 32; w++) m |= wact_sm[w];
-    nz[t] = m;
+    const uint32_t old = __shfl_sync(0xffffffffu, tid == 0 ? __ldcg(nz + t) : 0u, 0);
+    if (tid == 0) nz[t] = m;
+    append_next(nl, t, m, old, (uint32_t)tid);
   }
 }
 

@@ -1,16 +1,17 @@
 // k_fsp.cu -- the free-surface step as one persistent kernel per run of steps.
 //
-// The per-pass step (k_fs.cu, k_sc.cu) launches four kernels per time step:
-// FS_1, stream-collide, the flag pass and the list build.  On grids whose
+// The per-pass step (k_fs.cu, k_sc.cu) launches three kernels per time step:
+// FS_1, stream-collide and the flag pass (which lists the next step's
+// super-tiles).  On grids whose
 // live super-tiles fill the GPU about once (a few hundred on the 2048x512 dam
 // break) every pass is a single round of latency-bound work, and the launch,
 // ramp-up and drain of each kernel are a large part of the step.  Here one
 // cooperative launch runs an even number of steps: every CTA stays resident
 // (one per SM, 1024 threads, one cell per thread of a 128x8 super-tile), and
-// the four passes of each step are separated by grid barriers in global
+// the three passes of each step are separated by grid barriers in global
 // memory instead of kernel boundaries.  The passes themselves are the same
-// device code as the per-pass kernels (fs1_cell, sc_cell, fs234_super_tile,
-// list_flags), so both paths give identical results.
+// device code as the per-pass kernels (fs1_cell, sc_cell, fs234_super_tile),
+// so both paths give identical results.
 //
 // The reference runs five full-grid kernels per step with a host loop around
 // them (src/cuda/runCuda.cu:506-527); nothing there corresponds to the
@@ -93,7 +94,11 @@ __device__ __forceinline__ bool fsp_step(const KParams& p, const FspArgs& a, Fla
   const uint32_t* lfs = a.list[ODD][1];
   // lengths of this step's lists (built by the previous step)
   const uint32_t T = a.nsx * a.nsy;
-  const uint32_t nsc = min(__ldcg(a.lcount + 2 * ODD), T), nfs = min(__ldcg(a.lcount + 2 * ODD + 1), T);
+  const uint32_t nsc = min(__ldcg(a.lcount + 2 * ODD), T);
+  const uint32_t nfs = a.fs_all ? T : min(__ldcg(a.lcount + 2 * ODD + 1), T);
+  // the next step's list lengths and marks, which this step's flag pass
+  // appends to (the previous step's passes have finished reading them)
+  clear_next_lists(ListClear{a.lcount + 2 * (ODD ^ 1), a.lbits + (ODD ^ 1) * a.nwords, a.nwords});
   // FS_1: mass exchange and gas reconstruction
   for (uint32_t i = blockIdx.x; i < nsc; i += G) {
     const uint32_t t = __ldcg(lsc + i);
@@ -108,39 +113,12 @@ __device__ __forceinline__ bool fsp_step(const KParams& p, const FspArgs& a, Fla
     if (y < p.ny && x < p.nx) sc_cell<S, C, M, true, HW, true, ODD, FU>(p, x, y);
   }
   if (!next_barrier(a, nbar, ok)) return false;
-  // FS_2..4: flag stencil, mass / excess / fill level, activity words
+  // FS_2..4: flag stencil, mass / excess / fill level, activity words and the
+  // next step's lists
+  const NextLists nl{a.list[ODD ^ 1][0], a.list[ODD ^ 1][1], a.lcount + 2 * (ODD ^ 1), a.lbits + (ODD ^ 1) * a.nwords,
+                     a.nsx, a.nsy};
   for (uint32_t i = blockIdx.x; i < nfs; i += G)
-    fs234_super_tile<S, C, M, ODD, 128>(p, __ldcg(lfs + i), a.nsx, a.nz, sm, wact_sm);
-  if (!next_barrier(a, nbar, ok)) return false;
-  // list build for the next step (k_build_lists spread over the grid): append
-  // to the next parity's lengths, zeroed by the previous step's build; zero
-  // this parity's, which every CTA read before the first barrier
-  {
-    uint32_t* counts = a.lcount + 2 * (ODD ^ 1);
-    uint32_t* out_sc = a.list[ODD ^ 1][0];
-    uint32_t* out_fs = a.list[ODD ^ 1][1];
-    if (blockIdx.x == 0 && tid == 0) {
-      a.lcount[2 * ODD] = 0;
-      a.lcount[2 * ODD + 1] = 0;
-    }
-    for (uint32_t base = blockIdx.x * blockDim.x; base < T; base += G * blockDim.x) {
-      const uint32_t t = base + tid;
-      bool sc = false, fs = false;
-      if (t < T) list_flags(a.nz, a.nz_prev, a.nsx, a.nsy, a.prev_unknown, t, sc, fs);
-      const uint32_t bsc = __ballot_sync(0xffffffffu, sc), bfs = __ballot_sync(0xffffffffu, fs);
-      uint32_t base_sc = 0, base_fs = 0;
-      if (lane == 0) {
-        if (bsc) base_sc = atomicAdd(&counts[0], (uint32_t)__popc(bsc));
-        if (bfs) base_fs = atomicAdd(&counts[1], (uint32_t)__popc(bfs));
-      }
-      base_sc = __shfl_sync(0xffffffffu, base_sc, 0);
-      base_fs = __shfl_sync(0xffffffffu, base_fs, 0);
-      const uint32_t below = (1u << lane) - 1u;
-      const uint32_t ksc = base_sc + __popc(bsc & below), kfs = base_fs + __popc(bfs & below);
-      if (sc && ksc < T) out_sc[ksc] = t;
-      if (fs && kfs < T) out_fs[kfs] = t;
-    }
-  }
+    fs234_super_tile<S, C, M, ODD, 128>(p, a.fs_all ? i : __ldcg(lfs + i), a.nsx, a.nz, nl, sm, wact_sm);
   return next_barrier(a, nbar, ok);
 }
 

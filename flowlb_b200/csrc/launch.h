@@ -37,14 +37,16 @@ void launch_sc_list(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, c
 template <class S, class C, class M>
 int sc_list_blocks_per_sm();
 
-// FS_1, its reference-mode apply, FS_2..4 (listed super-tiles), and the list build
+// FS_1 (clears the next step's list lengths), its reference-mode apply, and
+// FS_2..4 on listed super-tiles (appends the next step's lists)
 template <class S, class C, class M>
-void launch_fs1(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl, uint32_t grid);
+void launch_fs1(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl, uint32_t grid,
+                const ListClear& lc);
 template <class S, class C, class M>
 void launch_apply_recon(const KParams& kp, cudaStream_t st, uint32_t odd);
 template <class S, class C, class M>
 int launch_fs234(const KParams& kp, cudaStream_t st, uint32_t odd, const TileList& tl, uint32_t grid, uint32_t* nz,
-                 const ListBuild& lb);
+                 const NextLists& nl);
 template <class S, class C, class M>
 int fs_blocks_per_sm(int which);  // 0: FS_1, 1: FS_2..4 on 128-wide tiles, 2: on 32-wide tiles
 

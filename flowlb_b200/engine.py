@@ -379,9 +379,9 @@ class Solver:
         """Runs n steps of the persistent free-surface step with its phases
         timed on the device clock; summed ms per phase (they add up to the
         step time of the production kernel)."""
-        arr = (C.c_double * 4)()
+        arr = (C.c_double * 3)()
         self._check(load_library().flb_profile_phases(self._h, int(n), arr))
-        return dict(fs1=arr[0], stream_collide=arr[1], fs234=arr[2], build=arr[3])
+        return dict(fs1=arr[0], stream_collide=arr[1], fs234=arr[2])
 
     def save_checkpoint(self, path: str):
         self._check(load_library().flb_save_checkpoint(self._h, path.encode()))

@@ -150,8 +150,9 @@ FLB_API flb_status flb_get_time(flb_handle h, uint64_t* t);
 
 /* How the free-surface steps that flb_step replays from CUDA graphs run (no
  * counterpart in the reference, whose host loop launches five kernels per
- * step, runCuda.cu:506-527).  FLB_STEP_KERNELS: FS_1, stream-collide, the
- * flag pass and the list build as four kernels per step.
+ * step, runCuda.cu:506-527).  FLB_STEP_KERNELS: FS_1, stream-collide and
+ * the flag pass (which lists the next step's super-tiles) as three kernels
+ * per step.
  * FLB_STEP_PERSISTENT: one cooperative kernel per graph (every CTA resident,
  * one per SM) runs all its steps, the passes separated by grid barriers in
  * global memory; a barrier wait gives up after a bounded number of polls
@@ -228,12 +229,12 @@ FLB_API flb_status flb_profile_steps(flb_handle h, uint64_t n, double pass_ms[3]
 /* Runs n time steps (rounded up to even, from the next even t in steady
  * state) in the persistent free-surface form with a device clock read by one
  * CTA as it leaves every grid barrier, and returns the summed time of each
- * phase in milliseconds: phase_ms[0] FS_1, [1] stream-collide, [2] FS_2..4,
- * [3] list build, each with the barrier that ends it.  Unlike
+ * phase in milliseconds: phase_ms[0] FS_1, [1] stream-collide, [2] FS_2..4
+ * (with the next step's lists), each with the barrier that ends it.  Unlike
  * flb_profile_steps nothing is serialised: the phases sum to the step time
- * of the production kernel.  Advances t; FLB_ERR_UNSUPPORTED without a
+ * of the persistent kernel.  Advances t; FLB_ERR_UNSUPPORTED without a
  * persistent form. */
-FLB_API flb_status flb_profile_phases(flb_handle h, uint64_t n, double phase_ms[4]);
+FLB_API flb_status flb_profile_phases(flb_handle h, uint64_t n, double phase_ms[3]);
 
 /* Kernels this handle has launched so far (graph replays count each kernel). */
 FLB_API flb_status flb_launch_count(flb_handle h, uint64_t* launches);
