@@ -47,11 +47,11 @@ WORKLOAD = ("free-surface culvert dam break 2048x512, tau 0.55, g_y -5e-5, FP32 
             "half-way walls, conservative free surface, velocity limiter 0.25")
 U_MAX = 0.25  # keeps the surge front stable (plain BGK at tau 0.55 diverges near Mach 0.6)
 KERNEL_OF_PASS = {"stream_collide": "k_sc_list (free-surface stream-collide)", "fs1": "k_fs1 (mass exchange)",
-                  "fs234": "k_fs234 + k_build_lists (flag stencil, mass/fill update, next lists)"}
+                  "fs234": "k_fs234 (flag stencil, mass/fill update, next step's lists)"}
 # each pass's share of the step's device time in the ncu launch list of this
-# workload (gpu__time_duration.sum per launch, a few hundred steps; the flag
-# pass counted with the list build it chains to)
-PASS_SHARE_NCU: dict = {"fs234": 0.486, "fs1": 0.286, "stream_collide": 0.223}
+# workload (gpu__time_duration.sum of ~1000 launches of each of the three
+# kernels of a step; profiles/dam_break_2048x512_launch_list.md)
+PASS_SHARE_NCU: dict = {"fs234": 0.461, "fs1": 0.306, "stream_collide": 0.233}
 # dram__bytes_read.sum + dram__bytes_write.sum per launch (mean of the two
 # parities) from one ncu capture of the workload at steps 300-303
 # (profiles/dam_break_2048x512_launch_list.md); ncu flushes the caches before

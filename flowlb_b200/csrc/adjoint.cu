@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_por_bwd(const AdjParams<T> p, con
                                                        const T* __restrict__ lam_next, T* __restrict__ lam,
                                                        double* __restrict__ sbar, double* __restrict__ gpart,
                                                        const SegDesc* __restrict__ seg, uint32_t j) {
-  __shared__ double red[2][kAdjBlock];
+  __shared__ double red[2][kAdjBlock / 32];
   const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
   double gxb_d = 0.0, gyb_d = 0.0;
   if (x < p.nx) {
@@ -284,20 +284,31 @@ __global__ void __launch_bounds__(kAdjBlock) k_por_bwd(const AdjParams<T> p, con
       gyb_d = (double)gyb;
     }
   }
-  red[0][threadIdx.x] = gxb_d;
-  red[1][threadIdx.x] = gyb_d;
-  __syncthreads();
-  for (uint32_t st = kAdjBlock / 2; st > 0; st >>= 1) {
-    if (threadIdx.x < st) {
-      red[0][threadIdx.x] += red[0][threadIdx.x + st];
-      red[1][threadIdx.x] += red[1][threadIdx.x + st];
-    }
-    __syncthreads();
+  // fixed-order tree: within each warp by shuffles, then over the warps
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    gxb_d += __shfl_down_sync(0xffffffffu, gxb_d, o);
+    gyb_d += __shfl_down_sync(0xffffffffu, gyb_d, o);
   }
-  if (threadIdx.x == 0) {
-    const uint32_t b = blockIdx.x + blockIdx.y * gridDim.x;
-    gpart[2 * b] += red[0][0];
-    gpart[2 * b + 1] += red[1][0];
+  if (lane == 0) {
+    red[0][warp] = gxb_d;
+    red[1][warp] = gyb_d;
+  }
+  __syncthreads();
+  if (warp == 0) {
+    constexpr int kWarps = kAdjBlock / 32;
+    double a0 = lane < (uint32_t)kWarps ? red[0][lane] : 0.0, a1 = lane < (uint32_t)kWarps ? red[1][lane] : 0.0;
+#pragma unroll
+    for (int o = kWarps / 2; o > 0; o >>= 1) {
+      a0 += __shfl_down_sync(0xffffffffu, a0, o);
+      a1 += __shfl_down_sync(0xffffffffu, a1, o);
+    }
+    if (lane == 0) {
+      const uint32_t b = blockIdx.x + blockIdx.y * gridDim.x;
+      gpart[2 * b] += a0;
+      gpart[2 * b + 1] += a1;
+    }
   }
 }
 
