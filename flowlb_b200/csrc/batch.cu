@@ -308,11 +308,13 @@ __device__ __forceinline__ void batch_step(const BatchCase& c, uint32_t y, uint3
   else batch_step_cells<HW, FU, ODD, WM>(c, y, s, lane);
 }
 
-// Team barrier (FLB_BATCH_TEAM): the CTAs of a team meet in global memory.
-// count: arrivals in the current round; gen: rounds completed.  One per team,
-// 128 bytes apart.
+// Team barrier (FLB_BATCH_TEAM): the CTAs of a team meet in global memory on
+// an arrival count, one per team, 128 bytes apart.  The counts are zeroed
+// before every launch and only grow: the r-th barrier of a team in a launch
+// is passed once its count reaches r times the team's size, so an arrival is
+// a single reduction with no reply and no reset is needed between rounds.
 struct TeamSync {
-  uint32_t count, gen, pad[30];
+  uint32_t count, pad[31];
 };
 // polls (about 1 us each) before a wait gives up, unless flb_batch_set_wait_limit set another
 constexpr uint32_t kTeamSpinLimit = 1u << 21;
@@ -324,37 +326,38 @@ __device__ __forceinline__ uint32_t ld_acquire(const uint32_t* a) {
   asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(a) : "memory");
   return v;
 }
+__device__ __forceinline__ void red_release_add(uint32_t* a, uint32_t v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(a), "r"(v) : "memory");
+}
 
 // All CTAs of the team have finished the step (and their writes are visible)
-// when this returns true.  Thread 0 arrives for the CTA; the last arrival
-// resets the count and opens the next round.  A wait longer than `limit`
-// polls, or an error raised elsewhere, sets *err and returns false (the
-// caller then leaves the kernel).  arrive = false (failure injection only)
-// makes this CTA wait without arriving, so the round never completes and
-// every wait of the team runs out.
-__device__ __forceinline__ bool team_sync(TeamSync* ts, uint32_t n, uint32_t& gen, uint32_t* err, int& ok,
-                                          uint32_t limit, bool arrive) {
+// when this returns true: the team's count has reached `target` arrivals.
+// Thread 0 arrives for the CTA (fence, then a release reduction) and polls
+// with acquire loads.  A wait longer than `limit` polls sets *err; a CTA that
+// sees *err set (checked every 64 polls) stops waiting too; either returns
+// false and the caller leaves the kernel.  arrive = false (failure injection
+// only) makes this CTA wait without arriving, so the round never completes
+// and every wait of the team runs out.
+__device__ __forceinline__ bool team_sync(TeamSync* ts, uint32_t target, uint32_t* err, int& ok, uint32_t limit,
+                                          bool arrive) {
   __syncthreads();
   if (threadIdx.x == 0) {
     bool good = true;
     __threadfence();
-    if (arrive && atomicAdd(&ts->count, 1u) == n - 1u) {
-      atomicExch(&ts->count, 0u);
-      __threadfence();
-      atomicAdd(&ts->gen, 1u);
-    } else {
-      uint32_t it = 0;
-      while (ld_acquire(&ts->gen) == gen) {
-        if (++it >= limit || ld_acquire(err) != 0u) {
-          good = false;
-          atomicOr(err, 1u);
-          break;
-        }
-        __nanosleep(64);
+    if (arrive) red_release_add(&ts->count, 1u);
+    uint32_t it = 0;
+    while (ld_acquire(&ts->count) < target) {
+      if (++it >= limit) {
+        good = false;
+        atomicOr(err, 1u);
+        break;
+      }
+      if ((it & 63u) == 0u && ld_acquire(err) != 0u) {
+        good = false;
+        break;
       }
     }
     __threadfence();
-    gen++;
     ok = good;
   }
   __syncthreads();
@@ -384,9 +387,7 @@ __global__ void __launch_bounds__(VEC ? kBatchVecMaxThreads : kBatchMaxThreads,
   const uint32_t warps = blockDim.x >> 5;
   const uint32_t wid = rank * warps + (threadIdx.x >> 5), nw = group * warps;
   const uint32_t lane = threadIdx.x & 31u;
-  uint32_t gen = 0;
-  // before this CTA's first arrival no round of its team can complete
-  if (TEAM && threadIdx.x == 0) gen = ld_acquire(&sync[cid].gen);
+  uint32_t round = 0;  // team barriers passed in this launch
   for (uint32_t k = start[cid]; k < start[cid + 1]; k++) {
     __syncthreads();  // the previous case's parameters are no longer read
     {
@@ -414,7 +415,7 @@ __global__ void __launch_bounds__(VEC ? kBatchVecMaxThreads : kBatchMaxThreads,
         else batch_step<HW, FU, false, false, VEC>(sc, y0, s0, lane);
       }
       if constexpr (TEAM) {
-        if (!team_sync(&sync[cid], group, gen, err, ok, wait_limit, rank != skip_rank)) return;
+        if (!team_sync(&sync[cid], ++round * group, err, ok, wait_limit, rank != skip_rank)) return;
       } else {
         cg::this_cluster().sync();
       }
@@ -656,6 +657,8 @@ flb_status bissue(flb_batch b, uint32_t n, int wm_last, uint32_t skip) {
   }
   cfg.attrs = attr;
   cfg.numAttrs = 1;
+  // the team arrival counts start every launch at zero
+  if (b->team) FLB_BCUDA(b, cudaMemsetAsync(b->d_sync, 0, (size_t)b->clusters * sizeof(TeamSync), b->stream));
   FLB_BCUDA(b, cudaLaunchKernelEx(&cfg, kern, (const BatchCase*)b->d_cases, (const uint32_t*)b->d_order,
                                   (const uint32_t*)b->d_start, (const uint32_t*)b->d_tstep, n, wm_last,
                                   (uint32_t)b->cluster, b->d_sync, b->d_err, b->wait_limit, skip));
@@ -808,11 +811,14 @@ flb_status btune(flb_batch b, uint32_t probe_steps) {
     }
     add_teams(false, threads);
   }
-  // the vector data path: teams, and 8- and 16-CTA clusters at the L2-sized count
+  // the vector data path: teams, one-CTA groups (every case of the batch at
+  // once), and 8- and 16-CTA clusters at the L2-sized count
   for (int threads : {256, 512}) {
-    for (int cs : {8, 16}) {
+    for (int cs : {1, 8, 16}) {
       const int mx = max_clusters(b, cs, threads, true);
-      if (mx > 0) add(false, true, cs, l2_fit, mx, threads);
+      if (mx <= 0) continue;
+      add(false, true, cs, l2_fit, mx, threads);
+      if (cs == 1) add(false, true, cs, mx, mx, threads);
     }
     add_teams(true, threads);
   }
