@@ -48,6 +48,7 @@ struct AdjParams {
   const uint8_t* flags;   // FLUID / WALL
   const uint8_t* srcw;    // bit i-1: the source x - c_i of population i >= 1 is a wall
   const T* s;             // drag coefficient per cell
+  const T* id;            // 1 / (1 + s/2) per cell (k_por_inv_d, whenever s is set)
   T om, omc, kk;          // w, 1 - w, 1 - w/2
   T gx, gy;
   T winv;                 // 1 / W
@@ -101,14 +102,15 @@ __device__ __forceinline__ void gather(const AdjParams<T>& p, const T* __restric
 // instruction sequence; the reverse step would otherwise need ten).
 template <class T>
 struct Cell {
-  T rho, ir, vx, vy, d, id, ux, uy, Fx, Fy, usq, uF;
+  T rho, ir, vx, vy, id, ux, uy, Fx, Fy, usq, uF;
 };
 
-// the rest of the intermediates from rho, v and s
+// the rest of the intermediates from rho, v, s and id = 1 / (1 + s/2), the
+// latter computed once per porosity field by k_por_inv_d with the same
+// operations
 template <class T>
-__device__ __forceinline__ void cell_rest(const AdjParams<T>& p, Cell<T>& c, T s) {
-  c.d = T(1) + T(0.5) * s;
-  c.id = T(1) / c.d;
+__device__ __forceinline__ void cell_rest(const AdjParams<T>& p, Cell<T>& c, T s, T id) {
+  c.id = id;
   c.ux = (c.vx + T(0.5) * p.gx) * c.id;
   c.uy = (c.vy + T(0.5) * p.gy) * c.id;
   c.Fx = c.rho * (p.gx - s * c.ux);
@@ -118,7 +120,7 @@ __device__ __forceinline__ void cell_rest(const AdjParams<T>& p, Cell<T>& c, T s
 }
 
 template <class T>
-__device__ __forceinline__ Cell<T> cell_state(const AdjParams<T>& p, const T* f, T s) {
+__device__ __forceinline__ Cell<T> cell_state(const AdjParams<T>& p, const T* f, T s, T id) {
   Cell<T> c;
   c.rho = f[0] + f[1] + f[2] + f[3] + f[4] + f[5] + f[6] + f[7] + f[8];
   const T jx = f[1] - f[2] + f[5] - f[6] + f[7] - f[8];
@@ -126,7 +128,7 @@ __device__ __forceinline__ Cell<T> cell_state(const AdjParams<T>& p, const T* f,
   c.ir = T(1) / c.rho;
   c.vx = jx * c.ir;
   c.vy = jy * c.ir;
-  cell_rest(p, c, s);
+  cell_rest(p, c, s, id);
   return c;
 }
 
@@ -151,7 +153,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_por_fwd(const AdjParams<T> p, con
   T f[9];
   gather(p, fin, idx, p.srcw[idx], nb, f);
   const T s = p.s[idx];
-  const Cell<T> c = cell_state(p, f, s);
+  const Cell<T> c = cell_state(p, f, s, p.id[idx]);
   if (mac) {  // the backward step's inputs: rho and v = j / rho
     mac[idx] = c.rho;
     mac[N + idx] = c.vx;
@@ -202,7 +204,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_por_bwd(const AdjParams<T> p, con
       c.ir = T(1) / c.rho;
       c.vx = mac[N + idx];
       c.vy = mac[2 * N + idx];
-      cell_rest(p, c, s);
+      cell_rest(p, c, s, p.id[idx]);
       const T base = T(1) - T(1.5) * c.usq;
       T fb[9];
       const T m0 = lam_next[idx];
@@ -312,6 +314,13 @@ __global__ void __launch_bounds__(kAdjBlock) k_por_bwd(const AdjParams<T> p, con
   }
 }
 
+// id = 1 / (1 + s/2) per cell
+template <class T>
+__global__ void k_por_inv_d(const T* __restrict__ s, T* __restrict__ id, uint32_t N) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < N) id[k] = T(1) / (T(1) + T(0.5) * s[k]);
+}
+
 // state = w_i (rest), also used to reset the adjoint to zero (zero = 1)
 template <class T>
 __global__ void k_por_fill(T* f, uint32_t N, int zero) {
@@ -353,6 +362,7 @@ struct flb_adjoint_s {
   bool own_stream = false;
   uint8_t *d_flags = nullptr, *d_srcw = nullptr;
   void* d_s = nullptr;
+  void* d_id = nullptr;
   void* d_state[2] = {nullptr, nullptr};
   void* d_ckpt = nullptr;  // nseg states
   void* d_tape = nullptr;  // 2 x K x (rho, v_x, v_y)
@@ -409,6 +419,7 @@ AdjParams<T> params(flb_adjoint a) {
   p.flags = a->d_flags;
   p.srcw = a->d_srcw;
   p.s = static_cast<const T*>(a->d_s);
+  p.id = static_cast<const T*>(a->d_id);
   const T tau = (T)a->d.tau;
   p.om = T(1) / tau;
   p.omc = T(1) - p.om;
@@ -431,7 +442,7 @@ void adrop_graphs(flb_adjoint a) {
 
 void afree(flb_adjoint a) {
   adrop_graphs(a);
-  void* bufs[] = {a->d_flags, a->d_srcw,   a->d_s,    a->d_state[0], a->d_state[1], a->d_ckpt, a->d_tape,
+  void* bufs[] = {a->d_flags, a->d_srcw,   a->d_s,    a->d_id,       a->d_state[0], a->d_state[1], a->d_ckpt, a->d_tape,
                   a->d_lam[0], a->d_lam[1], a->d_sbar, a->d_gpart,    a->d_jrow,     a->d_seg,
                   a->d_rstate[0], a->d_rstate[1]};
   for (void* p : bufs)
@@ -606,6 +617,10 @@ flb_status upload_s(flb_adjoint a, const double* s) {
   std::vector<T> v(a->N);
   for (uint32_t k = 0; k < a->N; k++) v[k] = (T)s[k];
   FLB_ACUDA(a, cudaMemcpy(a->d_s, v.data(), a->N * sizeof(T), cudaMemcpyHostToDevice));
+  k_por_inv_d<T><<<(a->N + 255) / 256, 256, 0, a->stream>>>(static_cast<const T*>(a->d_s), static_cast<T*>(a->d_id),
+                                                            a->N);
+  FLB_ACUDA(a, cudaGetLastError());
+  FLB_ACUDA(a, cudaStreamSynchronize(a->stream));
   return FLB_OK;
 }
 
@@ -681,7 +696,8 @@ FLB_API flb_status flb_adjoint_create(const flb_adjoint_desc* d, flb_adjoint* ou
     void** p;
     size_t bytes;
   } allocs[] = {{(void**)&a->d_flags, N},           {(void**)&a->d_srcw, N},
-                {&a->d_s, N * a->ts},               {&a->d_state[0], st},
+                {&a->d_s, N * a->ts},               {&a->d_id, N * a->ts},
+                {&a->d_state[0], st},
                 {&a->d_state[1], st},               {&a->d_ckpt, st * a->nseg},
                 {&a->d_tape, 2 * 3 * N * a->ts * a->K},
                 {&a->d_rstate[0], st},              {&a->d_rstate[1], st},            {&a->d_lam[0], st},

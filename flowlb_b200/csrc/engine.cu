@@ -154,7 +154,7 @@ struct Ops {
     launch_sc<S, C, M>(h->kp, h->stream, odd, h->fs, h->hw, wm, h->use_vec, h->fused);
   }
   static void sc_list(flb_engine* h, uint32_t odd, const TileList& tl) {
-    launch_sc_list<S, C, M>(h->kp, h->stream, odd, h->hw, tl, h->grid_sc, h->fused);
+    launch_sc_list<S, C, M>(h->kp, h->stream, odd, h->hw, tl, h->grid_sc, h->fused, h->use_vec);
   }
   static void fs1(flb_engine* h, uint32_t odd, const TileList& tl, const ListClear& lc) {
     launch_fs1<S, C, M>(h->kp, h->stream, odd, h->hw, tl, h->grid_fs1, lc);
@@ -163,7 +163,7 @@ struct Ops {
     return launch_fs234<S, C, M>(h->kp, h->stream, odd, tl, h->grid_fs234, h->d_nz, nl);
   }
   static void grids(flb_engine* h, int nsm) {
-    h->grid_sc = (uint32_t)(nsm * sc_list_blocks_per_sm<S, C, M>());
+    h->grid_sc = (uint32_t)(nsm * sc_list_blocks_per_sm<S, C, M>(h->use_vec));
     h->grid_fs1 = (uint32_t)(nsm * fs_blocks_per_sm<S, C, M>(0));
     h->grid_fs234 = (uint32_t)(nsm * fs_blocks_per_sm<S, C, M>(h->ntiles <= 4096u ? 1 : 2));
   }

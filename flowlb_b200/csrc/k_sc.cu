@@ -133,18 +133,16 @@ __device__ __forceinline__ void load_bytes(const uint8_t* ptr, uint8_t (&f)[V]) 
 
 constexpr int kVecBlock = 256;
 
+// V consecutive cells x0 .. x0+V-1 of row y per thread (x0 a multiple of V;
+// the 32 lanes of the warp take consecutive groups of one row, every lane of
+// the warp must call it).  Used over whole rows (k_sc_vec) and over the rows
+// of listed super-tiles (k_sc_list_vec).
 template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD, bool FU>
-__global__ void __launch_bounds__(kVecBlock, FU ? (std::is_same<S, __half>::value ? FLB_F16_MIN_BLOCKS
-                                                                                     : FLB_VEC_MIN_BLOCKS_FUSED)
-                                                    : FLB_VEC_MIN_BLOCKS)
-    k_sc_vec(const __grid_constant__ KParams p) {
+__device__ __forceinline__ void sc_vec_cells(const KParams& p, uint32_t x0, uint32_t y, uint32_t lane) {
   constexpr int V = Lanes<S>::V;
   constexpr bool DEV = kDev<S, FS, FU>;
   using K = typename std::conditional<DEV, RawHalf, Codec<S, C>>::type;
   const uint32_t nx = p.nx, ny = p.ny;
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t x0 = (blockIdx.x * blockDim.x + threadIdx.x) * V;
-  const uint32_t y = blockIdx.y;
   const bool inrow = x0 < nx;
   const uint32_t row = y * nx;
   const uint32_t rowu = (y + 1u == ny ? 0u : y + 1u) * nx;
@@ -279,6 +277,42 @@ __global__ void __launch_bounds__(kVecBlock, FU ? (std::is_same<S, __half>::valu
         if (tail) dst[xn] = nbr[q][V - 1];
       }
     }
+  }
+}
+
+template <class S, class C, class M, bool FS, bool HW, bool WM, bool ODD, bool FU>
+__global__ void __launch_bounds__(kVecBlock, FU ? (std::is_same<S, __half>::value ? FLB_F16_MIN_BLOCKS
+                                                                                     : FLB_VEC_MIN_BLOCKS_FUSED)
+                                                    : FLB_VEC_MIN_BLOCKS)
+    k_sc_vec(const __grid_constant__ KParams p) {
+  constexpr int V = Lanes<S>::V;
+  sc_vec_cells<S, C, M, FS, HW, WM, ODD, FU>(p, (blockIdx.x * blockDim.x + threadIdx.x) * V, blockIdx.y,
+                                             threadIdx.x & 31u);
+}
+
+// Free surface, vector data path: the listed super-tiles, each row of a
+// super-tile taken by kSTW / (32 V) warps (one warp for FP32 and FP16S).
+template <class S>
+constexpr int list_vec_block() {
+  return (int)kSTH * (int)(kSTW / (32u * (uint32_t)Lanes<S>::V)) * 32;
+}
+template <class S, class C, class M, bool HW, bool ODD, bool FU>
+__global__ void __launch_bounds__(list_vec_block<S>(), 1024 / list_vec_block<S>())
+    k_sc_list_vec(const __grid_constant__ KParams p, const TileList tl) {
+  constexpr uint32_t V = (uint32_t)Lanes<S>::V, wpr = kSTW / (32u * V);
+  // the list was built two kernels back (FS_1 waited for it), so it is read
+  // before waiting for FS_1, whose writes the cell updates need
+  const uint32_t n = tile_count(tl);
+  pdl_wait();
+  pdl_trigger();
+  const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+  const uint32_t row = warp / wpr, chunk = warp % wpr;
+  for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
+    const uint32_t t = tile_at(tl, i);
+    const uint32_t y = (t / tl.nsx) * kSTH + row;
+    if (y >= p.ny) continue;  // warp-uniform
+    const uint32_t x0 = (t % tl.nsx) * kSTW + (chunk * 32u + lane) * V;
+    sc_vec_cells<S, C, M, true, HW, true, ODD, FU>(p, x0, y, lane);
   }
 }
 
@@ -584,7 +618,18 @@ int vec_width(int precision) {
 
 template <class S, class C, class M, bool FU>
 static void launch_sc_list_f(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl,
-                             uint32_t grid) {
+                             uint32_t grid, bool vec) {
+  if (vec) {
+    constexpr int B = list_vec_block<S>();
+    if (hw) {
+      if (odd) launch_pdl(k_sc_list_vec<S, C, M, true, true, FU>, grid, B, st, kp, tl);
+      else launch_pdl(k_sc_list_vec<S, C, M, true, false, FU>, grid, B, st, kp, tl);
+    } else {
+      if (odd) launch_pdl(k_sc_list_vec<S, C, M, false, true, FU>, grid, B, st, kp, tl);
+      else launch_pdl(k_sc_list_vec<S, C, M, false, false, FU>, grid, B, st, kp, tl);
+    }
+    return;
+  }
   if (hw) {
     if (odd) launch_pdl(k_sc_list<S, C, M, true, true, FU>, grid, kListBlock, st, kp, tl);
     else launch_pdl(k_sc_list<S, C, M, true, false, FU>, grid, kListBlock, st, kp, tl);
@@ -596,16 +641,23 @@ static void launch_sc_list_f(const KParams& kp, cudaStream_t st, uint32_t odd, b
 
 template <class S, class C, class M>
 void launch_sc_list(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl, uint32_t grid,
-                    bool fu) {
-  if (fu) launch_sc_list_f<S, C, M, true>(kp, st, odd, hw, tl, grid);
-  else launch_sc_list_f<S, C, M, false>(kp, st, odd, hw, tl, grid);
+                    bool fu, bool vec) {
+  if (fu) launch_sc_list_f<S, C, M, true>(kp, st, odd, hw, tl, grid, vec);
+  else launch_sc_list_f<S, C, M, false>(kp, st, odd, hw, tl, grid, vec);
 }
 
 template <class S, class C, class M>
-int sc_list_blocks_per_sm() {
+int sc_list_blocks_per_sm(bool vec) {
   int n = 0, m = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sc_list<S, C, M, true, false, false>, kListBlock, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_sc_list<S, C, M, true, false, true>, kListBlock, 0);
+  if (vec) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sc_list_vec<S, C, M, true, false, false>,
+                                                  list_vec_block<S>(), 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_sc_list_vec<S, C, M, true, false, true>,
+                                                  list_vec_block<S>(), 0);
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_sc_list<S, C, M, true, false, false>, kListBlock, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_sc_list<S, C, M, true, false, true>, kListBlock, 0);
+  }
   n = n < m ? n : m;
   return n > 0 ? n : 1;
 }
@@ -613,8 +665,8 @@ int sc_list_blocks_per_sm() {
 #define FLB_INSTANTIATE(S, C, M)                                                                               \
   template void launch_sc<S, C, M>(const KParams&, cudaStream_t, uint32_t, bool, bool, bool, bool, bool);     \
   template void launch_sc_list<S, C, M>(const KParams&, cudaStream_t, uint32_t, bool, const TileList&, uint32_t,  \
-                                        bool);                                                                  \
-  template int sc_list_blocks_per_sm<S, C, M>();
+                                        bool, bool);                                                            \
+  template int sc_list_blocks_per_sm<S, C, M>(bool);
 FLB_FOR_EACH_VARIANT(FLB_INSTANTIATE)
 #undef FLB_INSTANTIATE
 

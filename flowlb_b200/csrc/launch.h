@@ -30,12 +30,13 @@ void fill_case_constants(const flb_case_desc* desc, KParams& k);
 template <class S, class C, class M>
 void launch_sc(const KParams& kp, cudaStream_t st, uint32_t odd, bool fs, bool hw, bool wm, bool vec, bool fu);
 int vec_width(int precision);
-// free surface: the listed super-tiles in a persistent grid of `grid` blocks
+// free surface: the listed super-tiles in a persistent grid of `grid` blocks;
+// vec: the vector data path (needs nx divisible by the vector width)
 template <class S, class C, class M>
 void launch_sc_list(const KParams& kp, cudaStream_t st, uint32_t odd, bool hw, const TileList& tl, uint32_t grid,
-                    bool fu);
+                    bool fu, bool vec);
 template <class S, class C, class M>
-int sc_list_blocks_per_sm();
+int sc_list_blocks_per_sm(bool vec);
 
 // FS_1 (clears the next step's list lengths), its reference-mode apply, and
 // FS_2..4 on listed super-tiles (appends the next step's lists)
