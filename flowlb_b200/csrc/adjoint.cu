@@ -616,7 +616,10 @@ template <class T>
 flb_status upload_s(flb_adjoint a, const double* s) {
   std::vector<T> v(a->N);
   for (uint32_t k = 0; k < a->N; k++) v[k] = (T)s[k];
-  FLB_ACUDA(a, cudaMemcpy(a->d_s, v.data(), a->N * sizeof(T), cudaMemcpyHostToDevice));
+  // on the handle's stream: a plain cudaMemcpy from pageable memory may return
+  // before its data reach the device, and the handle's non-blocking stream is
+  // not ordered after it
+  FLB_ACUDA(a, cudaMemcpyAsync(a->d_s, v.data(), a->N * sizeof(T), cudaMemcpyHostToDevice, a->stream));
   k_por_inv_d<T><<<(a->N + 255) / 256, 256, 0, a->stream>>>(static_cast<const T*>(a->d_s), static_cast<T*>(a->d_id),
                                                             a->N);
   FLB_ACUDA(a, cudaGetLastError());
@@ -718,7 +721,7 @@ FLB_API flb_status flb_adjoint_create(const flb_adjoint_desc* d, flb_adjoint* ou
     a->h_seg[k].t0 = (uint64_t)k * a->K;
     a->h_seg[k].ckpt = static_cast<char*>(a->d_ckpt) + (size_t)k * st;
   }
-  if (cudaMemcpy(a->d_flags, d->flags, N, cudaMemcpyHostToDevice) != cudaSuccess)
+  if (cudaMemcpyAsync(a->d_flags, d->flags, N, cudaMemcpyHostToDevice, a->stream) != cudaSuccess)
     return bail(afail(a, FLB_ERR_CUDA, "cudaMemcpy"));
   k_srcw<<<dim3(a->gx_blocks, a->ny), kAdjBlock, 0, a->stream>>>(a->d_flags, a->d_srcw, a->nx, a->ny);
   flb_status s = a->ts == 8 ? upload_s<double>(a, d->porosity) : upload_s<float>(a, d->porosity);

@@ -613,13 +613,20 @@ flb_status bassign(flb_batch b, int clusters) {
   // the previous assignment in place
   uint32_t* d_start = nullptr;
   FLB_BCUDA(b, cudaMalloc(&d_start, start.size() * sizeof(uint32_t)));
-  cudaError_t e = cudaMemcpy(d_start, start.data(), start.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+  // stream-ordered copies (the batch's stream is non-blocking, and a plain
+  // cudaMemcpy from pageable memory may return before its data land), waited
+  // for before the host arrays go out of scope
+  cudaError_t e = cudaMemcpyAsync(d_start, start.data(), start.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                                  b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess) {
     cudaFree(d_start);
     return bcuda(b, e, "cudaMemcpy");
   }
   bdrop_graph(b);  // the captured launch refers to the old arrays
-  FLB_BCUDA(b, cudaMemcpy(b->d_order, order.data(), order.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+  FLB_BCUDA(b, cudaMemcpyAsync(b->d_order, order.data(), order.size() * sizeof(uint32_t), cudaMemcpyHostToDevice,
+                               b->stream));
+  FLB_BCUDA(b, cudaStreamSynchronize(b->stream));
   if (b->d_start) cudaFree(b->d_start);
   b->d_start = d_start;
   b->clusters = clusters;
@@ -987,7 +994,9 @@ FLB_API flb_status flb_batch_create(const flb_case_desc* cases, uint32_t n, int 
     cudaError_t e = cudaMemcpyAsync(b->d_geo + o, cases[c].flags, N, cudaMemcpyHostToDevice, b->stream);
     if (e != cudaSuccess) return bail(bcuda(b, e, "cudaMemcpyAsync"));
   }
-  cudaError_t e = cudaMemcpy(b->d_cases, b->hcases.data(), n * sizeof(BatchCase), cudaMemcpyHostToDevice);
+  cudaError_t e = cudaMemcpyAsync(b->d_cases, b->hcases.data(), n * sizeof(BatchCase), cudaMemcpyHostToDevice,
+                                  b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
   if (e != cudaSuccess) return bail(bcuda(b, e, "cudaMemcpy"));
   flb_status s = FLB_OK;
   if (autotune) {

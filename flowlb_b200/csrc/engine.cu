@@ -55,7 +55,8 @@ struct flb_engine {
   bool own_stream = false;
   size_t s_size = 4, c_size = 4, m_size = 8;
   bool fs = false, hw = false, has_io = false;
-  bool use_vec = false;  // vectorised stream-collide
+  bool use_vec = false;       // vectorised stream-collide (single phase)
+  bool use_vec_list = false;  // vectorised listed stream-collide (free surface)
   bool fused = false;    // fused SRT arithmetic in stream-collide
   uint64_t t = 0;
   uint64_t launches = 0;
@@ -154,7 +155,7 @@ struct Ops {
     launch_sc<S, C, M>(h->kp, h->stream, odd, h->fs, h->hw, wm, h->use_vec, h->fused);
   }
   static void sc_list(flb_engine* h, uint32_t odd, const TileList& tl) {
-    launch_sc_list<S, C, M>(h->kp, h->stream, odd, h->hw, tl, h->grid_sc, h->fused, h->use_vec);
+    launch_sc_list<S, C, M>(h->kp, h->stream, odd, h->hw, tl, h->grid_sc, h->fused, h->use_vec_list);
   }
   static void fs1(flb_engine* h, uint32_t odd, const TileList& tl, const ListClear& lc) {
     launch_fs1<S, C, M>(h->kp, h->stream, odd, h->hw, tl, h->grid_fs1, lc);
@@ -163,7 +164,7 @@ struct Ops {
     return launch_fs234<S, C, M>(h->kp, h->stream, odd, tl, h->grid_fs234, h->d_nz, nl);
   }
   static void grids(flb_engine* h, int nsm) {
-    h->grid_sc = (uint32_t)(nsm * sc_list_blocks_per_sm<S, C, M>(h->use_vec));
+    h->grid_sc = (uint32_t)(nsm * sc_list_blocks_per_sm<S, C, M>(h->use_vec_list));
     h->grid_fs1 = (uint32_t)(nsm * fs_blocks_per_sm<S, C, M>(0));
     h->grid_fs234 = (uint32_t)(nsm * fs_blocks_per_sm<S, C, M>(h->ntiles <= 4096u ? 1 : 2));
   }
@@ -636,6 +637,15 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
     h->use_vec = desc->kernel_variant == 2 ||
                  (desc->kernel_variant == 0 && desc->nx % V == 0 &&
                   (desc->precision == 16 || (desc->precision == 32 && fused)));
+    // free surface, the listed stream-collide: measured on a B200, the vector
+    // path is slower for FP32 (2048x512 dam break 33.3 against 29.4 us per
+    // step; 8192x2048 53.4 against 54.8 GLUPS) and faster for FP16S on large
+    // grids (8192x2048: 57.5 against 54.7 GLUPS), so it runs there, or when
+    // asked for
+    const uint64_t tiles = (uint64_t)((desc->nx + kSTW - 1) / kSTW) * ((desc->ny + kSTH - 1) / kSTH);
+    h->use_vec_list = desc->kernel_variant == 2 ||
+                      (desc->kernel_variant == 0 && desc->nx % V == 0 && desc->precision == 16 && fused &&
+                       tiles > 4096u);
   }
   s = check_io(h, desc->flags);
   if (s != FLB_OK) {
