@@ -92,3 +92,24 @@ def test_adjoint_matches_finite_differences_full_case():
     assert worst <= 1e-4
     assert abs(fdg - dg[0]) <= 1e-4 * abs(fdg)
     a.close()
+
+
+def test_fp64_adjoint_cost_within_three_forwards():
+    """The FP64 form, whose gradient meets the finite-difference check above on
+    the same full-size case (1024x256, 4096 steps, checkpoints every 64), costs
+    at most three forward passes: backward (recomputation included) over
+    forward, device time of each, best of three after a warm-up pair."""
+    c = cases.porous_channel()
+    a = E.Adjoint(c.flags, c.porosity.astype(np.float64), tau=0.6, gx=5e-6, precision=64, steps=4096,
+                  window=512, checkpoint_every=64)
+    a.forward()
+    a.backward()
+    ratios = []
+    for _ in range(3):
+        a.forward()
+        a.backward()
+        f_ms, b_ms = a.timing()
+        ratios.append(b_ms / f_ms)
+    a.close()
+    print(f"FP64 backward / forward: {min(ratios):.3f} (runs {', '.join(f'{r:.3f}' for r in ratios)})")
+    assert min(ratios) <= 3.0, ratios
