@@ -10,12 +10,13 @@
 namespace flb {
 
 // ---- FS_1: mass exchange and gas reconstruction, lbmKernel2D.cu:14-121 -----
+// flag, nbm: the cell's flag and wall mask (0 without half-way walls),
+// loaded by the caller.
 template <class S, class C, class M, bool HW, bool ODD>
-__device__ __forceinline__ void fs1_cell(const KParams& p, uint32_t x, uint32_t y) {
+__device__ __forceinline__ void fs1_cell(const KParams& p, uint32_t x, uint32_t y, uint8_t flag, uint32_t nbm) {
   const uint32_t nx = p.nx, N = p.N;
   const uint32_t idx = x + y * nx;
   const uint8_t* flags = p.flags;
-  const uint8_t flag = flags[idx];
   if (flag & (kGas | kWall | kInlet)) return;
   const bool cons = p.fs_cons != 0;
   const uint8_t e = flag & kFGI;
@@ -23,7 +24,7 @@ __device__ __forceinline__ void fs1_cell(const KParams& p, uint32_t x, uint32_t 
   uint32_t nb[9];
   neighbours(x, y, nx, p.ny, nb);
   C in[9], out[9];
-  load_in<S, C, HW, ODD>(p, idx, nb, HW ? p.nbmask[idx] : 0u, in);
+  load_in<S, C, HW, ODD>(p, idx, nb, nbm, in);
   out[0] = in[0];
   load_out<S, C, ODD>(p, idx, nb, out);
   M* Ms = static_cast<M*>(p.mass);
@@ -108,6 +109,15 @@ __device__ __forceinline__ void fs1_cell(const KParams& p, uint32_t x, uint32_t 
     }
   }
   Ms[idx] = m;
+}
+
+// The cell's flag and wall mask in one round trip, then the cell.
+template <class S, class C, class M, bool HW, bool ODD>
+__device__ __forceinline__ void fs1_cell(const KParams& p, uint32_t x, uint32_t y) {
+  const uint32_t idx = x + y * p.nx;
+  const uint8_t flag = p.flags[idx];
+  const uint32_t nbm = HW ? p.nbmask[idx] : 0u;
+  fs1_cell<S, C, M, HW, ODD>(p, x, y, flag, nbm);
 }
 
 // ---- FS_2 + FS_3 + FS_4 fused: lbmKernel2D.cu:124-303 ----------------------

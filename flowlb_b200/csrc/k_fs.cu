@@ -20,17 +20,31 @@ __global__ void __launch_bounds__(kFs1Block, 2) k_fs1(const __grid_constant__ KP
   pdl_wait();
   pdl_trigger();
   clear_next_lists(lc);
+  // two cells per thread and super-tile, x and x + 64 of one row
+  constexpr uint32_t kCpr = kFs1Block / 32 / kSTH;
+  static_assert(2 * 32 * kCpr == kSTW, "FS_1: two cells per thread and super-tile");
   const uint32_t n = tile_count(tl);
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-  const uint32_t row = warp % kSTH, chunk = warp / kSTH, cpr = (blockDim.x >> 5) / kSTH;
+  const uint32_t row = warp % kSTH, chunk = warp / kSTH;
+  const uint32_t nx = p.nx;
   for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
     const uint32_t t = tile_at(tl, i);
     const uint32_t y = (t / tl.nsx) * kSTH + row;
     if (y >= p.ny) continue;
-    const uint32_t xb = (t % tl.nsx) * kSTW + lane;
-#pragma unroll 1
-    for (uint32_t j = chunk * 32u; j < kSTW; j += 32u * cpr)
-      if (xb + j < p.nx) fs1_cell<S, C, M, HW, ODD>(p, xb + j, y);
+    const uint32_t xa = (t % tl.nsx) * kSTW + chunk * 32u + lane, xc = xa + 32u * kCpr;
+    // both cells' flags and wall masks first: one round trip for the two
+    uint8_t fa = kGas, fc = kGas;
+    uint32_t ma = 0, mc = 0;
+    if (xa < nx) {
+      fa = p.flags[xa + y * nx];
+      if (HW) ma = p.nbmask[xa + y * nx];
+    }
+    if (xc < nx) {
+      fc = p.flags[xc + y * nx];
+      if (HW) mc = p.nbmask[xc + y * nx];
+    }
+    if (xa < nx) fs1_cell<S, C, M, HW, ODD>(p, xa, y, fa, ma);
+    if (xc < nx) fs1_cell<S, C, M, HW, ODD>(p, xc, y, fc, mc);
   }
 }
 

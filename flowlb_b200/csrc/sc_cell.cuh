@@ -209,9 +209,10 @@ __device__ __forceinline__ void sc_cell(const KParams& p, uint32_t x, uint32_t y
     load_in<S, C, HW, ODD, K>(p, idx, nb, nbm, f);
     if (flag & (kGas | kWall)) return;
   } else {
+    // the wall mask is loaded with the flag (one round trip, not two)
     flag = p.flags[idx];
-    if (flag & (kGas | kWall)) return;
     if (HW) nbm = p.nbmask[idx];
+    if (flag & (kGas | kWall)) return;
     load_in<S, C, HW, ODD, K>(p, idx, nb, nbm, f);
   }
   collide_cell<C, M, FS, WM, FU, DEV>(p, idx, x, y, flag, nbm, f, DEV ? p.tstep[ODD] : 0u);
