@@ -201,22 +201,24 @@ class ClockSampler:
                 "samples": len(sm), "sm_mhz_min": min(sm), "source": source}
 
 
-def algorithmic_bytes(counts: dict) -> dict:
-    """Bytes each free-surface pass must move per launch (FP32 populations,
-    FP64 mass), over the cells it visits: the listed super-tiles hold the
-    fluid and interface cells (gas cells outside them are not touched).
+def algorithmic_bytes(counts: dict, pop_bytes: float = 4.0) -> dict:
+    """Bytes each free-surface pass must move per launch (populations of
+    pop_bytes each: 4 for FP32, 2 for FP16S; FP64 mass), over the cells it
+    visits: the listed super-tiles hold the fluid and interface cells (gas
+    cells outside them are not touched).
       stream-collide: per fluid/interface cell its flag and wall mask (2 B),
-        9 population loads and stores (72 B), density and velocity (12 B);
-        interface cells also read their mass (8 B) and rewrite the flag (1 B);
+        9 population loads and stores (72 B in FP32), density and velocity
+        (12 B); interface cells also read their mass (8 B) and rewrite the
+        flag (1 B);
       FS_1: per fluid/interface cell 9 incoming and 8 outgoing populations
-        (68 B), its flag (1 B), mass read and write (16 B) and the excess
-        shares it collects (8 B);
+        (68 B in FP32), its flag (1 B), mass read and write (16 B) and the
+        excess shares it collects (8 B);
       FS_2..4: per fluid/interface cell the flag (1 B), the flag buffer read
         and write (2 B), density (4 B), mass read and write (16 B), excess and
         fill level (16 B)."""
     active = counts["fluid"] + counts["interface"]
-    return {"stream_collide": active * 86.0 + counts["interface"] * 9.0, "fs1": active * 93.0,
-            "fs234": active * 39.0}
+    return {"stream_collide": active * (14.0 + 18.0 * pop_bytes) + counts["interface"] * 9.0,
+            "fs1": active * (25.0 + 17.0 * pop_bytes), "fs234": active * 39.0}
 
 
 def _gpu_uuid(torch, device: int):
@@ -470,10 +472,20 @@ def side_measurements(args, device, E, cases, peak, uuid):
                      bounce_back=E.BB_HALFWAY, fs_mode=E.FS_CONSERVATIVE, device=device, u_max=U_MAX)
         s.step(S)
         s.sync()
+        c0 = s.cell_counts()
         ms = _timed(torch, s, 2 * S)
+        c1 = s.cell_counts()
         form = "persistent kernel" if s.persistent else "per-pass kernels"
         s.close()
-        return {"value": round(c.cells * 2 * S / (ms * 1e-3) / 1e6, 1), "unit": "MLUPS", "step_form": form}
+        # the step's algorithmic bytes from the live-cell census (mean of the
+        # window's ends), over the measured copy bandwidth
+        cavg = {k: 0.5 * (c0[k] + c1[k]) for k in c0}
+        step_bytes = sum(algorithmic_bytes(cavg, 4.0 if prec == 32 else 2.0).values())
+        gbs = step_bytes * 2 * S / (ms * 1e-3) / 1e9
+        return {"value": round(c.cells * 2 * S / (ms * 1e-3) / 1e6, 1), "unit": "MLUPS", "step_form": form,
+                "algorithmic_bytes_per_step": int(step_bytes), "achieved_gbs": round(gbs, 1),
+                "frac_of_measured_hbm": round(gbs / peak, 4),
+                "live_cells": int(cavg["fluid"] + cavg["interface"])}
 
     for prec in (32, 16):
         clocked(f"dam_break_8192x2048_fp{prec if prec == 32 else '16s'}", lambda: dam_break_big(prec))

@@ -57,6 +57,7 @@ struct flb_engine {
   bool fs = false, hw = false, has_io = false;
   bool use_vec = false;       // vectorised stream-collide (single phase)
   bool use_vec_list = false;  // vectorised listed stream-collide (free surface)
+  int fs_form = FS_FORM_W128X1;  // launch form of the flag pass (FsForm)
   bool fused = false;    // fused SRT arithmetic in stream-collide
   uint64_t t = 0;
   uint64_t launches = 0;
@@ -161,12 +162,12 @@ struct Ops {
     launch_fs1<S, C, M>(h->kp, h->stream, odd, h->hw, tl, h->grid_fs1, lc);
   }
   static int fs234(flb_engine* h, uint32_t odd, const TileList& tl, const NextLists& nl) {
-    return launch_fs234<S, C, M>(h->kp, h->stream, odd, tl, h->grid_fs234, h->d_nz, nl);
+    return launch_fs234<S, C, M>(h->kp, h->stream, odd, tl, h->grid_fs234, h->d_nz, nl, h->fs_form);
   }
   static void grids(flb_engine* h, int nsm) {
     h->grid_sc = (uint32_t)(nsm * sc_list_blocks_per_sm<S, C, M>(h->use_vec_list));
-    h->grid_fs1 = (uint32_t)(nsm * fs_blocks_per_sm<S, C, M>(0));
-    h->grid_fs234 = (uint32_t)(nsm * fs_blocks_per_sm<S, C, M>(h->ntiles <= 4096u ? 1 : 2));
+    h->grid_fs1 = (uint32_t)(nsm * fs_blocks_per_sm<S, C, M>(0, 0));
+    h->grid_fs234 = (uint32_t)(nsm * fs_blocks_per_sm<S, C, M>(1, h->fs_form));
   }
   static void apply_recon(flb_engine* h, uint32_t odd) { launch_apply_recon<S, C, M>(h->kp, h->stream, odd); }
   static cudaError_t persist(flb_engine* h, const KParams& p0, const KParams& p1, const FspArgs& a) {
@@ -646,6 +647,20 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
     h->use_vec_list = desc->kernel_variant == 2 ||
                       (desc->kernel_variant == 0 && desc->nx % V == 0 && desc->precision == 16 && fused &&
                        tiles > 4096u);
+    // flag pass: 128-wide tiles with one cell per thread (1024-thread
+    // blocks) on grids of up to 4096 super-tiles, two cells per thread
+    // (512-thread blocks, two per SM) above.  Measured on a B200: 2048x512
+    // dam break 29.2 us per step (two cells per thread 30.1, four 34.6);
+    // 8192x2048 flag pass 110 us per step (three 512-thread blocks per SM
+    // 114, four 119; one cell per thread 124, four 131, 32-wide tiles 158).  FLB_FS_FLAG_FORM (32, 128x1, 128x2 or 128x4: tile width x cells
+    // per thread) selects another form, with the same results.
+    h->fs_form = tiles <= 4096u ? FS_FORM_W128X1 : FS_FORM_W128X2;
+    if (const char* v = std::getenv("FLB_FS_FLAG_FORM")) {
+      if (!std::strcmp(v, "32")) h->fs_form = FS_FORM_W32;
+      else if (!std::strcmp(v, "128x1")) h->fs_form = FS_FORM_W128X1;
+      else if (!std::strcmp(v, "128x2")) h->fs_form = FS_FORM_W128X2;
+      else if (!std::strcmp(v, "128x4")) h->fs_form = FS_FORM_W128X4;
+    }
   }
   s = check_io(h, desc->flags);
   if (s != FLB_OK) {

@@ -125,15 +125,24 @@ __device__ __forceinline__ void fs1_cell(const KParams& p, uint32_t x, uint32_t 
 // of kTX x 8 cells stages the flags of its 3-cell halo in shared memory and
 // evaluates the chain there, so neighbour flags are never read while another
 // block rewrites them.  Reads p.flags, writes p.flags_out.
-// Tile width of the flag pass: 128 (a whole super-tile, 1024 threads) or 32
-// (a quarter, 256 threads).  Measured on a B200, dam break: 2048x512 (about
-// 300 active super-tiles) 31 vs 25 GLUPS in favour of 128; 8192x2048 (about
-// 4400) 53 vs 59 in favour of 32 (more resident warps).  launch_fs234 picks by
-// the grid's super-tile count (kWideTiles).
+// Tiles of the flag pass: 128 x 8 (a whole super-tile) or 32 x 8 (a quarter,
+// the super-tile's four quarters in turn), with one, two or four cells per
+// thread (FsForm; the host picks by the grid's super-tile count).  On grids
+// of up to kWideTiles super-tiles the pass is launched with programmatic
+// dependent launch.
 constexpr int kTY = 8, kHalo = 3;
-constexpr uint32_t kWideTiles = 4096;
+#ifndef FLB_FS_PDL_TILES
+#define FLB_FS_PDL_TILES 4096
+#endif
+constexpr uint32_t kWideTiles = FLB_FS_PDL_TILES;
 #ifndef FLB_FS_WIDE_MIN_BLOCKS
 #define FLB_FS_WIDE_MIN_BLOCKS 2
+#endif
+#ifndef FLB_FS_HALF_MIN_BLOCKS
+#define FLB_FS_HALF_MIN_BLOCKS 2
+#endif
+#ifndef FLB_FS_QUARTER_MIN_BLOCKS
+#define FLB_FS_QUARTER_MIN_BLOCKS 4
 #endif
 // periodic index; halos of in-range tiles need one add or subtract, the
 // modulo is only reached on grids narrower than a tile
@@ -225,106 +234,59 @@ __device__ __forceinline__ bool bit_at(const uint32_t (&m)[FlagMasks<TW>::kR][Fl
   return (m[r][c] >> i) & 1u;
 }
 
-// One TW x 8 tile (tile coordinates tx, ty) with the TW*8 threads of the block;
-// every thread of the block must call it.  Returns whether this thread's cell
-// is fluid or interface after the pass.
+// Per super-tile activity word written by the flag pass: bit 0 = it holds a
+// fluid or interface cell; bits 1..8 = it holds one within kReach cells of
+// the edge or corner facing the neighbour in direction (dx, dy) (edge_bit).
+// The stencil chain of the flag pass reaches kReach = 3 cells, so a neighbour
+// needs the pass next step only if such a cell faces it.
+constexpr int kReach = 3;
+__host__ __device__ constexpr int edge_bit(int dx, int dy) {
+  return dy == 0 ? (dx > 0 ? 1 : 2) : dx == 0 ? (dy > 0 ? 3 : 4) : dy > 0 ? (dx > 0 ? 5 : 6) : (dx > 0 ? 7 : 8);
+}
+
+// Activity word of a live cell at (lx, ly) in a super-tile of wact x hact cells.
+__device__ __forceinline__ uint32_t activity(int lx, int ly, int wact, int hact) {
+  const bool r = lx >= wact - kReach, l = lx < kReach, u = ly >= hact - kReach, d = ly < kReach;
+  return 1u | ((uint32_t)r << edge_bit(1, 0)) | ((uint32_t)l << edge_bit(-1, 0)) | ((uint32_t)u << edge_bit(0, 1)) |
+         ((uint32_t)d << edge_bit(0, -1)) | ((uint32_t)(u && r) << edge_bit(1, 1)) |
+         ((uint32_t)(u && l) << edge_bit(-1, 1)) | ((uint32_t)(d && r) << edge_bit(1, -1)) |
+         ((uint32_t)(d && l) << edge_bit(-1, -1));
+}
+
+// This cell's values after stream-collide that the flag pass reads and
+// rewrites; loaded before the stencil stages so that their latency overlaps.
+template <class C, class M>
+struct Fs4Own {
+  uint8_t f0, old;
+  M m, ex;
+  C rho;
+};
+
+template <class C, class M>
+__device__ __forceinline__ void fs4_own_load(const KParams& p, uint32_t idx, Fs4Own<C, M>& o) {
+  o.f0 = p.flags[idx];
+  o.old = p.flags_out[idx];
+  o.m = static_cast<const M*>(p.mass)[idx];
+  o.ex = static_cast<const M*>(p.excess)[idx];
+  o.rho = static_cast<const C*>(p.rho)[idx];
+}
+
+// The per-cell end of the flag pass: the byte chain of FS_2, FS_3 and FS_4 for
+// cell (gx, gy) at (lx, ly) in the tile, from the masks the stencil stages
+// left in sm, and the FS_3 / FS_4 field updates.  Returns whether the cell is
+// fluid or interface after the pass.
 template <class S, class C, class M, bool ODD, int TW>
-__device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int tid, FlagMasks<TW>& sm) {
-  constexpr int kTX = TW, kW = FlagMasks<TW>::kW, kR = FlagMasks<TW>::kR;
-  constexpr int kWarps = TW * kTY / 32;
+__device__ __forceinline__ bool fs234_cell(const KParams& p, const FlagMasks<TW>& sm, int gx, int gy, int lx, int ly,
+                                           const Fs4Own<C, M>& own) {
   const int nx = (int)p.nx, ny = (int)p.ny;
-  const uint8_t* flags = p.flags;
-  // this thread's cell: its own values are loaded now, so that their latency
-  // overlaps the mask building and the stencil stages
-  const int gx = tx * kTX + tid % kTX, gy = ty * kTY + tid / kTX;
-  const bool in = gx < nx && gy < ny;
-  const uint32_t idx = in ? (uint32_t)gx + (uint32_t)gy * (uint32_t)nx : 0u;
+  const int r = kHalo + ly, c = 1 + lx / 32, i = lx % 32;
+  const uint32_t idx = (uint32_t)gx + (uint32_t)gy * (uint32_t)nx;
+  const uint8_t f0 = own.f0, old = own.old;
+  const M m_old = own.m, ex_old = own.ex;
+  const C rho_own = own.rho;
   M* Ms = static_cast<M*>(p.mass);
   M* Exs = static_cast<M*>(p.excess);
   const C* R = static_cast<const C*>(p.rho);
-  uint8_t old = 0, f0 = 0;
-  M m_old = M(0), ex_old = M(0);
-  C rho_own = C(0);
-  if (in) {
-    f0 = flags[idx];
-    old = p.flags_out[idx];
-    m_old = Ms[idx];
-    ex_old = Exs[idx];
-    rho_own = R[idx];
-  }
-  // masks of the flags after stream-collide: every flag byte a lane needs is
-  // loaded first, so the loads of all its row-words are in flight together
-  const int lane = tid & 31, warp = tid >> 5;
-  const int xw = tx * kTX - 32 + lane;  // word 0 starts one word left of the tile
-  constexpr int kRW = kR * kW, kIters = (kRW + kWarps - 1) / kWarps;
-  uint8_t fv[kIters];
-#pragma unroll
-  for (int k = 0; k < kIters; k++) {
-    const int rw = warp + k * kWarps;
-    const int r = rw / kW, c = rw % kW;
-    fv[k] = rw < kRW ? flags[wrapi(xw + 32 * c, nx) + wrapi(ty * kTY - kHalo + r, ny) * nx] : 0;
-  }
-#pragma unroll
-  for (int k = 0; k < kIters; k++) {
-    const int rw = warp + k * kWarps;  // the same for the whole warp
-    if (rw >= kRW) break;
-    const int r = rw / kW, c = rw % kW;
-    const uint8_t f = fv[k];
-    // ballots of the flag bits; the masks a row needs are formed from them:
-    // the outer halo rows only feed FS_2's IF dilation, the next rows also
-    // FS_2's rewrite, the inner ten rows everything (warp-uniform branches)
-    const uint32_t bF = __ballot_sync(0xffffffffu, (f & kFluid) != 0);
-    const uint32_t bI = __ballot_sync(0xffffffffu, (f & kInterface) != 0);
-    if (lane == 0) sm.a[r][c] = bF & bI;
-    if (r == 0 || r == kR - 1) continue;
-    const uint32_t bG = __ballot_sync(0xffffffffu, (f & kGas) != 0);
-    const uint32_t bGI = __ballot_sync(0xffffffffu, (f & kGasInterface) != 0);
-    if (lane == 0) {
-      sm.gas[r][c] = bG;
-      sm.gonly[r][c] = bG & ~bI;
-      sm.gi[r][c] = bGI;
-      sm.it[r][c] = bI;
-    }
-    if (r == 1 || r == kR - 2) continue;
-    const uint32_t bIn = __ballot_sync(0xffffffffu, (f & kInlet) != 0);
-    const uint32_t bSk = __ballot_sync(0xffffffffu, (f & (kWall | kMovingWall | kInlet)) != 0);
-    if (lane == 0) {
-      sm.fl[r][c] = bF & ~bIn;
-      sm.fb[r][c] = bF;
-      sm.sk[r][c] = bSk;
-    }
-  }
-  __syncthreads();
-  // FS_2 on rows 1 .. kR-2: next to an IF cell, IG -> I and G -> GI
-  if (tid < (kR - 2) * kW) {
-    const int r = 1 + tid / kW, c = tid % kW;
-    const uint32_t any_if = dilate8<TW>(sm.a, r, c);
-    const uint32_t p1 = sm.gas[r][c] & ~any_if;
-    const uint32_t p7 = sm.gi[r][c] | (any_if & sm.gonly[r][c]);
-    sm.anyif[r][c] = any_if;
-    sm.p1[r][c] = p1;
-    sm.p7[r][c] = p7;
-    sm.ig1[r][c] = p1 & sm.it[r][c] & ~p7;
-  }
-  __syncthreads();
-  // FS_3 on rows 2 .. kR-3: next to an IG cell, F / IF (not inlet) -> I; then
-  // FS_4's conversion and the mask of the neighbours FS_4 counts
-  if (tid < (kR - 4) * kW) {
-    const int r = 2 + tid / kW, c = tid % kW;
-    const uint32_t any_ig = dilate8<TW>(sm.ig1, r, c);
-    const uint32_t conv = sm.fl[r][c] & any_ig;
-    const uint32_t P0 = sm.fb[r][c] & ~conv, P1 = sm.p1[r][c], P2 = sm.it[r][c] | conv, P7 = sm.p7[r][c];
-    const uint32_t go = ~sm.sk[r][c];
-    const uint32_t to_plain = go & ((P0 & ~P1 & P2 & ~P7) | (~P0 & P1 & P2 & ~P7));  // IF, IG lose the I bit
-    const uint32_t from_gi = go & (~P0 & ~P1 & ~P2 & P7);                          // GI -> I
-    const uint32_t P2f = (P2 & ~to_plain) | from_gi, P7f = P7 & ~from_gi;
-    sm.anyig[r][c] = any_ig;
-    sm.cnt[r][c] = p.fs_cons ? ((P0 ^ P2f) & ~P1 & go) : ((P0 | P2f) ^ P7f);
-  }
-  __syncthreads();
-  if (!in) return false;
-  const int lx = tid % kTX, ly = tid / kTX;
-  const int r = kHalo + ly, c = 1 + lx / 32, i = lx % 32;
   const bool any_if = (sm.anyif[r][c] >> i) & 1u, any_ig = (sm.anyig[r][c] >> i) & 1u;
   // the byte chain of the reference passes, for this cell
   uint8_t f1 = f0;
@@ -442,24 +404,110 @@ __device__ __forceinline__ bool fs234_tile(const KParams& p, int tx, int ty, int
   return live;
 }
 
-// Per super-tile activity word written by the flag pass: bit 0 = it holds a
-// fluid or interface cell; bits 1..8 = it holds one within kReach cells of
-// the edge or corner facing the neighbour in direction (dx, dy) (edge_bit).
-// The stencil chain of the flag pass reaches kReach = 3 cells, so a neighbour
-// needs the pass next step only if such a cell faces it.
-constexpr int kReach = 3;
-__host__ __device__ constexpr int edge_bit(int dx, int dy) {
-  return dy == 0 ? (dx > 0 ? 1 : 2) : dx == 0 ? (dy > 0 ? 3 : 4) : dy > 0 ? (dx > 0 ? 5 : 6) : (dx > 0 ? 7 : 8);
+// One TW x 8 tile (tile coordinates tx, ty) with the TW*8/CPT threads of the
+// block, CPT cells per thread (rows ly and ly + 8/CPT, ...); every thread of
+// the block must call it.  Returns the activity bits (activity, above) of
+// this thread's cells that are fluid or interface after the pass, with the
+// tile at column xoff of a super-tile of wact x hact cells.
+template <class S, class C, class M, bool ODD, int TW, int CPT>
+__device__ __forceinline__ uint32_t fs234_tile(const KParams& p, int tx, int ty, int tid, FlagMasks<TW>& sm,
+                                               int xoff, int wact, int hact) {
+  constexpr int kTX = TW, kW = FlagMasks<TW>::kW, kR = FlagMasks<TW>::kR;
+  constexpr int kThreads = TW * kTY / CPT, kWarps = kThreads / 32, kRowStep = kTY / CPT;
+  static_assert(kTY % CPT == 0 && kThreads >= (kR - 2) * kW, "flag pass: block too small for the stencil stages");
+  const int nx = (int)p.nx, ny = (int)p.ny;
+  const uint8_t* flags = p.flags;
+  // this thread's cells: their own values are loaded now, so that their
+  // latency overlaps the mask building and the stencil stages
+  const int lx = tid % kTX, ly0 = tid / kTX;
+  const int gx = tx * kTX + lx;
+  Fs4Own<C, M> own[CPT];
+#pragma unroll
+  for (int k = 0; k < CPT; k++) {
+    const int gy = ty * kTY + ly0 + k * kRowStep;
+    own[k] = Fs4Own<C, M>{0, 0, M(0), M(0), C(0)};
+    if (gx < nx && gy < ny) fs4_own_load<C, M>(p, (uint32_t)gx + (uint32_t)gy * (uint32_t)nx, own[k]);
+  }
+  // masks of the flags after stream-collide: every flag byte a lane needs is
+  // loaded first, so the loads of all its row-words are in flight together
+  const int lane = tid & 31, warp = tid >> 5;
+  const int xw = tx * kTX - 32 + lane;  // word 0 starts one word left of the tile
+  constexpr int kRW = kR * kW, kIters = (kRW + kWarps - 1) / kWarps;
+  uint8_t fv[kIters];
+#pragma unroll
+  for (int k = 0; k < kIters; k++) {
+    const int rw = warp + k * kWarps;
+    const int r = rw / kW, c = rw % kW;
+    fv[k] = rw < kRW ? flags[wrapi(xw + 32 * c, nx) + wrapi(ty * kTY - kHalo + r, ny) * nx] : 0;
+  }
+#pragma unroll
+  for (int k = 0; k < kIters; k++) {
+    const int rw = warp + k * kWarps;  // the same for the whole warp
+    if (rw >= kRW) break;
+    const int r = rw / kW, c = rw % kW;
+    const uint8_t f = fv[k];
+    // ballots of the flag bits; the masks a row needs are formed from them:
+    // the outer halo rows only feed FS_2's IF dilation, the next rows also
+    // FS_2's rewrite, the inner ten rows everything (warp-uniform branches)
+    const uint32_t bF = __ballot_sync(0xffffffffu, (f & kFluid) != 0);
+    const uint32_t bI = __ballot_sync(0xffffffffu, (f & kInterface) != 0);
+    if (lane == 0) sm.a[r][c] = bF & bI;
+    if (r == 0 || r == kR - 1) continue;
+    const uint32_t bG = __ballot_sync(0xffffffffu, (f & kGas) != 0);
+    const uint32_t bGI = __ballot_sync(0xffffffffu, (f & kGasInterface) != 0);
+    if (lane == 0) {
+      sm.gas[r][c] = bG;
+      sm.gonly[r][c] = bG & ~bI;
+      sm.gi[r][c] = bGI;
+      sm.it[r][c] = bI;
+    }
+    if (r == 1 || r == kR - 2) continue;
+    const uint32_t bIn = __ballot_sync(0xffffffffu, (f & kInlet) != 0);
+    const uint32_t bSk = __ballot_sync(0xffffffffu, (f & (kWall | kMovingWall | kInlet)) != 0);
+    if (lane == 0) {
+      sm.fl[r][c] = bF & ~bIn;
+      sm.fb[r][c] = bF;
+      sm.sk[r][c] = bSk;
+    }
+  }
+  __syncthreads();
+  // FS_2 on rows 1 .. kR-2: next to an IF cell, IG -> I and G -> GI
+  if (tid < (kR - 2) * kW) {
+    const int r = 1 + tid / kW, c = tid % kW;
+    const uint32_t any_if = dilate8<TW>(sm.a, r, c);
+    const uint32_t p1 = sm.gas[r][c] & ~any_if;
+    const uint32_t p7 = sm.gi[r][c] | (any_if & sm.gonly[r][c]);
+    sm.anyif[r][c] = any_if;
+    sm.p1[r][c] = p1;
+    sm.p7[r][c] = p7;
+    sm.ig1[r][c] = p1 & sm.it[r][c] & ~p7;
+  }
+  __syncthreads();
+  // FS_3 on rows 2 .. kR-3: next to an IG cell, F / IF (not inlet) -> I; then
+  // FS_4's conversion and the mask of the neighbours FS_4 counts
+  if (tid < (kR - 4) * kW) {
+    const int r = 2 + tid / kW, c = tid % kW;
+    const uint32_t any_ig = dilate8<TW>(sm.ig1, r, c);
+    const uint32_t conv = sm.fl[r][c] & any_ig;
+    const uint32_t P0 = sm.fb[r][c] & ~conv, P1 = sm.p1[r][c], P2 = sm.it[r][c] | conv, P7 = sm.p7[r][c];
+    const uint32_t go = ~sm.sk[r][c];
+    const uint32_t to_plain = go & ((P0 & ~P1 & P2 & ~P7) | (~P0 & P1 & P2 & ~P7));  // IF, IG lose the I bit
+    const uint32_t from_gi = go & (~P0 & ~P1 & ~P2 & P7);                          // GI -> I
+    const uint32_t P2f = (P2 & ~to_plain) | from_gi, P7f = P7 & ~from_gi;
+    sm.anyig[r][c] = any_ig;
+    sm.cnt[r][c] = p.fs_cons ? ((P0 ^ P2f) & ~P1 & go) : ((P0 | P2f) ^ P7f);
+  }
+  __syncthreads();
+  uint32_t act = 0;
+#pragma unroll
+  for (int k = 0; k < CPT; k++) {
+    const int ly = ly0 + k * kRowStep, gy = ty * kTY + ly;
+    if (gx < nx && gy < ny && fs234_cell<S, C, M, ODD, TW>(p, sm, gx, gy, lx, ly, own[k]))
+      act |= activity(xoff + lx, ly, wact, hact);
+  }
+  return act;
 }
 
-// Activity word of a live cell at (lx, ly) in a super-tile of wact x hact cells.
-__device__ __forceinline__ uint32_t activity(int lx, int ly, int wact, int hact) {
-  const bool r = lx >= wact - kReach, l = lx < kReach, u = ly >= hact - kReach, d = ly < kReach;
-  return 1u | ((uint32_t)r << edge_bit(1, 0)) | ((uint32_t)l << edge_bit(-1, 0)) | ((uint32_t)u << edge_bit(0, 1)) |
-         ((uint32_t)d << edge_bit(0, -1)) | ((uint32_t)(u && r) << edge_bit(1, 1)) |
-         ((uint32_t)(u && l) << edge_bit(-1, 1)) | ((uint32_t)(d && r) << edge_bit(1, -1)) |
-         ((uint32_t)(d && l) << edge_bit(-1, -1));
-}
 
 // Appends super-tile t to the next step's lists (NextLists), with warp 0 of
 // the block (every lane calls it): t itself when it holds fluid or interface
@@ -505,14 +553,14 @@ __device__ __forceinline__ void append_next(const NextLists& nl, uint32_t t, uin
 }
 
 // The flag pass over one super-tile t (its kSTW / TW tiles in turn) with the
-// TW*kTY threads of the block; every thread of the block must call it.
+// TW*kTY/CPT threads of the block; every thread of the block must call it.
 // Records the super-tile's activity word in nz[t] (whose previous value, the
 // word of the last step, it reads first) and appends to the next step's
 // lists.  wact_sm: one word per warp of the block.
-template <class S, class C, class M, bool ODD, int TW>
+template <class S, class C, class M, bool ODD, int TW, int CPT = 1>
 __device__ __forceinline__ void fs234_super_tile(const KParams& p, uint32_t t, uint32_t nsx, uint32_t* nz,
                                                  const NextLists& nl, FlagMasks<TW>& sm, uint32_t* wact_sm) {
-  constexpr int kTX = TW;
+  constexpr int kTX = TW, kWarps = TW * kTY / CPT / 32;
   const int tid = threadIdx.x;
   const int sx = (int)(t % nsx), sy = (int)(t / nsx);
   const int wact = min((int)kSTW, (int)p.nx - sx * (int)kSTW), hact = min((int)kSTH, (int)p.ny - sy * (int)kSTH);
@@ -520,8 +568,7 @@ __device__ __forceinline__ void fs234_super_tile(const KParams& p, uint32_t t, u
 #pragma unroll 1
   for (int j = 0; j < (int)(kSTW / kTX); j++) {
     const int tx = sx * (int)(kSTW / kTX) + j;
-    if (tx * kTX < (int)p.nx && fs234_tile<S, C, M, ODD, TW>(p, tx, sy, tid, sm))
-      act |= activity(j * kTX + tid % kTX, tid / kTX, wact, hact);
+    if (tx * kTX < (int)p.nx) act |= fs234_tile<S, C, M, ODD, TW, CPT>(p, tx, sy, tid, sm, j * kTX, wact, hact);
     __syncthreads();
   }
   act = __reduce_or_sync(0xffffffffu, act);
@@ -529,7 +576,7 @@ __device__ __forceinline__ void fs234_super_tile(const KParams& p, uint32_t t, u
   __syncthreads();
   if (tid < 32) {
     uint32_t m = 0;
-    for (int w = 0; w < TW * kTY / 32; w++) m |= wact_sm[w];
+    for (int w = 0; w < kWarps; w++) m |= wact_sm[w];
     const uint32_t old = __shfl_sync(0xffffffffu, tid == 0 ? __ldcg(nz + t) : 0u, 0);
     if (tid == 0) nz[t] = m;
     append_next(nl, t, m, old, (uint32_t)tid);

@@ -75,18 +75,24 @@ __global__ void k_apply_recon(const __grid_constant__ KParams p, uint32_t odd) {
 
 // The listed super-tiles: each block runs the flag pass on a super-tile,
 // records its activity word in nz and appends to the next step's lists.
-template <class S, class C, class M, bool ODD, int TW>
-__global__ void __launch_bounds__(TW* kTY, TW == 128 ? FLB_FS_WIDE_MIN_BLOCKS : 6)
+// TW x 8 tiles, CPT cells per thread.
+template <int TW, int CPT>
+constexpr int fs234_min_blocks() {
+  return TW == 128 ? (CPT == 1 ? FLB_FS_WIDE_MIN_BLOCKS : CPT == 2 ? FLB_FS_HALF_MIN_BLOCKS : FLB_FS_QUARTER_MIN_BLOCKS)
+                   : 6;
+}
+template <class S, class C, class M, bool ODD, int TW, int CPT>
+__global__ void __launch_bounds__(TW* kTY / CPT, fs234_min_blocks<TW, CPT>())
     k_fs234(const __grid_constant__ KParams p, const TileList tl, uint32_t* __restrict__ nz, const NextLists nl) {
   __shared__ FlagMasks<TW> sm;
-  __shared__ uint32_t wact_sm[TW * kTY / 32];
+  __shared__ uint32_t wact_sm[TW * kTY / CPT / 32];
   // the list was built by the previous step (FS_1 waited for it), so it is
   // read before waiting for stream-collide, whose flags the pass needs
   const uint32_t n = tile_count(tl);
   pdl_wait();
   pdl_trigger();
   for (uint32_t i = blockIdx.x; i < n; i += gridDim.x)
-    fs234_super_tile<S, C, M, ODD, TW>(p, tile_at(tl, i), tl.nsx, nz, nl, sm, wact_sm);
+    fs234_super_tile<S, C, M, ODD, TW, CPT>(p, tile_at(tl, i), tl.nsx, nz, nl, sm, wact_sm);
 }
 
 // ---- launchers -------------------------------------------------------------------
@@ -107,32 +113,53 @@ void launch_apply_recon(const KParams& kp, cudaStream_t st, uint32_t odd) {
   k_apply_recon<S, C><<<dim3((kp.nx + kBlock - 1) / kBlock, kp.ny), kBlock, 0, st>>>(kp, odd);
 }
 
-// The flag pass, which also lists the next step's super-tiles.  On grids of
-// up to kWideTiles super-tiles it is launched so that it may start while
-// stream-collide drains (programmatic dependent launch), with 128-wide tiles;
-// above, with an ordinary launch and 32-wide tiles (more resident warps,
-// measured faster on the 8192x2048 dam break).  Returns the number of kernels
-// launched.
-template <class S, class C, class M>
-int launch_fs234(const KParams& kp, cudaStream_t st, uint32_t odd, const TileList& tl, uint32_t grid, uint32_t* nz,
-                 const NextLists& nl) {
+// The flag pass, which also lists the next step's super-tiles, in one of its
+// launch forms (FsForm: tile width and cells per thread).  On grids of up to
+// kWideTiles super-tiles it is launched so that it may start while
+// stream-collide drains (programmatic dependent launch); above, with an
+// ordinary launch (measured faster on the 8192x2048 dam break).  Returns the
+// number of kernels launched.
+template <class S, class C, class M, int TW, int CPT>
+void launch_fs234_form(const KParams& kp, cudaStream_t st, uint32_t odd, const TileList& tl, uint32_t grid,
+                       uint32_t* nz, const NextLists& nl) {
+  constexpr int threads = TW * kTY / CPT;
   if (tl.ntiles <= kWideTiles) {
-    if (odd) launch_pdl(k_fs234<S, C, M, true, 128>, grid, 128 * kTY, st, kp, tl, nz, nl);
-    else launch_pdl(k_fs234<S, C, M, false, 128>, grid, 128 * kTY, st, kp, tl, nz, nl);
-    return 1;
+    if (odd) launch_pdl(k_fs234<S, C, M, true, TW, CPT>, grid, threads, st, kp, tl, nz, nl);
+    else launch_pdl(k_fs234<S, C, M, false, TW, CPT>, grid, threads, st, kp, tl, nz, nl);
+  } else {
+    if (odd) k_fs234<S, C, M, true, TW, CPT><<<grid, threads, 0, st>>>(kp, tl, nz, nl);
+    else k_fs234<S, C, M, false, TW, CPT><<<grid, threads, 0, st>>>(kp, tl, nz, nl);
   }
-  if (odd) k_fs234<S, C, M, true, 32><<<grid, 32 * kTY, 0, st>>>(kp, tl, nz, nl);
-  else k_fs234<S, C, M, false, 32><<<grid, 32 * kTY, 0, st>>>(kp, tl, nz, nl);
-  return 1;
 }
 
 template <class S, class C, class M>
-int fs_blocks_per_sm(int which) {
+int launch_fs234(const KParams& kp, cudaStream_t st, uint32_t odd, const TileList& tl, uint32_t grid, uint32_t* nz,
+                 const NextLists& nl, int form) {
+  switch (form) {
+    case FS_FORM_W32: launch_fs234_form<S, C, M, 32, 1>(kp, st, odd, tl, grid, nz, nl); break;
+    case FS_FORM_W128X2: launch_fs234_form<S, C, M, 128, 2>(kp, st, odd, tl, grid, nz, nl); break;
+    case FS_FORM_W128X4: launch_fs234_form<S, C, M, 128, 4>(kp, st, odd, tl, grid, nz, nl); break;
+    default: launch_fs234_form<S, C, M, 128, 1>(kp, st, odd, tl, grid, nz, nl); break;
+  }
+  return 1;
+}
+
+// Resident blocks per SM of FS_1 (which 0) or of the flag pass in the given
+// form (which 1).
+template <class S, class C, class M, int TW, int CPT>
+int fs234_blocks_per_sm() {
+  int n = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fs234<S, C, M, false, TW, CPT>, TW * kTY / CPT, 0);
+  return n;
+}
+template <class S, class C, class M>
+int fs_blocks_per_sm(int which, int form) {
   int n = 0;
   if (which == 0) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fs1<S, C, M, true, false>, kFs1Block, 0);
-  else if (which == 1)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fs234<S, C, M, false, 128>, 128 * kTY, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_fs234<S, C, M, false, 32>, 32 * kTY, 0);
+  else if (form == FS_FORM_W32) n = fs234_blocks_per_sm<S, C, M, 32, 1>();
+  else if (form == FS_FORM_W128X2) n = fs234_blocks_per_sm<S, C, M, 128, 2>();
+  else if (form == FS_FORM_W128X4) n = fs234_blocks_per_sm<S, C, M, 128, 4>();
+  else n = fs234_blocks_per_sm<S, C, M, 128, 1>();
   return n > 0 ? n : 1;
 }
 
@@ -141,8 +168,8 @@ int fs_blocks_per_sm(int which) {
                                     const ListClear&);                                                          \
   template void launch_apply_recon<S, C, M>(const KParams&, cudaStream_t, uint32_t);                             \
   template int launch_fs234<S, C, M>(const KParams&, cudaStream_t, uint32_t, const TileList&, uint32_t, uint32_t*,   \
-                                     const NextLists&);                                                          \
-  template int fs_blocks_per_sm<S, C, M>(int);
+                                     const NextLists&, int);                                                     \
+  template int fs_blocks_per_sm<S, C, M>(int, int);
 FLB_FOR_EACH_VARIANT(FLB_INSTANTIATE)
 #undef FLB_INSTANTIATE
 

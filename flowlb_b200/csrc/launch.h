@@ -47,9 +47,13 @@ template <class S, class C, class M>
 void launch_apply_recon(const KParams& kp, cudaStream_t st, uint32_t odd);
 template <class S, class C, class M>
 int launch_fs234(const KParams& kp, cudaStream_t st, uint32_t odd, const TileList& tl, uint32_t grid, uint32_t* nz,
-                 const NextLists& nl);
+                 const NextLists& nl, int form);
+// launch forms of the flag pass: tile width x cells per thread (threads per
+// block = width * 8 / cells per thread)
+enum FsForm { FS_FORM_W128X1 = 0, FS_FORM_W32 = 1, FS_FORM_W128X2 = 2, FS_FORM_W128X4 = 4 };
+// resident blocks per SM of FS_1 (which 0) or of the flag pass in `form` (which 1)
 template <class S, class C, class M>
-int fs_blocks_per_sm(int which);  // 0: FS_1, 1: FS_2..4 on 128-wide tiles, 2: on 32-wide tiles
+int fs_blocks_per_sm(int which, int form);
 
 // the free-surface step as one persistent cooperative kernel (k_fsp.cu):
 // a.steps steps per launch, `grid` CTAs of 1024 threads all resident at once

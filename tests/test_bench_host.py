@@ -59,3 +59,16 @@ def test_clock_sampler_nvidia_smi_lines():
     s = c.summary()
     assert s["samples"] == 2 and s["sm_max_mhz"] == 1965 and s["reasons"] == ["sw_power_cap"]
     assert s["source"].startswith("nvidia-smi")
+
+
+def test_algorithmic_bytes_per_pass():
+    """Per fluid or interface cell: stream-collide 86 B (+9 B per interface
+    cell), FS_1 93 B, the flag pass 39 B with FP32 populations; FP16S
+    storage halves the population bytes only."""
+    counts = {"fluid": 1000, "interface": 10, "gas": 5000, "wall": 100}
+    b32 = bench.algorithmic_bytes(counts)
+    assert b32 == {"stream_collide": 1010 * 86.0 + 10 * 9.0, "fs1": 1010 * 93.0, "fs234": 1010 * 39.0}
+    b16 = bench.algorithmic_bytes(counts, 2.0)
+    assert b16["stream_collide"] == 1010 * (86.0 - 36.0) + 10 * 9.0
+    assert b16["fs1"] == 1010 * (93.0 - 34.0)
+    assert b16["fs234"] == b32["fs234"]

@@ -287,6 +287,24 @@ def test_long_violent_free_surface_run_matches_oracle(kv):
     s.close()
 
 
+@pytest.mark.parametrize("form", ["32", "128x1", "128x2", "128x4"])
+@pytest.mark.parametrize("shape", [(1280, 320), (4352, 1024)], ids=["400-tiles", "4352-tiles"])
+def test_flag_pass_launch_forms_match_oracle(monkeypatch, form, shape):
+    """The flag pass in each launch form (tile width x cells per thread:
+    32x1, 128x1, 128x2, 128x4; FLB_FS_FLAG_FORM, read at creation), on a
+    grid below and one above 4,096 super-tiles (launched with and without
+    programmatic dependent launch), against the oracle at every check."""
+    monkeypatch.setenv("FLB_FS_FLAG_FORM", form)
+    c = cases.small_dam_break(*shape)
+    s, o = make_pair(c.flags, O.F32, free_surface=True, bb=O.BB_HALFWAY, fs_mode=O.FS_CONSERVATIVE, tau=0.55,
+                     fy=-2e-4, u_max=0.25, arith=O.ARITH_FUSED)
+    for n in ((1, 2, 97, 200) if shape[0] < 4000 else (1, 2, 60)):
+        s.step(n)
+        o.step(n)
+        assert_same_state(s, o, O.F32, True, f"form {form} t={o.t}")
+    s.close()
+
+
 def test_inlet_outlet_match_oracle():
     flags = cases.plain_channel(96, 32).flags.copy()
     flags[1:-1, 0] = cases.INLET
