@@ -277,7 +277,7 @@ __device__ __forceinline__ void fs4_own_load(const KParams& p, uint32_t idx, Fs4
 // fluid or interface after the pass.
 template <class S, class C, class M, bool ODD, int TW>
 __device__ __forceinline__ bool fs234_cell(const KParams& p, const FlagMasks<TW>& sm, int gx, int gy, int lx, int ly,
-                                           const Fs4Own<C, M>& own) {
+                                           const Fs4Own<C, M>& own, bool quiet) {
   const int nx = (int)p.nx, ny = (int)p.ny;
   const int r = kHalo + ly, c = 1 + lx / 32, i = lx % 32;
   const uint32_t idx = (uint32_t)gx + (uint32_t)gy * (uint32_t)nx;
@@ -287,7 +287,8 @@ __device__ __forceinline__ bool fs234_cell(const KParams& p, const FlagMasks<TW>
   M* Ms = static_cast<M*>(p.mass);
   M* Exs = static_cast<M*>(p.excess);
   const C* R = static_cast<const C*>(p.rho);
-  const bool any_if = (sm.anyif[r][c] >> i) & 1u, any_ig = (sm.anyig[r][c] >> i) & 1u;
+  // (a quiet tile has no IF or IG cell near: the stages that set these bits did not run)
+  const bool any_if = !quiet && ((sm.anyif[r][c] >> i) & 1u), any_ig = !quiet && ((sm.anyig[r][c] >> i) & 1u);
   // the byte chain of the reference passes, for this cell
   uint8_t f1 = f0;
   if (any_if) {
@@ -404,42 +405,15 @@ __device__ __forceinline__ bool fs234_cell(const KParams& p, const FlagMasks<TW>
   return live;
 }
 
-// One TW x 8 tile (tile coordinates tx, ty) with the TW*8/CPT threads of the
-// block, CPT cells per thread (rows ly and ly + 8/CPT, ...); every thread of
-// the block must call it.  Returns the activity bits (activity, above) of
-// this thread's cells that are fluid or interface after the pass, with the
-// tile at column xoff of a super-tile of wact x hact cells.
-template <class S, class C, class M, bool ODD, int TW, int CPT>
-__device__ __forceinline__ uint32_t fs234_tile(const KParams& p, int tx, int ty, int tid, FlagMasks<TW>& sm,
-                                               int xoff, int wact, int hact) {
-  constexpr int kTX = TW, kW = FlagMasks<TW>::kW, kR = FlagMasks<TW>::kR;
-  constexpr int kThreads = TW * kTY / CPT, kWarps = kThreads / 32, kRowStep = kTY / CPT;
-  static_assert(kTY % CPT == 0 && kThreads >= (kR - 2) * kW, "flag pass: block too small for the stencil stages");
-  const int nx = (int)p.nx, ny = (int)p.ny;
-  const uint8_t* flags = p.flags;
-  // this thread's cells: their own values are loaded now, so that their
-  // latency overlaps the mask building and the stencil stages
-  const int lx = tid % kTX, ly0 = tid / kTX;
-  const int gx = tx * kTX + lx;
-  Fs4Own<C, M> own[CPT];
-#pragma unroll
-  for (int k = 0; k < CPT; k++) {
-    const int gy = ty * kTY + ly0 + k * kRowStep;
-    own[k] = Fs4Own<C, M>{0, 0, M(0), M(0), C(0)};
-    if (gx < nx && gy < ny) fs4_own_load<C, M>(p, (uint32_t)gx + (uint32_t)gy * (uint32_t)nx, own[k]);
-  }
-  // masks of the flags after stream-collide: every flag byte a lane needs is
-  // loaded first, so the loads of all its row-words are in flight together
+// The general stencil stages of the flag pass on a tile (every thread of the
+// block calls it): the masks of the flags after stream-collide (from the flag
+// bytes fv each warp loaded), FS_2 and FS_3 as dilations and word logic, and
+// FS_4's conversion and neighbour-count mask.
+template <int TW, int kWarps, int kIters>
+__device__ __forceinline__ void fs234_stages(const KParams& p, FlagMasks<TW>& sm, const uint8_t (&fv)[kIters],
+                                             int tid) {
+  constexpr int kW = FlagMasks<TW>::kW, kR = FlagMasks<TW>::kR, kRW = kR * kW;
   const int lane = tid & 31, warp = tid >> 5;
-  const int xw = tx * kTX - 32 + lane;  // word 0 starts one word left of the tile
-  constexpr int kRW = kR * kW, kIters = (kRW + kWarps - 1) / kWarps;
-  uint8_t fv[kIters];
-#pragma unroll
-  for (int k = 0; k < kIters; k++) {
-    const int rw = warp + k * kWarps;
-    const int r = rw / kW, c = rw % kW;
-    fv[k] = rw < kRW ? flags[wrapi(xw + 32 * c, nx) + wrapi(ty * kTY - kHalo + r, ny) * nx] : 0;
-  }
 #pragma unroll
   for (int k = 0; k < kIters; k++) {
     const int rw = warp + k * kWarps;  // the same for the whole warp
@@ -498,15 +472,89 @@ __device__ __forceinline__ uint32_t fs234_tile(const KParams& p, int tx, int ty,
     sm.cnt[r][c] = p.fs_cons ? ((P0 ^ P2f) & ~P1 & go) : ((P0 | P2f) ^ P7f);
   }
   __syncthreads();
+}
+
+// One TW x 8 tile (tile coordinates tx, ty) with the TW*8/CPT threads of the
+// block, CPT cells per thread (rows ly and ly + 8/CPT, ...); every thread of
+// the block must call it.  Returns the activity bits (activity, above) of
+// this thread's cells that are fluid or interface after the pass, with the
+// tile at column xoff of a super-tile of wact x hact cells.
+template <class S, class C, class M, bool ODD, int TW, int CPT>
+__device__ __forceinline__ uint32_t fs234_tile(const KParams& p, int tx, int ty, int tid, FlagMasks<TW>& sm,
+                                               int xoff, int wact, int hact) {
+  constexpr int kTX = TW, kW = FlagMasks<TW>::kW, kR = FlagMasks<TW>::kR;
+  constexpr int kThreads = TW * kTY / CPT, kWarps = kThreads / 32, kRowStep = kTY / CPT;
+  static_assert(kTY % CPT == 0 && kThreads >= (kR - 2) * kW, "flag pass: block too small for the stencil stages");
+  const int nx = (int)p.nx, ny = (int)p.ny;
+  const uint8_t* flags = p.flags;
+  // this thread's cells: their own values are loaded now, so that their
+  // latency overlaps the mask building and the stencil stages
+  const int lx = tid % kTX, ly0 = tid / kTX;
+  const int gx = tx * kTX + lx;
+  Fs4Own<C, M> own[CPT];
+#pragma unroll
+  for (int k = 0; k < CPT; k++) {
+    const int gy = ty * kTY + ly0 + k * kRowStep;
+    own[k] = Fs4Own<C, M>{0, 0, M(0), M(0), C(0)};
+    if (gx < nx && gy < ny) fs4_own_load<C, M>(p, (uint32_t)gx + (uint32_t)gy * (uint32_t)nx, own[k]);
+  }
+  // masks of the flags after stream-collide: every flag byte a lane needs is
+  // loaded first, so the loads of all its row-words are in flight together
+  const int lane = tid & 31, warp = tid >> 5;
+  const int xw = tx * kTX - 32 + lane;  // word 0 starts one word left of the tile
+  constexpr int kRW = kR * kW, kIters = (kRW + kWarps - 1) / kWarps;
+  // a window inside the grid is addressed directly; one that crosses an
+  // edge wraps (periodic)
+  const int wx0 = tx * kTX - 32, wy0 = ty * kTY - kHalo;
+  const bool inner = wx0 >= 0 && wx0 + 32 * kW <= nx && wy0 >= 0 && wy0 + kR <= ny;
+  const uint8_t* wbase = flags + (inner ? xw + wy0 * nx : 0);
+  uint8_t fv[kIters];
+#pragma unroll
+  for (int k = 0; k < kIters; k++) {
+    const int rw = warp + k * kWarps;
+    const int r = rw / kW, c = rw % kW;
+    fv[k] = rw >= kRW ? 0
+            : inner   ? wbase[r * nx + 32 * c]
+                      : flags[wrapi(xw + 32 * c, nx) + wrapi(wy0 + r, ny) * nx];
+  }
+  // A quiet tile: no gas, interface or gas-interface cell in the loaded
+  // window (the tile, its 3-row halo and a word on either side: all that the
+  // three stencils reach).  There FS_2 and FS_3 change no flag and FS_4
+  // converts none, so of the masks only FS_4's neighbour count is needed:
+  // fluid cells that are not solid or inlet (conservative mode; all fluid
+  // cells in the reference mode), exactly what the general stages give when
+  // no IF, IG or GI cell is near.
+  bool nq = false;
+#pragma unroll
+  for (int k = 0; k < kIters; k++) nq |= (fv[k] & (kGas | kInterface | kGasInterface)) != 0;
+  const bool quiet = __syncthreads_or(nq) == 0;
+  if (quiet) {
+    const bool cons = p.fs_cons != 0;
+#pragma unroll
+    for (int k = 0; k < kIters; k++) {
+      const int rw = warp + k * kWarps;  // the same for the whole warp
+      if (rw >= kRW) break;
+      const int r = rw / kW, c = rw % kW;
+      if (r < 2 || r > kR - 3) continue;
+      const uint8_t f = fv[k];
+      const bool counted = (f & kFluid) && !(cons && (f & (kWall | kMovingWall | kInlet)));
+      const uint32_t b = __ballot_sync(0xffffffffu, counted);
+      if (lane == 0) sm.cnt[r][c] = b;
+    }
+    __syncthreads();
+  } else {
+    fs234_stages<TW, kWarps, kIters>(p, sm, fv, tid);
+  }
   uint32_t act = 0;
 #pragma unroll
   for (int k = 0; k < CPT; k++) {
     const int ly = ly0 + k * kRowStep, gy = ty * kTY + ly;
-    if (gx < nx && gy < ny && fs234_cell<S, C, M, ODD, TW>(p, sm, gx, gy, lx, ly, own[k]))
+    if (gx < nx && gy < ny && fs234_cell<S, C, M, ODD, TW>(p, sm, gx, gy, lx, ly, own[k], quiet))
       act |= activity(xoff + lx, ly, wact, hact);
   }
   return act;
 }
+
 
 
 // Appends super-tile t to the next step's lists (NextLists), with warp 0 of
