@@ -9,20 +9,31 @@
 namespace flb {
 
 // FS_1 on the listed super-tiles, one row of a super-tile per warp.
-// FS_1 blocks: 512 threads, two per SM at 64 registers, so that a step's
-// listed super-tiles (a few hundred on a 2048x512 dam break) run in one wave.
-constexpr int kFs1Block = 512;
+// FS_1 blocks: kFs1Block threads (512: two cells per thread and super-tile,
+// x and x + 64 of a row; 1024: one cell per thread), FLB_FS1_MIN_BLOCKS per
+// SM.  Measured on a B200 (dam break, step time at 2048x512 / FS_1 time at
+// 8192x2048): 512 threads, two blocks per SM (64 registers) 28.4 / 83 us;
+// 1024 threads at 32 registers 33.3 / 103 us and at 64 registers 29.8 /
+// 93 us; 512 threads at 40 registers 33.1 / 90 us (the spills cost more than
+// the added warps gain).
+#ifndef FLB_FS1_BLOCK
+#define FLB_FS1_BLOCK 512
+#endif
+#ifndef FLB_FS1_MIN_BLOCKS
+#define FLB_FS1_MIN_BLOCKS 2
+#endif
+constexpr int kFs1Block = FLB_FS1_BLOCK;
 // lc: the next step's list lengths and marks, cleared here for this step's
 // flag pass.
 template <class S, class C, class M, bool HW, bool ODD>
-__global__ void __launch_bounds__(kFs1Block, 2) k_fs1(const __grid_constant__ KParams p, const TileList tl,
-                                                      const ListClear lc) {
+__global__ void __launch_bounds__(kFs1Block, FLB_FS1_MIN_BLOCKS) k_fs1(const __grid_constant__ KParams p,
+                                                                       const TileList tl, const ListClear lc) {
   pdl_wait();
   pdl_trigger();
   clear_next_lists(lc);
-  // two cells per thread and super-tile, x and x + 64 of one row
-  constexpr uint32_t kCpr = kFs1Block / 32 / kSTH;
-  static_assert(2 * 32 * kCpr == kSTW, "FS_1: two cells per thread and super-tile");
+  constexpr uint32_t kCpr = kFs1Block / 32 / kSTH;     // warps per row of a super-tile
+  constexpr uint32_t kCells = kSTW / (32u * kCpr);     // cells per thread and super-tile
+  static_assert(kCells * 32u * kCpr == kSTW && kCells <= 2u, "FS_1: one or two cells per thread and super-tile");
   const uint32_t n = tile_count(tl);
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t row = warp % kSTH, chunk = warp / kSTH;
@@ -32,19 +43,19 @@ __global__ void __launch_bounds__(kFs1Block, 2) k_fs1(const __grid_constant__ KP
     const uint32_t y = (t / tl.nsx) * kSTH + row;
     if (y >= p.ny) continue;
     const uint32_t xa = (t % tl.nsx) * kSTW + chunk * 32u + lane, xc = xa + 32u * kCpr;
-    // both cells' flags and wall masks first: one round trip for the two
+    // the cells' flags and wall masks first: one round trip for both
     uint8_t fa = kGas, fc = kGas;
     uint32_t ma = 0, mc = 0;
     if (xa < nx) {
       fa = p.flags[xa + y * nx];
       if (HW) ma = p.nbmask[xa + y * nx];
     }
-    if (xc < nx) {
+    if (kCells == 2u && xc < nx) {
       fc = p.flags[xc + y * nx];
       if (HW) mc = p.nbmask[xc + y * nx];
     }
     if (xa < nx) fs1_cell<S, C, M, HW, ODD>(p, xa, y, fa, ma);
-    if (xc < nx) fs1_cell<S, C, M, HW, ODD>(p, xc, y, fc, mc);
+    if (kCells == 2u && xc < nx) fs1_cell<S, C, M, HW, ODD>(p, xc, y, fc, mc);
   }
 }
 
