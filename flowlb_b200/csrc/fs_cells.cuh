@@ -274,10 +274,12 @@ __device__ __forceinline__ void fs4_own_load(const KParams& p, uint32_t idx, Fs4
 // The per-cell end of the flag pass: the byte chain of FS_2, FS_3 and FS_4 for
 // cell (gx, gy) at (lx, ly) in the tile, from the masks the stencil stages
 // left in sm, and the FS_3 / FS_4 field updates.  Returns whether the cell is
-// fluid or interface after the pass.
-template <class S, class C, class M, bool ODD, int TW>
+// fluid or interface after the pass.  Q: the cell lies in a quiet tile (no
+// gas, interface or gas-interface cell within reach), where the byte chain
+// leaves the flag as it is and no cell turns from gas to interface.
+template <class S, class C, class M, bool ODD, int TW, bool Q>
 __device__ __forceinline__ bool fs234_cell(const KParams& p, const FlagMasks<TW>& sm, int gx, int gy, int lx, int ly,
-                                           const Fs4Own<C, M>& own, bool quiet) {
+                                           const Fs4Own<C, M>& own) {
   const int nx = (int)p.nx, ny = (int)p.ny;
   const int r = kHalo + ly, c = 1 + lx / 32, i = lx % 32;
   const uint32_t idx = (uint32_t)gx + (uint32_t)gy * (uint32_t)nx;
@@ -288,7 +290,7 @@ __device__ __forceinline__ bool fs234_cell(const KParams& p, const FlagMasks<TW>
   M* Exs = static_cast<M*>(p.excess);
   const C* R = static_cast<const C*>(p.rho);
   // (a quiet tile has no IF or IG cell near: the stages that set these bits did not run)
-  const bool any_if = !quiet && ((sm.anyif[r][c] >> i) & 1u), any_ig = !quiet && ((sm.anyig[r][c] >> i) & 1u);
+  const bool any_if = !Q && ((sm.anyif[r][c] >> i) & 1u), any_ig = !Q && ((sm.anyig[r][c] >> i) & 1u);
   // the byte chain of the reference passes, for this cell
   uint8_t f1 = f0;
   if (any_if) {
@@ -302,7 +304,7 @@ __device__ __forceinline__ bool fs234_cell(const KParams& p, const FlagMasks<TW>
     if (e != kInletFluid && (e == kFluid || e == kIF) && any_ig) f3 = (uint8_t)((f3 & ~kIF) | kInterface);
   }
   uint8_t fin = f3;
-  if (!(fin & (kWall | kMovingWall | kInlet))) {
+  if (!Q && !(fin & (kWall | kMovingWall | kInlet))) {
     const uint8_t sw = fin & (kFGI | kGasInterface);
     if (sw == kIF || sw == kIG) fin = (uint8_t)(fin & ~kInterface);
     else if (sw == kGasInterface) fin = (uint8_t)((fin & ~kGasInterface) | kInterface);
@@ -324,7 +326,7 @@ __device__ __forceinline__ bool fs234_cell(const KParams& p, const FlagMasks<TW>
   const C* U = static_cast<const C*>(p.u);
   // FS_3 fields: a gas->interface cell starts from feq of the neighbour
   // average (calculateAverageValuesNeighbors2D, accumulating in float)
-  if ((f1 & (kGasInterface | kIG)) == kGasInterface) {
+  if (!Q && (f1 & (kGasInterface | kIG)) == kGasInterface) {
     uint32_t nb[9];
     neighbours((uint32_t)gx, (uint32_t)gy, (uint32_t)nx, (uint32_t)ny, nb);
     float count = 0.0f, lrho = 0.0f, lux = 0.0f, luy = 0.0f;
@@ -549,7 +551,9 @@ __device__ __forceinline__ uint32_t fs234_tile(const KParams& p, int tx, int ty,
 #pragma unroll
   for (int k = 0; k < CPT; k++) {
     const int ly = ly0 + k * kRowStep, gy = ty * kTY + ly;
-    if (gx < nx && gy < ny && fs234_cell<S, C, M, ODD, TW>(p, sm, gx, gy, lx, ly, own[k], quiet))
+    if (gx < nx && gy < ny &&
+        (quiet ? fs234_cell<S, C, M, ODD, TW, true>(p, sm, gx, gy, lx, ly, own[k])
+               : fs234_cell<S, C, M, ODD, TW, false>(p, sm, gx, gy, lx, ly, own[k])))
       act |= activity(xoff + lx, ly, wact, hact);
   }
   return act;
