@@ -184,6 +184,53 @@ __device__ __forceinline__ uint32_t tile_count(const TileList& tl) {
 }
 __device__ __forceinline__ uint32_t tile_at(const TileList& tl, uint32_t i) { return tl.all ? i : tl.list[i]; }
 
+// ---- L2 prefetch of a super-tile ------------------------------------------------
+// Bulk L2 prefetch (a hint with no reply) of `bytes` bytes from `p`, rounded
+// inward to 16-byte boundaries so that it never leaves the range given.
+__device__ __forceinline__ void l2_prefetch_inward(const char* p, uint32_t bytes) {
+  const uintptr_t a = ((uintptr_t)p + 15u) & ~(uintptr_t)15u, e = ((uintptr_t)p + bytes) & ~(uintptr_t)15u;
+  if (e > a) asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a), "r"((uint32_t)(e - a)) : "memory");
+}
+
+// The rows a listed pass reads for super-tile t, prefetched into L2 while the
+// block works on its current super-tile: the nine population slots (pop
+// bytes per value) of rows y0-1 .. y0+8, the flags of the same rows, and
+// (with_mass) the mass of rows y0 .. y0+7 and the excess of rows y0-1 ..
+// y0+8 (FP64 or FP32, m bytes), each row over the super-tile's columns.
+// Rows outside the grid are left out (their periodic images are read
+// normally).  Thread k of the block issues task k; the block needs at least
+// 9 * 10 + 10 (+ 8 + 10) threads.  FS_1 uses it (8192x2048 dam break: 83 ->
+// 80 us per step); in the listed stream-collide it measured slower (76.5 ->
+// 85.4 us), so that pass does without.
+__device__ __forceinline__ void prefetch_super_tile(const KParams& p, uint32_t t, uint32_t nsx, uint32_t pop,
+                                                   bool with_mass, uint32_t m) {
+  const uint32_t k = threadIdx.x;
+  const uint32_t x0 = (t % nsx) * kSTW, y0 = (t / nsx) * kSTH;
+  const uint32_t w = min(kSTW, p.nx - x0);
+  int row = -1;
+  const char* base = nullptr;
+  uint32_t elem = 0;
+  if (k < 90u) {  // populations: slot k / 10, row y0 - 1 + k % 10
+    row = (int)y0 - 1 + (int)(k % 10u);
+    base = static_cast<const char*>(p.slot[k / 10u]);
+    elem = pop;
+  } else if (k < 100u) {  // flags
+    row = (int)y0 - 1 + (int)(k - 90u);
+    base = reinterpret_cast<const char*>(p.flags);
+    elem = 1;
+  } else if (with_mass && k < 108u) {  // mass
+    row = (int)y0 + (int)(k - 100u);
+    base = static_cast<const char*>(p.mass);
+    elem = m;
+  } else if (with_mass && k < 118u) {  // excess
+    row = (int)y0 - 1 + (int)(k - 108u);
+    base = static_cast<const char*>(p.excess);
+    elem = m;
+  }
+  if (row < 0 || row >= (int)p.ny) return;
+  l2_prefetch_inward(base + ((size_t)row * p.nx + x0) * elem, w * elem);
+}
+
 template <class S>
 __device__ __forceinline__ S* slotp(const KParams& p, int s) {
   return static_cast<S*>(p.slot[s]);

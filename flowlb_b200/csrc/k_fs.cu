@@ -34,12 +34,15 @@ __global__ void __launch_bounds__(kFs1Block, FLB_FS1_MIN_BLOCKS) k_fs1(const __g
   constexpr uint32_t kCpr = kFs1Block / 32 / kSTH;     // warps per row of a super-tile
   constexpr uint32_t kCells = kSTW / (32u * kCpr);     // cells per thread and super-tile
   static_assert(kCells * 32u * kCpr == kSTW && kCells <= 2u, "FS_1: one or two cells per thread and super-tile");
+  static_assert(kFs1Block >= 118, "FS_1: prefetch_super_tile needs 118 threads");
   const uint32_t n = tile_count(tl);
   const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
   const uint32_t row = warp % kSTH, chunk = warp / kSTH;
   const uint32_t nx = p.nx;
   for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) {
     const uint32_t t = tile_at(tl, i);
+    // the block's next super-tile into L2 while this one is worked on
+    if (i + gridDim.x < n) prefetch_super_tile(p, tile_at(tl, i + gridDim.x), tl.nsx, sizeof(S), true, sizeof(M));
     const uint32_t y = (t / tl.nsx) * kSTH + row;
     if (y >= p.ny) continue;
     const uint32_t xa = (t % tl.nsx) * kSTW + chunk * 32u + lane, xc = xa + 32u * kCpr;

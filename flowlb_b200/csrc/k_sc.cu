@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(kVecBlock, FU ? (std::is_same<S, __half>::valu
 // Free surface, vector data path: the listed super-tiles, each row of a
 // super-tile taken by kSTW / (32 V) warps (one warp for FP32 and FP16S).
 template <class S>
-constexpr int list_vec_block() {
+__host__ __device__ constexpr int list_vec_block() {
   return (int)kSTH * (int)(kSTW / (32u * (uint32_t)Lanes<S>::V)) * 32;
 }
 template <class S, class C, class M, bool HW, bool ODD, bool FU>
