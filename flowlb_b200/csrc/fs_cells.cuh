@@ -267,8 +267,10 @@ __device__ __forceinline__ void fs4_own_load(const KParams& p, uint32_t idx, Fs4
   o.f0 = p.flags[idx];
   o.old = p.flags_out[idx];
   o.m = static_cast<const M*>(p.mass)[idx];
-  o.ex = static_cast<const M*>(p.excess)[idx];
   o.rho = static_cast<const C*>(p.rho)[idx];
+  // the old excess is compared only by a gas cell that stays gas (write
+  // skipping), so only a cell with the gas bit reads it
+  o.ex = (o.f0 & kGas) ? static_cast<const M*>(p.excess)[idx] : M(0);
 }
 
 // The per-cell end of the flag pass: the byte chain of FS_2, FS_3 and FS_4 for
