@@ -305,6 +305,24 @@ def test_flag_pass_launch_forms_match_oracle(monkeypatch, form, shape):
     s.close()
 
 
+@pytest.mark.parametrize("form", ["128x1", "128x2"])
+def test_reference_mode_quiet_tiles_match_oracle(monkeypatch, form):
+    """The reference free-surface mode (FlowLB's rules, implicit walls,
+    reference arithmetic, FP32 mass) on a dam break wide and tall enough
+    that many super-tiles are quiet (deep fluid: the flag pass builds only
+    FS_4's count mask, which in this mode counts every fluid cell), against
+    the oracle at every check."""
+    monkeypatch.setenv("FLB_FS_FLAG_FORM", form)
+    c = cases.small_dam_break(1280, 320)
+    s, o = make_pair(c.flags, O.F32_M32, free_surface=True, bb=O.BB_IMPLICIT, fs_mode=O.FS_REFERENCE, tau=0.55,
+                     fy=-2e-4, u_max=0.25, arith=O.ARITH_REFERENCE)
+    for n in (1, 2, 97, 100):
+        s.step(n)
+        o.step(n)
+        assert_same_state(s, o, O.F32_M32, True, f"form {form} t={o.t}")
+    s.close()
+
+
 def test_inlet_outlet_match_oracle():
     flags = cases.plain_channel(96, 32).flags.copy()
     flags[1:-1, 0] = cases.INLET
