@@ -619,11 +619,13 @@ __device__ __forceinline__ void fs234_super_tile(const KParams& p, uint32_t t, u
   const int sx = (int)(t % nsx), sy = (int)(t / nsx);
   const int wact = min((int)kSTW, (int)p.nx - sx * (int)kSTW), hact = min((int)kSTH, (int)p.ny - sy * (int)kSTH);
   uint32_t act = 0;
+  // (no barrier between tiles: a tile's first write to sm comes after its
+  // __syncthreads_or, which no thread passes before every thread has
+  // finished reading the previous tile's masks)
 #pragma unroll 1
   for (int j = 0; j < (int)(kSTW / kTX); j++) {
     const int tx = sx * (int)(kSTW / kTX) + j;
     if (tx * kTX < (int)p.nx) act |= fs234_tile<S, C, M, ODD, TW, CPT>(p, tx, sy, tid, sm, j * kTX, wact, hact);
-    __syncthreads();
   }
   act = __reduce_or_sync(0xffffffffu, act);
   if ((tid & 31) == 0) wact_sm[tid >> 5] = act;
