@@ -502,8 +502,7 @@ def side_measurements(args, device, E, cases, peak, uuid):
     spec = [(e.flags, e.tau, e.fx, 0.0) for e in ens]
     cells = sum(e.flags.size for e in ens)
 
-    def batch():
-        b = E.Batch(spec, autotune=1, device=device)
+    def timed_batch(b):
         b.step(2)
         b.sync()
         torch.cuda.synchronize()
@@ -511,10 +510,23 @@ def side_measurements(args, device, E, cases, peak, uuid):
         b.step(n_b)
         b.sync()
         tb = time.perf_counter() - t0
-        info = b.info()
-        b.close()
         return {"cases_per_s": round(len(ens) / tb, 2), "unit": f"cases/s ({n_b} steps each)",
-                "glups": round(cells * n_b / tb / 1e9, 1), "steps_timed": n_b, "config": info, "wall_s": tb}
+                "glups": round(cells * n_b / tb / 1e9, 1), "steps_timed": n_b, "config": b.info(), "wall_s": tb}
+
+    def batch():
+        # the tuned form (the persistent kernel's shapes and the streams form)
+        b = E.Batch(spec, autotune=1, device=device)
+        res = timed_batch(b)
+        b.close()
+        return res
+
+    def batch_persistent():
+        # the persistent kernel's best shape alone: one graph-captured launch per flb_batch_step
+        b = E.Batch(spec, autotune=0, device=device)
+        b.tune(0, E.TUNE_PERSISTENT)
+        res = timed_batch(b)
+        b.close()
+        return res
 
     def loop():
         sm = torch.cuda.Stream()
@@ -533,10 +545,13 @@ def side_measurements(args, device, E, cases, peak, uuid):
         return {"cases_per_s": round(len(ens) / tl, 2), "wall_s": tl}
 
     clocked("batch_512_cases", batch)
+    clocked("batch_512_cases_persistent_kernel", batch_persistent)
     clocked("per_case_loop_512_cases", loop)
-    bt, lt = out["batch_512_cases"], out["per_case_loop_512_cases"]
-    bt["loop_cases_per_s"] = lt["cases_per_s"]
-    bt["speedup_vs_per_case_loop"] = round(lt["wall_s"] / bt["wall_s"], 3)
+    lt = out["per_case_loop_512_cases"]
+    for key in ("batch_512_cases", "batch_512_cases_persistent_kernel"):
+        bt = out[key]
+        bt["loop_cases_per_s"] = lt["cases_per_s"]
+        bt["speedup_vs_per_case_loop"] = round(lt["wall_s"] / bt["wall_s"], 3)
 
     # adjoint: backward (with checkpoint recomputation) over forward, FP64
     # (the form whose gradient meets the finite-difference check) and FP32

@@ -38,6 +38,7 @@ namespace flb {
 namespace {
 
 constexpr int kBatchMaxThreads = 1024;  // CTA sizes 256, 512 or 1024 (autotuned)
+constexpr int kMaxStreams = 64;         // streams of the streams form
 #ifndef FLB_BATCH_MIN_BLOCKS
 #define FLB_BATCH_MIN_BLOCKS 2  // two 1024-thread CTAs per SM: at most 32 registers
 #endif
@@ -484,6 +485,20 @@ struct flb_batch_s {
   int cluster = 8, clusters = 0, threads = 512, tuned = 0;
   bool team = false;
   bool vec = false;  // the vector data path (kVecCells cells per thread)
+  // FLB_BATCH_STREAMS: every case an engine handle (the single-case kernels
+  // and step graphs) on one of `nstreams` streams, longest cases first, so
+  // that the cases' step sequences run concurrently; while the form is on,
+  // the handles hold the state
+  bool streams_mode = false;
+  int nstreams = 0;
+  std::vector<flb_case_desc> descs;  // the cases (flags point into hgeo)
+  std::vector<uint8_t> hgeo;         // host copy of every case's geometry flags
+  std::vector<flb_handle> handles;
+  std::vector<uint32_t> stream_of;   // the pool stream of each case
+  std::vector<uint32_t> sorder;      // the cases longest first
+  std::vector<cudaStream_t> pool;
+  std::vector<cudaEvent_t> pool_ev;
+  cudaEvent_t start_ev = nullptr;
   uint64_t launches = 0;
   // the step graph (batch kernel + counter update) for one step count
   cudaGraph_t graph = nullptr;
@@ -533,6 +548,15 @@ void bdrop_graph(flb_batch b) {
 
 void bfree(flb_batch b) {
   bdrop_graph(b);
+  for (flb_handle h : b->handles)
+    if (h) flb_destroy(h);
+  b->handles.clear();
+  for (cudaStream_t st : b->pool) cudaStreamDestroy(st);
+  for (cudaEvent_t ev : b->pool_ev) cudaEventDestroy(ev);
+  b->pool.clear();
+  b->pool_ev.clear();
+  if (b->start_ev) cudaEventDestroy(b->start_ev);
+  b->start_ev = nullptr;
   void* bufs[] = {b->d_sf,    b->d_srho,  b->d_su,    b->d_sflags, b->d_snb,
                   b->d_f,     b->d_rho,   b->d_u,     b->d_flags, b->d_geo, b->d_nbmask,
                   b->d_tstep, b->d_cases, b->d_order, b->d_start, b->d_sync, b->d_err};
@@ -772,6 +796,136 @@ flb_status bcheck(flb_batch b) {
   return bfail(b, FLB_ERR_CUDA, "a team barrier gave up waiting; the batch state is undefined until reset");
 }
 
+// ---- the streams form (FLB_BATCH_STREAMS) -----------------------------------
+void streams_free(flb_batch b) {
+  for (flb_handle h : b->handles)
+    if (h) flb_destroy(h);
+  b->handles.clear();
+  b->streams_mode = false;
+}
+
+// The pool of nstreams streams, the cases longest first, and every case's
+// handle bound to its stream (rank k of that order on stream k % nstreams);
+// the handles are created on first use, from the cases' descriptors.
+flb_status streams_setup(flb_batch b, int nstreams) {
+  while ((int)b->pool.size() < nstreams) {
+    cudaStream_t st = nullptr;
+    FLB_BCUDA(b, cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    b->pool.push_back(st);
+    cudaEvent_t ev = nullptr;
+    FLB_BCUDA(b, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    b->pool_ev.push_back(ev);
+  }
+  if (!b->start_ev) FLB_BCUDA(b, cudaEventCreateWithFlags(&b->start_ev, cudaEventDisableTiming));
+  b->sorder.resize(b->n);
+  std::iota(b->sorder.begin(), b->sorder.end(), 0u);
+  std::stable_sort(b->sorder.begin(), b->sorder.end(), [&](uint32_t a, uint32_t c) {
+    return (uint64_t)b->nx[a] * b->ny[a] > (uint64_t)b->nx[c] * b->ny[c];
+  });
+  b->stream_of.assign(b->n, 0u);
+  for (uint32_t k = 0; k < b->n; k++) b->stream_of[b->sorder[k]] = k % (uint32_t)nstreams;
+  if (b->handles.empty()) {
+    b->handles.assign(b->n, nullptr);
+    for (uint32_t c = 0; c < b->n; c++) {
+      flb_case_desc d = b->descs[c];
+      d.device = b->device;
+      d.stream = b->pool[b->stream_of[c]];
+      const flb_status s = flb_create(&d, &b->handles[c]);
+      if (s != FLB_OK) {
+        streams_free(b);
+        return bfail(b, s, "the streams form could not create the handle of case " + std::to_string(c));
+      }
+    }
+  } else {
+    for (uint32_t c = 0; c < b->n; c++) {
+      const flb_status s = flb_set_stream(b->handles[c], b->pool[b->stream_of[c]]);
+      if (s != FLB_OK) return bfail(b, s, flb_last_error(b->handles[c]));
+    }
+  }
+  b->nstreams = nstreams;
+  return FLB_OK;
+}
+
+// Populations, density and velocity of case c between the batch's arrays
+// (rows padded to sx) and its handle (compact rows), through the scratch.
+flb_status case_state_copy(flb_batch b, uint32_t c, bool to_handle) {
+  const size_t po = b->poff[c], nx = b->nx[c], ny = b->ny[c], sx = b->sx[c];
+  const struct {
+    int field;
+    float* arr;
+    size_t rows;
+  } fs[] = {{FLB_FIELD_F, b->d_f + 9 * po, 9 * ny}, {FLB_FIELD_RHO, b->d_rho + po, ny},
+            {FLB_FIELD_U, b->d_u + 2 * po, 2 * ny}};
+  const cudaMemcpyKind dd = cudaMemcpyDeviceToDevice;
+  for (const auto& f : fs) {
+    if (to_handle) {
+      FLB_BCUDA(b, copy_rows(b->d_sf, nx * 4, f.arr, sx * 4, nx * 4, f.rows, dd, b->stream));
+      FLB_BCUDA(b, cudaStreamSynchronize(b->stream));
+      const flb_status s = flb_write_field(b->handles[c], f.field, b->d_sf, 1);  // ends with a stream sync
+      if (s != FLB_OK) return bfail(b, s, flb_last_error(b->handles[c]));
+    } else {
+      const flb_status s = flb_read_field(b->handles[c], f.field, b->d_sf, 1);  // ends with a stream sync
+      if (s != FLB_OK) return bfail(b, s, flb_last_error(b->handles[c]));
+      FLB_BCUDA(b, copy_rows(f.arr, sx * 4, b->d_sf, nx * 4, nx * 4, f.rows, dd, b->stream));
+      FLB_BCUDA(b, cudaStreamSynchronize(b->stream));
+    }
+  }
+  return FLB_OK;
+}
+
+// Into the streams form with nstreams streams: the state moves into the
+// handles.  At an even step only (a handle starts at t = 0, and the slot
+// pattern follows the step's parity).
+flb_status streams_enter(flb_batch b, int nstreams) {
+  if (b->t & 1u) return bfail(b, FLB_ERR_UNSUPPORTED, "the streams form is entered at an even step");
+  FLB_BCUDA(b, cudaStreamSynchronize(b->stream));
+  const bool was = b->streams_mode;
+  flb_status s = streams_setup(b, nstreams);
+  if (s != FLB_OK || was) return s;
+  // each handle back to t = 0 (its slot pattern then follows the batch's
+  // even step), then the batch's state copied in
+  for (uint32_t c = 0; c < b->n && s == FLB_OK; c++) {
+    s = flb_reset(b->handles[c], b->hgeo.data() + b->off[c]);
+    if (s != FLB_OK) bfail(b, s, flb_last_error(b->handles[c]));
+    else s = case_state_copy(b, c, true);
+  }
+  if (s == FLB_OK) b->streams_mode = true;
+  return s;
+}
+
+// Out of the streams form: the state moves back into the batch's arrays.
+flb_status streams_leave(flb_batch b) {
+  if (!b->streams_mode) return FLB_OK;
+  flb_status s = FLB_OK;
+  for (uint32_t c = 0; c < b->n && s == FLB_OK; c++) s = case_state_copy(b, c, false);
+  if (s != FLB_OK) return s;
+  // the persistent kernel takes the step's parity from the device counter,
+  // which the streams form's steps did not advance
+  const uint32_t t32 = (uint32_t)b->t;
+  FLB_BCUDA(b, cudaMemcpyAsync(b->d_tstep, &t32, sizeof(t32), cudaMemcpyHostToDevice, b->stream));
+  FLB_BCUDA(b, cudaStreamSynchronize(b->stream));
+  b->streams_mode = false;
+  return FLB_OK;
+}
+
+// n steps in the streams form: every case's own step graphs on its stream,
+// after the work already on the batch's stream; the batch's stream then
+// waits for every stream of the pool.
+flb_status streams_step(flb_batch b, uint64_t n) {
+  FLB_BCUDA(b, cudaEventRecord(b->start_ev, b->stream));
+  for (int k = 0; k < b->nstreams; k++) FLB_BCUDA(b, cudaStreamWaitEvent(b->pool[k], b->start_ev, 0));
+  for (uint32_t c : b->sorder) {
+    const flb_status s = flb_step(b->handles[c], n);
+    if (s != FLB_OK) return bfail(b, s, flb_last_error(b->handles[c]));
+  }
+  for (int k = 0; k < b->nstreams; k++) {
+    FLB_BCUDA(b, cudaEventRecord(b->pool_ev[k], b->pool[k]));
+    FLB_BCUDA(b, cudaStreamWaitEvent(b->stream, b->pool_ev[k], 0));
+  }
+  b->t += n;
+  return FLB_OK;
+}
+
 // Timed search over launch shapes: probe steps of the whole batch from the
 // initial state for every candidate; the fastest wins.  Each group of CTAs
 // holds one case at a time, so the number of groups sets how many bytes of
@@ -780,7 +934,9 @@ flb_status bcheck(flb_batch b) {
 // steps by default, is long enough for that reuse to show).  Hardware
 // clusters give the cheapest barrier but pack into the GPCs unevenly at 8 or
 // 16 CTAs; teams take any number of CTAs and fill every SM.
-flb_status btune(flb_batch b, uint32_t probe_steps) {
+// forms: FLB_TUNE_PERSISTENT (the persistent kernel's shapes) and / or
+// FLB_TUNE_STREAMS (the streams form with 8 and 16 streams).
+flb_status btune(flb_batch b, uint32_t probe_steps, int forms) {
   int nsm = 0;
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
   int l2 = 0;
@@ -791,13 +947,15 @@ flb_status btune(flb_batch b, uint32_t probe_steps) {
   struct Cand {
     bool team, vec;
     int cs, clusters, threads;
+    int streams;  // > 0: the streams form with that many streams
   };
   std::vector<Cand> cands;
   auto add = [&](bool team, bool vec, int cs, int k, int mx, int threads) {
+    if (!(forms & FLB_TUNE_PERSISTENT)) return;
     const int cl = std::min(std::max(k, 1), std::min(mx, (int)b->n));
     for (auto& c : cands)
       if (c.team == team && c.vec == vec && c.cs == cs && c.clusters == cl && c.threads == threads) return;
-    cands.push_back({team, vec, cs, cl, threads});
+    cands.push_back({team, vec, cs, cl, threads, 0});
   };
   // teams: every resident CTA, split into l2_fit/2 .. 2 l2_fit teams (on a
   // B200 the ensemble runs fastest with its active cases near l2_fit)
@@ -829,7 +987,15 @@ flb_status btune(flb_batch b, uint32_t probe_steps) {
     }
     add_teams(true, threads);
   }
+  // the streams form: the cases' own step graphs on 8 or 16 concurrent
+  // streams (more streams than hardware queues measured slower on a B200)
+  if (forms & FLB_TUNE_STREAMS)
+    for (int st : {8, 16}) cands.push_back({false, false, 1, 1, 0, std::min(st, kMaxStreams)});
   if (cands.empty()) return bfail(b, FLB_ERR_UNSUPPORTED, "no launch shape can run the batch");
+  if (b->streams_mode) {
+    flb_status s = streams_leave(b);
+    if (s != FLB_OK) return s;
+  }
   cudaEvent_t e0, e1;
   FLB_BCUDA(b, cudaEventCreate(&e0));
   FLB_BCUDA(b, cudaEventCreate(&e1));
@@ -837,6 +1003,19 @@ flb_status btune(flb_batch b, uint32_t probe_steps) {
   Cand win = cands[0];
   flb_status s = FLB_OK;
   for (const Cand& c : cands) {
+    b->streams_mode = false;
+    if (c.streams > 0) {
+      s = binit(b);
+      if (s == FLB_OK) s = streams_enter(b, c.streams);
+      if (s == FLB_OK) s = streams_step(b, 2);  // warm-up: the handles capture their graphs
+      if (s == FLB_OK) {
+        cudaEventRecord(e0, b->stream);
+        s = streams_step(b, probe_steps);
+        cudaEventRecord(e1, b->stream);
+      }
+      if (s == FLB_OK) FLB_BCUDA(b, cudaStreamSynchronize(b->stream));
+      b->streams_mode = false;  // the next candidate starts from the initial state again
+    } else {
     b->team = c.team;
     b->vec = c.vec;
     b->cluster = c.cs;
@@ -848,6 +1027,7 @@ flb_status btune(flb_batch b, uint32_t probe_steps) {
       cudaEventRecord(e0, b->stream);
       s = blaunch(b, probe_steps, 0);
       cudaEventRecord(e1, b->stream);
+    }
     }
     if (s != FLB_OK) {
       // a shape that does not launch is skipped; an error that outlives the
@@ -871,13 +1051,19 @@ flb_status btune(flb_batch b, uint32_t probe_steps) {
   if (s != FLB_OK) return s;
   FLB_BCUDA(b, cudaGetLastError());
   if (best == 1e30f) return bfail(b, FLB_ERR_CUDA, "no launch shape completed the probe steps");
+  b->tuned = 1;
+  if (win.streams > 0) {
+    s = binit(b);
+    if (s == FLB_OK) s = streams_enter(b, win.streams);  // the handles start from the initial state too
+    return s;
+  }
+  streams_free(b);  // not chosen: the handles' memory goes back
   b->team = win.team;
   b->vec = win.vec;
   b->cluster = win.cs;
   b->threads = win.threads;
   s = bassign(b, win.clusters);
   if (s != FLB_OK) return s;
-  b->tuned = 1;
   return binit(b);
 }
 
@@ -938,6 +1124,13 @@ FLB_API flb_status flb_batch_create(const flb_case_desc* cases, uint32_t n, int 
     b->cells += (size_t)cases[c].nx * cases[c].ny;
     b->pcells += (size_t)b->sx[c] * cases[c].ny;
     b->max_cells = std::max(b->max_cells, (size_t)cases[c].nx * cases[c].ny);
+  }
+  // the cases as given, for the handles of the streams form
+  b->hgeo.resize(b->cells);
+  b->descs.assign(cases, cases + n);
+  for (uint32_t c = 0; c < n; c++) {
+    std::memcpy(b->hgeo.data() + b->off[c], cases[c].flags, (size_t)cases[c].nx * cases[c].ny);
+    b->descs[c].flags = b->hgeo.data() + b->off[c];
   }
   auto bail = [&](flb_status s) {
     std::fprintf(stderr, "flb_batch_create: %s\n", b->err.c_str());
@@ -1000,7 +1193,7 @@ FLB_API flb_status flb_batch_create(const flb_case_desc* cases, uint32_t n, int 
   if (e != cudaSuccess) return bail(bcuda(b, e, "cudaMemcpy"));
   flb_status s = FLB_OK;
   if (autotune) {
-    s = btune(b, autotune > 1 ? (uint32_t)autotune : 100u);
+    s = btune(b, autotune > 1 ? (uint32_t)autotune : 100u, FLB_TUNE_PERSISTENT | FLB_TUNE_STREAMS);
   } else {
     int nsm = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, b->device);
@@ -1019,6 +1212,7 @@ FLB_API flb_status flb_batch_step(flb_batch b, uint64_t n) {
     return bfail(b, FLB_ERR_CUDA, "a team barrier gave up waiting in an earlier launch; call flb_batch_reset");
   if (n == 0) return FLB_OK;
   BDevice g(b->device);
+  if (b->streams_mode) return streams_step(b, n);
   return blaunch(b, n, 1);
 }
 
@@ -1031,12 +1225,26 @@ FLB_API flb_status flb_batch_sync(flb_batch b) {
 
 FLB_API flb_status flb_batch_reset(flb_batch b) {
   if (!b) return FLB_ERR_INVALID_ARGUMENT;
-  return binit(b);
+  BDevice g(b->device);
+  flb_status s = binit(b);
+  if (s == FLB_OK && b->streams_mode)
+    for (uint32_t c = 0; c < b->n && s == FLB_OK; c++) {
+      s = flb_reset(b->handles[c], b->hgeo.data() + b->off[c]);
+      if (s != FLB_OK) bfail(b, s, flb_last_error(b->handles[c]));
+    }
+  return s;
 }
 
 FLB_API flb_status flb_batch_read_field(flb_batch b, uint32_t i, int field, void* dst, int on_device) {
   if (!b || !dst || i >= b->n) return FLB_ERR_INVALID_ARGUMENT;
   BDevice g(b->device);
+  if (b->streams_mode) {
+    if (field != FLB_FIELD_F && field != FLB_FIELD_RHO && field != FLB_FIELD_U && field != FLB_FIELD_FLAGS)
+      return bfail(b, FLB_ERR_INVALID_ARGUMENT, "the batch holds populations, density, velocity and flags");
+    FLB_BCUDA(b, cudaStreamSynchronize(b->stream));
+    const flb_status s = flb_read_field(b->handles[i], field, dst, on_device);
+    return s == FLB_OK ? s : bfail(b, s, flb_last_error(b->handles[i]));
+  }
   // the state is stored with padded rows; the copy drops the padding
   const size_t po = b->poff[i], nx = b->nx[i], ny = b->ny[i], sx = b->sx[i];
   const void* src = nullptr;
@@ -1064,16 +1272,30 @@ FLB_API flb_status flb_batch_info(flb_batch b, int64_t info[8]) {
   info[5] = b->tuned;
   info[6] = b->threads;
   info[7] = (b->team ? FLB_BATCH_TEAM : FLB_BATCH_CLUSTER) | (b->vec ? FLB_BATCH_VECTOR : 0);
+  if (b->streams_mode) {
+    info[3] = 1;
+    info[4] = b->nstreams;
+    info[6] = 0;
+    info[7] = FLB_BATCH_STREAMS;
+  }
   return FLB_OK;
 }
 
 FLB_API flb_status flb_batch_set_launch(flb_batch b, int mode, int group, int groups, int threads) {
   if (!b) return FLB_ERR_INVALID_ARGUMENT;
+  if (mode == FLB_BATCH_STREAMS) {
+    if (group != 1 || groups < 1 || groups > kMaxStreams)
+      return bfail(b, FLB_ERR_INVALID_ARGUMENT,
+                   "the streams form takes group 1 and 1 to " + std::to_string(kMaxStreams) + " streams");
+    BDevice g(b->device);
+    return streams_enter(b, groups);
+  }
   const bool vec = (mode & FLB_BATCH_VECTOR) != 0;
   mode &= ~FLB_BATCH_VECTOR;
   if (mode != FLB_BATCH_CLUSTER && mode != FLB_BATCH_TEAM)
     return bfail(b, FLB_ERR_INVALID_ARGUMENT,
-                 "mode must be FLB_BATCH_CLUSTER or FLB_BATCH_TEAM, optionally with FLB_BATCH_VECTOR");
+                 "mode must be FLB_BATCH_CLUSTER or FLB_BATCH_TEAM, optionally with FLB_BATCH_VECTOR, or "
+                 "FLB_BATCH_STREAMS");
   const bool team = mode == FLB_BATCH_TEAM;
   if (!team && group != 1 && group != 2 && group != 4 && group != 8 && group != 16)
     return bfail(b, FLB_ERR_INVALID_ARGUMENT, "a cluster has 1, 2, 4, 8 or 16 CTAs");
@@ -1090,6 +1312,10 @@ FLB_API flb_status flb_batch_set_launch(flb_batch b, int mode, int group, int gr
   if (groups > mx)
     return bfail(b, FLB_ERR_UNSUPPORTED,
                  "at most " + std::to_string(mx) + " groups of this shape fit on the device at once");
+  if (b->streams_mode) {
+    const flb_status s = streams_leave(b);
+    if (s != FLB_OK) return s;
+  }
   const int pc = b->cluster, pt = b->threads;
   const bool pm = b->team, pv = b->vec;
   b->team = team;
@@ -1104,6 +1330,13 @@ FLB_API flb_status flb_batch_set_launch(flb_batch b, int mode, int group, int gr
     b->threads = pt;
   }
   return s;
+}
+
+FLB_API flb_status flb_batch_tune(flb_batch b, uint32_t probe_steps, int forms) {
+  if (!b || !(forms & (FLB_TUNE_PERSISTENT | FLB_TUNE_STREAMS))) return FLB_ERR_INVALID_ARGUMENT;
+  BDevice g(b->device);
+  FLB_BCUDA(b, cudaStreamSynchronize(b->stream));
+  return btune(b, probe_steps ? probe_steps : 100u, forms);
 }
 
 FLB_API flb_status flb_batch_set_wait_limit(flb_batch b, uint32_t polls) {

@@ -32,7 +32,7 @@ EXPORTS = [
     "flb_total_mass_noalloc", "flb_cell_counts", "flb_check_finite", "flb_run_pass", "flb_profile_steps", "flb_profile_phases", "flb_launch_count", "flb_save_checkpoint",
     "flb_load_checkpoint", "flb_last_error", "flb_status_string", "flb_version",
     "flb_batch_create", "flb_batch_step", "flb_batch_sync", "flb_batch_reset", "flb_batch_read_field",
-    "flb_batch_info", "flb_batch_set_launch", "flb_batch_set_wait_limit", "flb_batch_destroy",
+    "flb_batch_info", "flb_batch_set_launch", "flb_batch_set_wait_limit", "flb_batch_tune", "flb_batch_destroy",
     "flb_batch_last_error",
     "flb_adjoint_desc_init", "flb_adjoint_create", "flb_adjoint_set_porosity", "flb_adjoint_set_force",
     "flb_adjoint_forward", "flb_adjoint_backward", "flb_adjoint_timing", "flb_adjoint_destroy",
@@ -77,7 +77,8 @@ class SetupStruct(C.Structure):
 
 VTI_UINT8, VTI_FLOAT32, VTI_FLOAT64 = 0, 1, 2
 VIZ_UX, VIZ_UY, VIZ_MAGNITUDE, VIZ_PRESSURE = 0, 1, 2, 3
-BATCH_CLUSTER, BATCH_TEAM, BATCH_VECTOR = 0, 1, 4
+BATCH_CLUSTER, BATCH_TEAM, BATCH_VECTOR, BATCH_STREAMS = 0, 1, 4, 8
+TUNE_PERSISTENT, TUNE_STREAMS = 1, 2
 STEP_AUTO, STEP_KERNELS, STEP_PERSISTENT = 0, 1, 2
 
 
@@ -148,6 +149,7 @@ def load_library(path: str = LIB_PATH) -> C.CDLL:
         "flb_batch_info": (C.c_int, [H, C.POINTER(C.c_int64)]),
         "flb_batch_set_launch": (C.c_int, [H, C.c_int, C.c_int, C.c_int, C.c_int]),
         "flb_batch_set_wait_limit": (C.c_int, [H, C.c_uint32]),
+        "flb_batch_tune": (C.c_int, [H, C.c_uint32, C.c_int]),
         "flb_batch_destroy": (C.c_int, [H]),
         "flb_batch_last_error": (C.c_char_p, [H]),
         "flb_adjoint_desc_init": (None, [C.POINTER(AdjointDesc)]),
@@ -550,16 +552,24 @@ class Batch:
     def info(self) -> dict:
         a = (C.c_int64 * 8)()
         self._check(load_library().flb_batch_info(self._h, a))
+        mode = "streams" if a[7] == BATCH_STREAMS else "team" if (a[7] & ~BATCH_VECTOR) == BATCH_TEAM else "cluster"
         return dict(cases=a[0], cells=a[1], t=a[2], group=a[3], groups=a[4], tuned=bool(a[5]), threads=a[6],
-                    mode="team" if (a[7] & ~BATCH_VECTOR) == BATCH_TEAM else "cluster",
-                    vector=bool(a[7] & BATCH_VECTOR))
+                    mode=mode, vector=bool(a[7] & BATCH_VECTOR) and mode != "streams")
 
     def set_launch(self, mode: str, group: int, groups: int, threads: int, vector: bool = False):
         """Launch shape for the following steps: ``mode`` "cluster" or "team",
         CTAs per group, groups, threads per CTA (``info()`` of a tuned batch,
-        for instance), and the vector data path; the state is kept."""
-        m = {"cluster": BATCH_CLUSTER, "team": BATCH_TEAM}[mode] | (BATCH_VECTOR if vector else 0)
+        for instance), and the vector data path; or "streams" with group 1
+        and ``groups`` streams (each case its own handle, the cases' step
+        graphs on concurrent streams; an even step only).  The state is kept."""
+        m = ({"cluster": BATCH_CLUSTER, "team": BATCH_TEAM, "streams": BATCH_STREAMS}[mode]
+             | (BATCH_VECTOR if vector else 0))
         self._check(load_library().flb_batch_set_launch(self._h, m, int(group), int(groups), int(threads)))
+
+    def tune(self, probe_steps: int = 0, forms: int = TUNE_PERSISTENT | TUNE_STREAMS):
+        """Times the launch shapes of the given forms again, keeps the fastest
+        and restarts from the initial state (t = 0)."""
+        self._check(load_library().flb_batch_tune(self._h, int(probe_steps), int(forms)))
 
     def set_wait_limit(self, polls: int):
         """Polls a team-mode CTA waits at its team's barrier before the launch

@@ -7,7 +7,8 @@ The ensemble is ``cases.ensemble()`` (seeded single-phase culvert channels);
 ``--cases`` takes the first n of the 512.  Without ``--shape`` the launch shape
 is chosen by the batch's own timed search (``--autotune`` probe steps); with it
 the search is skipped and the shape "mode,CTAs per group,groups,threads[,vector]"
-is set (``flb_batch_set_launch``).  Prints one JSON line: the shape that ran,
+is set (``flb_batch_set_launch``; "streams,1,S,0" for the streams form on S
+streams).  Prints one JSON line: the shape that ran,
 the wall time of the stepped launch (after a 2-step warm-up) and its rate.
 """
 from __future__ import annotations

@@ -258,11 +258,20 @@ FLB_API flb_status flb_load_checkpoint(flb_handle h, const char* path);
  * cooperative launch; a team barrier gives up after about two seconds, or
  * the limit of flb_batch_set_wait_limit, and flb_batch_sync then returns
  * FLB_ERR_CUDA).
+ * The streams form (FLB_BATCH_STREAMS) is not one persistent launch: every
+ * case becomes an engine handle (the single-case kernels and step graphs,
+ * so the results are those of flb_step by construction), the cases spread
+ * over a pool of streams longest first, and a batch step launches each
+ * case's own step graphs on its stream; the cases run concurrently, which
+ * hides the per-step launch latency that bounds a per-case loop on one
+ * stream.  It keeps a second copy of the state (the handles') and is
+ * entered at even steps only.
  * autotune: 0 uses 8-CTA clusters, one CTA per SM; 1 (100 probe steps) or a
- * probe step count > 1 times candidate modes, group sizes and counts on the
- * batch itself and keeps the fastest, then rebuilds the initial state.  The
+ * probe step count > 1 times candidate modes, group sizes and counts of the
+ * persistent kernel and the streams form with 8 and 16 streams on the batch
+ * itself and keeps the fastest, then rebuilds the initial state.  The
  * device, and the stream if given, come from cases[0]. */
-enum { FLB_BATCH_CLUSTER = 0, FLB_BATCH_TEAM = 1, FLB_BATCH_VECTOR = 4 };
+enum { FLB_BATCH_CLUSTER = 0, FLB_BATCH_TEAM = 1, FLB_BATCH_VECTOR = 4, FLB_BATCH_STREAMS = 8 };
 typedef struct flb_batch_s* flb_batch;
 FLB_API flb_status flb_batch_create(const flb_case_desc* cases, uint32_t n, int autotune, flb_batch* out);
 FLB_API flb_status flb_batch_step(flb_batch b, uint64_t n);
@@ -273,7 +282,8 @@ FLB_API flb_status flb_batch_reset(flb_batch b);
 FLB_API flb_status flb_batch_read_field(flb_batch b, uint32_t i, int field, void* dst, int on_device);
 /* info[0..7] = cases, cells, t, CTAs per group, groups, autotuned, threads
  * per CTA, mode (FLB_BATCH_CLUSTER or FLB_BATCH_TEAM, with FLB_BATCH_VECTOR
- * set when the vector data path runs) */
+ * set when the vector data path runs; FLB_BATCH_STREAMS with group 1,
+ * groups = streams, threads 0) */
 FLB_API flb_status flb_batch_info(flb_batch b, int64_t info[8]);
 /* Sets the launch shape (info[7], [3], [4], [6] of an earlier tuned batch,
  * for instance): mode, with FLB_BATCH_VECTOR or'ed in for the vector data
@@ -283,6 +293,8 @@ FLB_API flb_status flb_batch_info(flb_batch b, int64_t info[8]);
  * 1 <= groups <= the groups of that shape that fit on the device at once, and
  * <= the number of cases; 256, 512 or 1024 threads per CTA (256 or 512 on the
  * vector path).
+ * FLB_BATCH_STREAMS with group 1 and 1..64 streams selects the streams
+ * form (FLB_ERR_UNSUPPORTED at an odd step).
  * The state and t are kept (results do not depend on the shape).
  * FLB_ERR_INVALID_ARGUMENT for a shape out of range, FLB_ERR_UNSUPPORTED for
  * one that cannot launch. */
@@ -295,6 +307,12 @@ FLB_API flb_status flb_batch_set_launch(flb_batch b, int mode, int group, int gr
  * injection for tests, read at every flb_batch_step) one CTA of every team
  * never arrives, so every wait runs out. */
 FLB_API flb_status flb_batch_set_wait_limit(flb_batch b, uint32_t polls);
+/* Times the launch shapes again (probe_steps each, 0: 100) among the forms
+ * given (FLB_TUNE_PERSISTENT: the persistent kernel's shapes;
+ * FLB_TUNE_STREAMS: the streams form), keeps the fastest and rebuilds the
+ * initial state (t = 0), as flb_batch_create with autotune does. */
+enum { FLB_TUNE_PERSISTENT = 1, FLB_TUNE_STREAMS = 2 };
+FLB_API flb_status flb_batch_tune(flb_batch b, uint32_t probe_steps, int forms);
 FLB_API flb_status flb_batch_destroy(flb_batch b);
 FLB_API const char* flb_batch_last_error(flb_batch b);
 

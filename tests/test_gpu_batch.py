@@ -89,6 +89,88 @@ def test_batch_vector_path_matches_single_handles(bb, arith, shape):
     b.close()
 
 
+def _check_cases(b, ens, steps, bb=E.BB_HALFWAY, arith=E.ARITH_FUSED):
+    for i, (flags, tau, gx, gy) in enumerate(ens):
+        s = E.Solver(flags, precision=32, tau=tau, fx=gx, fy=gy, bounce_back=bb, arithmetic=arith)
+        s.step(steps)
+        for name, fid, ref in (("f", E.FIELD_F, s.f), ("rho", E.FIELD_RHO, s.rho), ("u", E.FIELD_U, s.u),
+                               ("flags", E.FIELD_FLAGS, s.flags)):
+            got = b.read(i, fid)
+            assert exact_equal(got, ref), f"case {i} {flags.shape} {name}: {first_mismatch(got, ref)}"
+        s.close()
+
+
+@pytest.mark.parametrize("bb", [E.BB_HALFWAY, E.BB_IMPLICIT], ids=["halfway", "implicit"])
+@pytest.mark.parametrize("arith", [E.ARITH_FUSED, E.ARITH_REFERENCE], ids=["fused", "ref-arith"])
+def test_batch_streams_form_matches_single_handles(bb, arith):
+    """The streams form (each case an engine handle, the cases' step graphs
+    on concurrent streams): every case equals its own handle bit for bit,
+    over launches of both parities, with more cases than streams."""
+    ens = _small_ensemble(13, 1357)
+    b = E.Batch(ens, bounce_back=bb, arithmetic=arith, autotune=0)
+    b.set_launch("streams", 1, 4, 0)
+    info = b.info()
+    assert info["mode"] == "streams" and info["groups"] == 4
+    for n in (2, 37, 27):
+        b.step(n)
+    b.sync()
+    assert b.info()["t"] == 66
+    _check_cases(b, ens, 66, bb, arith)
+    b.close()
+
+
+def test_batch_streams_form_switches_keep_the_state():
+    """The state moves between the persistent kernel's arrays and the
+    streams form's handles: the form is refused at an odd step, entered at
+    an even one, left for a team shape, entered again; a reset in the form
+    restarts every case; every case still equals its own handle."""
+    ens = _small_ensemble(9, 2468)
+    b = E.Batch(ens, autotune=0)
+    b.set_launch("team", 2, 3, 256)
+    b.step(3)
+    with pytest.raises(E.FlowLBError) as ei:  # odd step: refused, the state stays in the batch's arrays
+        b.set_launch("streams", 1, 3, 0)
+    assert ei.value.status == 4
+    b.step(1)
+    b.set_launch("streams", 1, 3, 0)
+    b.step(5)
+    b.set_launch("team", 3, 2, 512)
+    b.step(7)
+    b.set_launch("streams", 1, 5, 0)
+    b.step(4)
+    b.sync()
+    assert b.info()["t"] == 20
+    _check_cases(b, ens, 20)
+    b.reset()
+    assert b.info()["t"] == 0 and b.info()["mode"] == "streams"
+    b.step(6)
+    b.sync()
+    _check_cases(b, ens, 6)
+    b.close()
+
+
+def test_batch_tune_restricted_to_a_form():
+    """flb_batch_tune among the streams form only and among the persistent
+    kernel's shapes only: each keeps a shape of its form and restarts from
+    the initial state."""
+    ens = _small_ensemble(11, 97)
+    b = E.Batch(ens, autotune=0)
+    b.step(3)
+    b.tune(8, E.TUNE_STREAMS)
+    info = b.info()
+    assert info["mode"] == "streams" and info["t"] == 0 and info["tuned"]
+    b.step(10)
+    b.tune(8, E.TUNE_PERSISTENT)
+    info = b.info()
+    assert info["mode"] in ("team", "cluster") and info["t"] == 0
+    b.step(12)
+    b.sync()
+    _check_cases(b, ens, 12)
+    with pytest.raises(E.FlowLBError):
+        b.tune(8, 0)
+    b.close()
+
+
 def test_batch_rejects_unsupported_cases():
     ens = _small_ensemble(2, 1)
     with pytest.raises(E.FlowLBError):
