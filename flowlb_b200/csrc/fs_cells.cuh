@@ -478,6 +478,63 @@ __device__ __forceinline__ void fs234_stages(const KParams& p, FlagMasks<TW>& sm
   __syncthreads();
 }
 
+// The flag bytes of a TW x 8 tile's window (the tile, its kHalo-row halo and
+// one 32-cell word on either side: all that the three stencils reach), one
+// byte per lane and row-word, with the kWarps warps of the block; a window
+// inside the grid is addressed directly, one that crosses an edge wraps
+// (periodic).  Returns whether one of this lane's bytes has a gas,
+// interface or gas-interface bit.
+template <int TW, int kWarps, int kIters>
+__device__ __forceinline__ bool load_window(const KParams& p, int tx, int ty, int tid, uint8_t (&fv)[kIters]) {
+  constexpr int kTX = TW, kW = FlagMasks<TW>::kW, kR = FlagMasks<TW>::kR, kRW = kR * kW;
+  static_assert(kIters * kWarps >= kRW, "window: too few loads");
+  const int nx = (int)p.nx, ny = (int)p.ny;
+  const uint8_t* flags = p.flags;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int xw = tx * kTX - 32 + lane;  // word 0 starts one word left of the tile
+  const int wx0 = tx * kTX - 32, wy0 = ty * kTY - kHalo;
+  const bool inner = wx0 >= 0 && wx0 + 32 * kW <= nx && wy0 >= 0 && wy0 + kR <= ny;
+  const uint8_t* wbase = flags + (inner ? xw + wy0 * nx : 0);
+  bool nq = false;
+#pragma unroll
+  for (int k = 0; k < kIters; k++) {
+    const int rw = warp + k * kWarps;
+    const int r = rw / kW, c = rw % kW;
+    fv[k] = rw >= kRW ? 0
+            : inner   ? wbase[r * nx + 32 * c]
+                      : flags[wrapi(xw + 32 * c, nx) + wrapi(wy0 + r, ny) * nx];
+  }
+#pragma unroll
+  for (int k = 0; k < kIters; k++) nq |= (fv[k] & (kGas | kInterface | kGasInterface)) != 0;
+  return nq;
+}
+
+// A quiet tile: no gas, interface or gas-interface cell in its window.  There
+// FS_2 and FS_3 change no flag and FS_4 converts none, so of the masks only
+// FS_4's neighbour count is needed: fluid cells that are not solid or inlet
+// (conservative mode; all fluid cells in the reference mode), exactly what
+// the general stages give when no IF, IG or GI cell is near.  Writes that
+// mask (rows 2 .. kR-3) from the window bytes; the caller's next block
+// barrier publishes it.
+template <int TW, int kWarps, int kIters>
+__device__ __forceinline__ void quiet_count_mask(const KParams& p, FlagMasks<TW>& sm, const uint8_t (&fv)[kIters],
+                                                 int tid) {
+  constexpr int kW = FlagMasks<TW>::kW, kR = FlagMasks<TW>::kR, kRW = kR * kW;
+  const int lane = tid & 31, warp = tid >> 5;
+  const bool cons = p.fs_cons != 0;
+#pragma unroll
+  for (int k = 0; k < kIters; k++) {
+    const int rw = warp + k * kWarps;  // the same for the whole warp
+    if (rw >= kRW) break;
+    const int r = rw / kW, c = rw % kW;
+    if (r < 2 || r > kR - 3) continue;
+    const uint8_t f = fv[k];
+    const bool counted = (f & kFluid) && !(cons && (f & (kWall | kMovingWall | kInlet)));
+    const uint32_t b = __ballot_sync(0xffffffffu, counted);
+    if (lane == 0) sm.cnt[r][c] = b;
+  }
+}
+
 // One TW x 8 tile (tile coordinates tx, ty) with the TW*8/CPT threads of the
 // block, CPT cells per thread (rows ly and ly + 8/CPT, ...); every thread of
 // the block must call it.  Returns the activity bits (activity, above) of
@@ -490,7 +547,6 @@ __device__ __forceinline__ uint32_t fs234_tile(const KParams& p, int tx, int ty,
   constexpr int kThreads = TW * kTY / CPT, kWarps = kThreads / 32, kRowStep = kTY / CPT;
   static_assert(kTY % CPT == 0 && kThreads >= (kR - 2) * kW, "flag pass: block too small for the stencil stages");
   const int nx = (int)p.nx, ny = (int)p.ny;
-  const uint8_t* flags = p.flags;
   // this thread's cells: their own values are loaded now, so that their
   // latency overlaps the mask building and the stencil stages
   const int lx = tid % kTX, ly0 = tid / kTX;
@@ -504,47 +560,12 @@ __device__ __forceinline__ uint32_t fs234_tile(const KParams& p, int tx, int ty,
   }
   // masks of the flags after stream-collide: every flag byte a lane needs is
   // loaded first, so the loads of all its row-words are in flight together
-  const int lane = tid & 31, warp = tid >> 5;
-  const int xw = tx * kTX - 32 + lane;  // word 0 starts one word left of the tile
   constexpr int kRW = kR * kW, kIters = (kRW + kWarps - 1) / kWarps;
-  // a window inside the grid is addressed directly; one that crosses an
-  // edge wraps (periodic)
-  const int wx0 = tx * kTX - 32, wy0 = ty * kTY - kHalo;
-  const bool inner = wx0 >= 0 && wx0 + 32 * kW <= nx && wy0 >= 0 && wy0 + kR <= ny;
-  const uint8_t* wbase = flags + (inner ? xw + wy0 * nx : 0);
   uint8_t fv[kIters];
-#pragma unroll
-  for (int k = 0; k < kIters; k++) {
-    const int rw = warp + k * kWarps;
-    const int r = rw / kW, c = rw % kW;
-    fv[k] = rw >= kRW ? 0
-            : inner   ? wbase[r * nx + 32 * c]
-                      : flags[wrapi(xw + 32 * c, nx) + wrapi(wy0 + r, ny) * nx];
-  }
-  // A quiet tile: no gas, interface or gas-interface cell in the loaded
-  // window (the tile, its 3-row halo and a word on either side: all that the
-  // three stencils reach).  There FS_2 and FS_3 change no flag and FS_4
-  // converts none, so of the masks only FS_4's neighbour count is needed:
-  // fluid cells that are not solid or inlet (conservative mode; all fluid
-  // cells in the reference mode), exactly what the general stages give when
-  // no IF, IG or GI cell is near.
-  bool nq = false;
-#pragma unroll
-  for (int k = 0; k < kIters; k++) nq |= (fv[k] & (kGas | kInterface | kGasInterface)) != 0;
+  const bool nq = load_window<TW, kWarps, kIters>(p, tx, ty, tid, fv);
   const bool quiet = __syncthreads_or(nq) == 0;
   if (quiet) {
-    const bool cons = p.fs_cons != 0;
-#pragma unroll
-    for (int k = 0; k < kIters; k++) {
-      const int rw = warp + k * kWarps;  // the same for the whole warp
-      if (rw >= kRW) break;
-      const int r = rw / kW, c = rw % kW;
-      if (r < 2 || r > kR - 3) continue;
-      const uint8_t f = fv[k];
-      const bool counted = (f & kFluid) && !(cons && (f & (kWall | kMovingWall | kInlet)));
-      const uint32_t b = __ballot_sync(0xffffffffu, counted);
-      if (lane == 0) sm.cnt[r][c] = b;
-    }
+    quiet_count_mask<TW, kWarps, kIters>(p, sm, fv, tid);
     __syncthreads();
   } else {
     fs234_stages<TW, kWarps, kIters>(p, sm, fv, tid);
@@ -560,8 +581,6 @@ __device__ __forceinline__ uint32_t fs234_tile(const KParams& p, int tx, int ty,
   }
   return act;
 }
-
-
 
 // Appends super-tile t to the next step's lists (NextLists), with warp 0 of
 // the block (every lane calls it): t itself when it holds fluid or interface
@@ -586,18 +605,18 @@ __device__ __forceinline__ void append_next(const NextLists& nl, uint32_t t, uin
     const uint32_t yy = dy > 0 ? (sy + 1u == nl.nsy ? 0u : sy + 1u) : dy < 0 ? (sy == 0u ? nl.nsy - 1u : sy - 1u) : sy;
     cand = xx + yy * nl.nsx;
   }
+  // the stream-collide slot is taken beside the marks (independent atomics,
+  // so their round trips overlap)
+  const bool add_sc = lane == 0 && (m & 1u);
+  uint32_t base_fs = 0, base_sc = 0;
+  if (add_sc) base_sc = atomicAdd(nl.counts, 1u);
   bool add_fs = false;
   if (cand != kNone) {
     const uint32_t bit = 1u << (cand & 31u);
     add_fs = (atomicOr(nl.bits + (cand >> 5), bit) & bit) == 0u;
   }
   const uint32_t bfs = __ballot_sync(0xffffffffu, add_fs);
-  const bool add_sc = lane == 0 && (m & 1u);
-  uint32_t base_fs = 0, base_sc = 0;
-  if (lane == 0) {
-    if (bfs) base_fs = atomicAdd(nl.counts + 1, (uint32_t)__popc(bfs));
-    if (add_sc) base_sc = atomicAdd(nl.counts, 1u);
-  }
+  if (lane == 0 && bfs) base_fs = atomicAdd(nl.counts + 1, (uint32_t)__popc(bfs));
   base_fs = __shfl_sync(0xffffffffu, base_fs, 0);
   if (add_fs) {
     const uint32_t k = base_fs + __popc(bfs & ((1u << lane) - 1u));
@@ -619,6 +638,9 @@ __device__ __forceinline__ void fs234_super_tile(const KParams& p, uint32_t t, u
   const int sx = (int)(t % nsx), sy = (int)(t / nsx);
   const int wact = min((int)kSTW, (int)p.nx - sx * (int)kSTW), hact = min((int)kSTH, (int)p.ny - sy * (int)kSTH);
   uint32_t act = 0;
+  // the word of the last step, read now so that its latency overlaps the
+  // tile (only this block writes nz[t] during the pass, at the end)
+  const uint32_t word = tid < 32 ? __ldcg(nz + t) : 0u;
   // (no barrier between tiles: a tile's first write to sm comes after its
   // __syncthreads_or, which no thread passes before every thread has
   // finished reading the previous tile's masks)
@@ -633,9 +655,8 @@ __device__ __forceinline__ void fs234_super_tile(const KParams& p, uint32_t t, u
   if (tid < 32) {
     uint32_t m = 0;
     for (int w = 0; w < kWarps; w++) m |= wact_sm[w];
-    const uint32_t old = __shfl_sync(0xffffffffu, tid == 0 ? __ldcg(nz + t) : 0u, 0);
     if (tid == 0) nz[t] = m;
-    append_next(nl, t, m, old, (uint32_t)tid);
+    append_next(nl, t, m, word, (uint32_t)tid);
   }
 }
 

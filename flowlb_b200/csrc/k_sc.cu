@@ -241,7 +241,7 @@ __device__ __forceinline__ void sc_vec_cells(const KParams& p, uint32_t x0, uint
         if ((nbm >> (i - 1)) & 1u) f[i + 1] = K::ld(slotp<S>(p, slot_a<ODD>(i)), nb[i], i + 1, p.f16_inv);
       }
     }
-    collide_cell<C, M, FS, WM, FU, DEV>(p, idx, x, y, fl[k], nbm, f, DEV ? p.tstep[ODD] : 0u);
+    collide_cell<C, M, FS, WM, FU, DEV, S>(p, idx, x, y, fl[k], nbm, f, DEV ? p.tstep[ODD] : 0u);
     K::st(raw0, k, 0, f[0], p.f16_scale);
 #pragma unroll
     for (int q = 0; q < 4; q++) {

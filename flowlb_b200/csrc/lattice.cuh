@@ -62,6 +62,20 @@ struct Codec<__half, float> {
   }
 };
 
+// The value population v of direction dir reads back as once it has been
+// stored in the population array (S) and loaded again: v itself unless the
+// storage is narrower than the arithmetic (FP16S).
+template <class S, class C>
+__device__ __forceinline__ C stored_value(C v, int, float, float) {
+  return v;
+}
+template <>
+__device__ __forceinline__ float stored_value<__half, float>(float v, int dir, float scale, float inv_scale) {
+  __half h;
+  Codec<__half, float>::st(&h, 0, dir, v, scale);
+  return Codec<__half, float>::ld(&h, 0, dir, inv_scale);
+}
+
 // Raw FP16S access: the stored scaled deviation h = (f - w) * scale as a
 // float, for arithmetic done in deviation units (collide_fused_dev).
 // Stores round toward zero: the values arrive already rounded to binary16

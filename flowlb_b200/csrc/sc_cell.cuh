@@ -16,8 +16,10 @@ namespace flb {
 // FU: the fused SRT arithmetic (collide_fused) for cells that are neither inlet
 // nor outlet; the host selects it only for SRT without the subgrid model.
 // DEV: f holds FP16S deviations h = (f - w) * scale (single phase with FU).
-// tnow: the time step (DEV only, for the stochastic rounding).
-template <class C, class M, bool FS, bool WM, bool FU, bool DEV = false>
+// tnow: the time step (DEV only, for the stochastic rounding).  S: the
+// storage type of the populations (a parked population is used as the
+// value it would read back as from the population array).
+template <class C, class M, bool FS, bool WM, bool FU, bool DEV = false, class S = C>
 __device__ __forceinline__ void collide_cell(const KParams& p, uint32_t idx, uint32_t x, uint32_t y, uint8_t flag,
                                              uint32_t nbm, C* f, uint32_t tnow = 0u) {
   const uint32_t N = p.N;
@@ -47,6 +49,8 @@ __device__ __forceinline__ void collide_cell(const KParams& p, uint32_t idx, uin
     // reference mode: FS_1 left the populations it rebuilt toward gas here.
     // FS_1 wrote them to their regular slots; where a half-way wall reflects
     // the population instead (its source is a wall), that slot is not read.
+    // Each is taken at the value its slot would hold (rounded to the
+    // storage), as if FS_1 had stored it and this step had loaded it.
     if (!p.fs_cons && (flag & (kFGI | kInlet)) == kInterface) {
       uint32_t wallsrc = 0;  // bit k: the source of incoming population k+1 is a wall
 #pragma unroll
@@ -59,7 +63,7 @@ __device__ __forceinline__ void collide_cell(const KParams& p, uint32_t idx, uin
         const C* rec = static_cast<const C*>(p.recon);
 #pragma unroll
         for (int k = 0; k < 8; k++)
-          if ((m >> k) & 1u) f[k + 1] = rec[(uint32_t)k * N + idx];
+          if ((m >> k) & 1u) f[k + 1] = stored_value<S, C>(rec[(uint32_t)k * N + idx], k + 1, p.f16_scale, p.f16_inv);
       }
     }
   }
@@ -215,7 +219,7 @@ __device__ __forceinline__ void sc_cell(const KParams& p, uint32_t x, uint32_t y
     if (flag & (kGas | kWall)) return;
     load_in<S, C, HW, ODD, K>(p, idx, nb, nbm, f);
   }
-  collide_cell<C, M, FS, WM, FU, DEV>(p, idx, x, y, flag, nbm, f, DEV ? p.tstep[ODD] : 0u);
+  collide_cell<C, M, FS, WM, FU, DEV, S>(p, idx, x, y, flag, nbm, f, DEV ? p.tstep[ODD] : 0u);
   store_post<S, C, ODD, K>(p, idx, nb, f);
 }
 

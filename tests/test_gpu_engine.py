@@ -94,6 +94,7 @@ def test_f16s_row_chunks_match_oracle(nx, ny, bb):
     (O.F32, O.BB_HALFWAY, O.FS_CONSERVATIVE),
     (O.F64, O.BB_HALFWAY, O.FS_CONSERVATIVE),
     (O.F16S, O.BB_HALFWAY, O.FS_CONSERVATIVE),
+    (O.F16S, O.BB_IMPLICIT, O.FS_REFERENCE),
     (O.F32, O.BB_IMPLICIT, O.FS_CONSERVATIVE),
     (O.F32, O.BB_HALFWAY, O.FS_REFERENCE),
 ], ids=lambda v: str(v))
@@ -320,6 +321,23 @@ def test_reference_mode_quiet_tiles_match_oracle(monkeypatch, form):
         s.step(n)
         o.step(n)
         assert_same_state(s, o, O.F32_M32, True, f"form {form} t={o.t}")
+    s.close()
+
+
+@ARITHS
+def test_f16s_reference_mode_parked_populations_match_oracle(arith):
+    """FP16 storage in the reference's free-surface mode (implicit walls):
+    the populations FS_1 rebuilds toward gas are parked and handed to
+    stream-collide, which must use them at the value their FP16 slot would
+    hold (the oracle stores them into the population array and loads them
+    back), on a dam break large enough that many interface cells rebuild."""
+    c = cases.small_dam_break(1280, 320)
+    s, o = make_pair(c.flags, O.F16S, free_surface=True, bb=O.BB_IMPLICIT, fs_mode=O.FS_REFERENCE, tau=0.55,
+                     fy=-2e-4, u_max=0.25, arith=arith)
+    for n in (1, 2, 61, 64):
+        s.step(n)
+        o.step(n)
+        assert_same_state(s, o, O.F16S, True, f"t={o.t}")
     s.close()
 
 
