@@ -261,6 +261,21 @@ __device__ __forceinline__ void load_in(const KParams& p, uint32_t idx, const ui
   }
 }
 
+// The half-way wall part of load_in alone: f holds what load_in reads when
+// no neighbour is a wall, and the populations that arrive from a wall
+// neighbour (nbm) are replaced by their reflections.
+template <class S, class C, bool ODD, class K = Codec<S, C>>
+__device__ __forceinline__ void reload_reflected(const KParams& p, uint32_t idx, const uint32_t* nb, uint32_t nbm,
+                                                 C* f) {
+  const float inv = p.f16_inv;
+#pragma unroll
+  for (int i = 1; i < 9; i += 2) {
+    const int a = slot_a<ODD>(i), b = slot_b<ODD>(i);
+    if ((nbm >> i) & 1u) f[i] = K::ld(slotp<S>(p, b), idx, i, inv);
+    if ((nbm >> (i - 1)) & 1u) f[i + 1] = K::ld(slotp<S>(p, a), nb[i], i + 1, inv);
+  }
+}
+
 // loadOutgoingf, cellCalculations.cuh:207-217.
 template <class S, class C, bool ODD>
 __device__ __forceinline__ void load_out(const KParams& p, uint32_t idx, const uint32_t* nb, C* out) {

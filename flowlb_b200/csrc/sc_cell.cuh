@@ -213,11 +213,14 @@ __device__ __forceinline__ void sc_cell(const KParams& p, uint32_t x, uint32_t y
     load_in<S, C, HW, ODD, K>(p, idx, nb, nbm, f);
     if (flag & (kGas | kWall)) return;
   } else {
-    // the wall mask is loaded with the flag (one round trip, not two)
+    // the wall mask and the populations are loaded with the flag (one round
+    // trip, not two): the populations as if no neighbour were a wall, and a
+    // cell next to a wall then reloads the ones a wall reflects
     flag = p.flags[idx];
     if (HW) nbm = p.nbmask[idx];
+    load_in<S, C, false, ODD, K>(p, idx, nb, 0u, f);
     if (flag & (kGas | kWall)) return;
-    load_in<S, C, HW, ODD, K>(p, idx, nb, nbm, f);
+    if (HW && nbm) reload_reflected<S, C, ODD, K>(p, idx, nb, nbm, f);
   }
   collide_cell<C, M, FS, WM, FU, DEV, S>(p, idx, x, y, flag, nbm, f, DEV ? p.tstep[ODD] : 0u);
   store_post<S, C, ODD, K>(p, idx, nb, f);
