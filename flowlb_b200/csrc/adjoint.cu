@@ -39,6 +39,11 @@ namespace flb {
 namespace {
 
 constexpr int kAdjBlock = 256;
+// resident blocks per SM the reverse step is compiled for: four (at most 64
+// registers a thread; the FP64 step spills 44 bytes) measured faster than the
+// 92-register build's two on a B200 (FP64 backward of the 1024x256 case 68.1
+// -> 62.7 ms; three blocks, 80 registers: 67.4 ms)
+constexpr int kAdjBwdBlocks = 4;
 // opposite direction (directions of lattice.cuh: i and i+1 opposite for odd i)
 __host__ __device__ constexpr int opp(int i) { return i == 0 ? 0 : ((i & 1) ? i + 1 : i - 1); }
 
@@ -186,7 +191,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_por_fwd(const AdjParams<T> p, con
 // t) (scattered).  sbar: dJ/ds per cell; gpart: dJ/dg per block (2 doubles per
 // block).  The update's derivative needs no population itself, only rho and v.
 template <class T>
-__global__ void __launch_bounds__(kAdjBlock) k_por_bwd(const AdjParams<T> p, const T* __restrict__ mac,
+__global__ void __launch_bounds__(kAdjBlock, kAdjBwdBlocks) k_por_bwd(const AdjParams<T> p, const T* __restrict__ mac,
                                                        const T* __restrict__ lam_next, T* __restrict__ lam,
                                                        double* __restrict__ sbar, double* __restrict__ gpart,
                                                        const SegDesc* __restrict__ seg, uint32_t j) {

@@ -17,22 +17,30 @@ __device__ __forceinline__ void fs1_cell(const KParams& p, uint32_t x, uint32_t 
   const uint32_t nx = p.nx, N = p.N;
   const uint32_t idx = x + y * nx;
   const uint8_t* flags = p.flags;
-  if (flag & (kGas | kWall | kInlet)) return;
-  const bool cons = p.fs_cons != 0;
-  const uint8_t e = flag & kFGI;
-  if (cons && (!(e == kFluid || e == kInterface) || (flag & kMovingWall))) return;
+  // the populations, the mass and the neighbours' excess are loaded before
+  // the flag is tested (a caller that has just loaded the flag then waits
+  // one round trip, not two), the populations as if no neighbour were a
+  // wall; a cell next to a wall reloads the ones a wall reflects
   uint32_t nb[9];
   neighbours(x, y, nx, p.ny, nb);
   C in[9], out[9];
-  load_in<S, C, HW, ODD>(p, idx, nb, nbm, in);
-  out[0] = in[0];
+  load_in<S, C, false, ODD>(p, idx, nb, 0u, in);
   load_out<S, C, ODD>(p, idx, nb, out);
   M* Ms = static_cast<M*>(p.mass);
   const M* Ex = static_cast<const M*>(p.excess);
   const M* Ph = static_cast<const M*>(p.phi);
   M m = Ms[idx];
+  M exn[9];
 #pragma unroll
-  for (int i = 1; i < 9; i++) m += Ex[nb[i]];
+  for (int i = 1; i < 9; i++) exn[i] = Ex[nb[i]];
+  if (flag & (kGas | kWall | kInlet)) return;
+  const bool cons = p.fs_cons != 0;
+  const uint8_t e = flag & kFGI;
+  if (cons && (!(e == kFluid || e == kInterface) || (flag & kMovingWall))) return;
+  if (HW && nbm) reload_reflected<S, C, ODD>(p, idx, nb, nbm, in);
+  out[0] = in[0];
+#pragma unroll
+  for (int i = 1; i < 9; i++) m += exn[i];
   if (e == kFluid) {
     if (!cons) {
 #pragma unroll
