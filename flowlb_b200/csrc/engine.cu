@@ -647,14 +647,17 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
     h->use_vec_list = desc->kernel_variant == 2 ||
                       (desc->kernel_variant == 0 && desc->nx % V == 0 && desc->precision == 16 && fused &&
                        tiles > 4096u);
-    // flag pass: 128-wide tiles with one cell per thread (1024-thread
-    // blocks) on grids of up to 4096 super-tiles, two cells per thread
-    // (512-thread blocks, two per SM) above.  Measured on a B200: 2048x512
-    // dam break 29.2 us per step (two cells per thread 30.1, four 34.6);
-    // 8192x2048 flag pass 110 us per step (three 512-thread blocks per SM
-    // 114, four 119; one cell per thread 124, four 131, 32-wide tiles 158).  FLB_FS_FLAG_FORM (32, 128x1, 128x2 or 128x4: tile width x cells
+    // flag pass: 128-wide tiles with two cells per thread (512-thread
+    // blocks, two per SM).  Measured on a B200 (quiet tiles counting their
+    // neighbours from the flags): 2048x512 dam break 25.9 us per step against
+    // 28.0 with one cell per thread (1024-thread blocks); 8192x2048 227.2
+    // against 242.0.  Earlier builds (before the quiet-tile path): 2048x512
+    // one cell per thread 29.2, two 30.1, four 34.6; 8192x2048 flag pass 110
+    // us per step with two cells per thread at two blocks per SM (114 at
+    // three, 119 at four), one cell per thread 124, four 131, 32-wide tiles
+    // 158.  FLB_FS_FLAG_FORM (32, 128x1, 128x2 or 128x4: tile width x cells
     // per thread) selects another form, with the same results.
-    h->fs_form = tiles <= 4096u ? FS_FORM_W128X1 : FS_FORM_W128X2;
+    h->fs_form = FS_FORM_W128X2;
     if (const char* v = std::getenv("FLB_FS_FLAG_FORM")) {
       if (!std::strcmp(v, "32")) h->fs_form = FS_FORM_W32;
       else if (!std::strcmp(v, "128x1")) h->fs_form = FS_FORM_W128X1;

@@ -402,8 +402,24 @@ __device__ __forceinline__ bool fs234_cell(const KParams& p, const FlagMasks<TW>
       break;
   }
   // FS_4's count of fluid / interface neighbours after the conversion
-  const int cont = __popc(window3<TW>(sm.cnt, r - 1, c, i)) + __popc(window3<TW>(sm.cnt, r, c, i) & 5u) +
-                   __popc(window3<TW>(sm.cnt, r + 1, c, i));
+  int cont = 0;
+  if constexpr (Q) {
+    // a quiet tile converts no cell: the count comes straight from the
+    // neighbours' flags (which the window's loads left in L1): fluid cells
+    // that are not solid or inlet (conservative mode), all fluid cells in the
+    // reference mode
+    uint32_t nb[9];
+    neighbours((uint32_t)gx, (uint32_t)gy, (uint32_t)nx, (uint32_t)ny, nb);
+    const bool cons = p.fs_cons != 0;
+#pragma unroll
+    for (int k = 1; k < 9; k++) {
+      const uint8_t f = p.flags[nb[k]];
+      cont += ((f & kFluid) && !(cons && (f & (kWall | kMovingWall | kInlet)))) ? 1 : 0;
+    }
+  } else {
+    cont = __popc(window3<TW>(sm.cnt, r - 1, c, i)) + __popc(window3<TW>(sm.cnt, r, c, i) & 5u) +
+           __popc(window3<TW>(sm.cnt, r + 1, c, i));
+  }
   m += cont > 0 ? 0.0f : ex;
   ex = cont > 0 ? div_count(ex, cont) : M(0);
   if (gas_stays) {
@@ -517,32 +533,6 @@ __device__ __forceinline__ bool load_window(const KParams& p, int tx, int ty, in
   return nq;
 }
 
-// A quiet tile: no gas, interface or gas-interface cell in its window.  There
-// FS_2 and FS_3 change no flag and FS_4 converts none, so of the masks only
-// FS_4's neighbour count is needed: fluid cells that are not solid or inlet
-// (conservative mode; all fluid cells in the reference mode), exactly what
-// the general stages give when no IF, IG or GI cell is near.  Writes that
-// mask (rows 2 .. kR-3) from the window bytes; the caller's next block
-// barrier publishes it.
-template <int TW, int kWarps, int kIters>
-__device__ __forceinline__ void quiet_count_mask(const KParams& p, FlagMasks<TW>& sm, const uint8_t (&fv)[kIters],
-                                                 int tid) {
-  constexpr int kW = FlagMasks<TW>::kW, kR = FlagMasks<TW>::kR, kRW = kR * kW;
-  const int lane = tid & 31, warp = tid >> 5;
-  const bool cons = p.fs_cons != 0;
-#pragma unroll
-  for (int k = 0; k < kIters; k++) {
-    const int rw = warp + k * kWarps;  // the same for the whole warp
-    if (rw >= kRW) break;
-    const int r = rw / kW, c = rw % kW;
-    if (r < 2 || r > kR - 3) continue;
-    const uint8_t f = fv[k];
-    const bool counted = (f & kFluid) && !(cons && (f & (kWall | kMovingWall | kInlet)));
-    const uint32_t b = __ballot_sync(0xffffffffu, counted);
-    if (lane == 0) sm.cnt[r][c] = b;
-  }
-}
-
 // One TW x 8 tile (tile coordinates tx, ty) with the TW*8/CPT threads of the
 // block, CPT cells per thread (rows ly and ly + 8/CPT, ...); every thread of
 // the block must call it.  Returns the activity bits (activity, above) of
@@ -571,13 +561,11 @@ __device__ __forceinline__ uint32_t fs234_tile(const KParams& p, int tx, int ty,
   constexpr int kRW = kR * kW, kIters = (kRW + kWarps - 1) / kWarps;
   uint8_t fv[kIters];
   const bool nq = load_window<TW, kWarps, kIters>(p, tx, ty, tid, fv);
+  // a quiet tile (no gas, interface or gas-interface cell in the window)
+  // needs none of the masks: FS_2 and FS_3 change no flag there and FS_4
+  // converts none, and each cell counts its neighbours itself
   const bool quiet = __syncthreads_or(nq) == 0;
-  if (quiet) {
-    quiet_count_mask<TW, kWarps, kIters>(p, sm, fv, tid);
-    __syncthreads();
-  } else {
-    fs234_stages<TW, kWarps, kIters>(p, sm, fv, tid);
-  }
+  if (!quiet) fs234_stages<TW, kWarps, kIters>(p, sm, fv, tid);
   uint32_t act = 0;
 #pragma unroll
   for (int k = 0; k < CPT; k++) {
