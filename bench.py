@@ -51,12 +51,12 @@ KERNEL_OF_PASS = {"stream_collide": "k_sc_list (free-surface stream-collide)", "
 # each pass's share of the step's device time in the ncu launch list of this
 # workload (gpu__time_duration.sum of ~1000 launches of each of the three
 # kernels of a step; profiles/dam_break_2048x512_launch_list.md)
-PASS_SHARE_NCU: dict = {"fs234": 0.447, "fs1": 0.308, "stream_collide": 0.245}
+PASS_SHARE_NCU: dict = {"fs234": 0.463, "fs1": 0.284, "stream_collide": 0.252}
 # dram__bytes_read.sum + dram__bytes_write.sum per launch (mean of the two
 # parities) from one ncu capture of the workload at steps 300-303
 # (profiles/dam_break_2048x512_launch_list.md); ncu flushes the caches before
 # each launch, so these are cold-start figures for an L2-resident working set
-TRAFFIC_NCU: dict = {"fs234": 7353600, "stream_collide": 9787776, "fs1": 13919616}
+TRAFFIC_NCU: dict = {"fs234": 5356800, "stream_collide": 9796224, "fs1": 13932288}
 # the persistent step: one launch runs PERSIST_STEPS lattice steps of every pass
 KERNEL_PERSIST = "k_fs_persist (FS_1, stream-collide, FS_2..4 and list build, grid barriers)"
 PERSIST_STEPS = 32
