@@ -648,21 +648,27 @@ FLB_API flb_status flb_create(const flb_case_desc* desc, flb_handle* out) {
                       (desc->kernel_variant == 0 && desc->nx % V == 0 && desc->precision == 16 && fused &&
                        tiles > 4096u);
     // flag pass: 128-wide tiles with two cells per thread (512-thread
-    // blocks, two per SM).  Measured on a B200 (quiet tiles counting their
-    // neighbours from the flags): 2048x512 dam break 25.9 us per step against
-    // 28.0 with one cell per thread (1024-thread blocks); 8192x2048 227.2
-    // against 242.0.  Earlier builds (before the quiet-tile path): 2048x512
-    // one cell per thread 29.2, two 30.1, four 34.6; 8192x2048 flag pass 110
-    // us per step with two cells per thread at two blocks per SM (114 at
-    // three, 119 at four), one cell per thread 124, four 131, 32-wide tiles
-    // 158.  FLB_FS_FLAG_FORM (32, 128x1, 128x2 or 128x4: tile width x cells
-    // per thread) selects another form, with the same results.
-    h->fs_form = FS_FORM_W128X2;
+    // blocks, two per SM) on grids of up to 4096 super-tiles, 64-wide tiles
+    // with two cells per thread (256-thread blocks, five per SM at 48
+    // registers) above.  Measured on a B200 (quiet tiles counting their
+    // neighbours from the flags): 2048x512 dam break 25.9 us per step with
+    // 128x2 against 28.0 with 128x1, 28.0 with 64x1, 33.4 with 64x2 and 33.5
+    // with 128x4; 8192x2048 224.5 with 64x2 against 226.9 with 128x2, 232.1
+    // with 64x1 and 242.0 with 128x1.  Earlier builds (before the quiet-tile
+    // path): 2048x512 one cell per thread 29.2, two 30.1, four 34.6;
+    // 8192x2048 flag pass 110 us per step with two cells per thread at two
+    // blocks per SM (114 at three, 119 at four), one cell per thread 124,
+    // four 131, 32-wide tiles 158.  FLB_FS_FLAG_FORM (32, 64x1, 64x2, 128x1,
+    // 128x2 or 128x4: tile width x cells per thread) selects another form,
+    // with the same results.
+    h->fs_form = tiles <= 4096u ? FS_FORM_W128X2 : FS_FORM_W64X2;
     if (const char* v = std::getenv("FLB_FS_FLAG_FORM")) {
       if (!std::strcmp(v, "32")) h->fs_form = FS_FORM_W32;
       else if (!std::strcmp(v, "128x1")) h->fs_form = FS_FORM_W128X1;
       else if (!std::strcmp(v, "128x2")) h->fs_form = FS_FORM_W128X2;
       else if (!std::strcmp(v, "128x4")) h->fs_form = FS_FORM_W128X4;
+      else if (!std::strcmp(v, "64x1")) h->fs_form = FS_FORM_W64X1;
+      else if (!std::strcmp(v, "64x2")) h->fs_form = FS_FORM_W64X2;
     }
   }
   s = check_io(h, desc->flags);

@@ -149,6 +149,12 @@ constexpr uint32_t kWideTiles = FLB_FS_PDL_TILES;
 #ifndef FLB_FS_HALF_MIN_BLOCKS
 #define FLB_FS_HALF_MIN_BLOCKS 2
 #endif
+#ifndef FLB_FS_W64_MIN_BLOCKS
+#define FLB_FS_W64_MIN_BLOCKS 3
+#endif
+#ifndef FLB_FS_W64X2_MIN_BLOCKS
+#define FLB_FS_W64X2_MIN_BLOCKS 5
+#endif
 #ifndef FLB_FS_QUARTER_MIN_BLOCKS
 #define FLB_FS_QUARTER_MIN_BLOCKS 4
 #endif

@@ -92,8 +92,9 @@ __global__ void k_apply_recon(const __grid_constant__ KParams p, uint32_t odd) {
 // TW x 8 tiles, CPT cells per thread.
 template <int TW, int CPT>
 constexpr int fs234_min_blocks() {
-  return TW == 128 ? (CPT == 1 ? FLB_FS_WIDE_MIN_BLOCKS : CPT == 2 ? FLB_FS_HALF_MIN_BLOCKS : FLB_FS_QUARTER_MIN_BLOCKS)
-                   : 6;
+  return TW == 128  ? (CPT == 1 ? FLB_FS_WIDE_MIN_BLOCKS : CPT == 2 ? FLB_FS_HALF_MIN_BLOCKS : FLB_FS_QUARTER_MIN_BLOCKS)
+         : TW == 64 ? (CPT == 1 ? FLB_FS_W64_MIN_BLOCKS : FLB_FS_W64X2_MIN_BLOCKS)
+                    : 6;
 }
 template <class S, class C, class M, bool ODD, int TW, int CPT>
 __global__ void __launch_bounds__(TW* kTY / CPT, fs234_min_blocks<TW, CPT>())
@@ -153,6 +154,8 @@ int launch_fs234(const KParams& kp, cudaStream_t st, uint32_t odd, const TileLis
     case FS_FORM_W32: launch_fs234_form<S, C, M, 32, 1>(kp, st, odd, tl, grid, nz, nl); break;
     case FS_FORM_W128X2: launch_fs234_form<S, C, M, 128, 2>(kp, st, odd, tl, grid, nz, nl); break;
     case FS_FORM_W128X4: launch_fs234_form<S, C, M, 128, 4>(kp, st, odd, tl, grid, nz, nl); break;
+    case FS_FORM_W64X1: launch_fs234_form<S, C, M, 64, 1>(kp, st, odd, tl, grid, nz, nl); break;
+    case FS_FORM_W64X2: launch_fs234_form<S, C, M, 64, 2>(kp, st, odd, tl, grid, nz, nl); break;
     default: launch_fs234_form<S, C, M, 128, 1>(kp, st, odd, tl, grid, nz, nl); break;
   }
   return 1;
@@ -173,6 +176,8 @@ int fs_blocks_per_sm(int which, int form) {
   else if (form == FS_FORM_W32) n = fs234_blocks_per_sm<S, C, M, 32, 1>();
   else if (form == FS_FORM_W128X2) n = fs234_blocks_per_sm<S, C, M, 128, 2>();
   else if (form == FS_FORM_W128X4) n = fs234_blocks_per_sm<S, C, M, 128, 4>();
+  else if (form == FS_FORM_W64X1) n = fs234_blocks_per_sm<S, C, M, 64, 1>();
+  else if (form == FS_FORM_W64X2) n = fs234_blocks_per_sm<S, C, M, 64, 2>();
   else n = fs234_blocks_per_sm<S, C, M, 128, 1>();
   return n > 0 ? n : 1;
 }

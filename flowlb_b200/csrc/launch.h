@@ -50,7 +50,8 @@ int launch_fs234(const KParams& kp, cudaStream_t st, uint32_t odd, const TileLis
                  const NextLists& nl, int form);
 // launch forms of the flag pass: tile width x cells per thread (threads per
 // block = width * 8 / cells per thread)
-enum FsForm { FS_FORM_W128X1 = 0, FS_FORM_W32 = 1, FS_FORM_W128X2 = 2, FS_FORM_W128X4 = 4 };
+enum FsForm { FS_FORM_W128X1 = 0, FS_FORM_W32 = 1, FS_FORM_W128X2 = 2, FS_FORM_W128X4 = 4, FS_FORM_W64X1 = 5,
+              FS_FORM_W64X2 = 6 };
 // resident blocks per SM of FS_1 (which 0) or of the flag pass in `form` (which 1)
 template <class S, class C, class M>
 int fs_blocks_per_sm(int which, int form);

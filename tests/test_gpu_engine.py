@@ -288,11 +288,11 @@ def test_long_violent_free_surface_run_matches_oracle(kv):
     s.close()
 
 
-@pytest.mark.parametrize("form", ["32", "128x1", "128x2", "128x4"])
+@pytest.mark.parametrize("form", ["32", "64x1", "64x2", "128x1", "128x2", "128x4"])
 @pytest.mark.parametrize("shape", [(1280, 320), (4352, 1024)], ids=["400-tiles", "4352-tiles"])
 def test_flag_pass_launch_forms_match_oracle(monkeypatch, form, shape):
     """The flag pass in each launch form (tile width x cells per thread:
-    32x1, 128x1, 128x2, 128x4; FLB_FS_FLAG_FORM, read at creation), on a
+    32x1, 64x1, 64x2, 128x1, 128x2, 128x4; FLB_FS_FLAG_FORM, read at creation), on a
     grid below and one above 4,096 super-tiles (launched with and without
     programmatic dependent launch), against the oracle at every check."""
     monkeypatch.setenv("FLB_FS_FLAG_FORM", form)
