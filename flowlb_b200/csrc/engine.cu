@@ -456,12 +456,16 @@ flb_status validate(const flb_case_desc* d, std::string& msg) {
 }
 
 flb_status check_io(flb_engine* h, const uint8_t* flags) {
-  h->has_io = false;
-  for (uint64_t i = 0; i < h->N; i++) {
-    if (flags[i] & (kInlet | kOutlet)) h->has_io = true;
-    if ((flags[i] & kInlet) && i + 1 >= h->N) return fail(h, FLB_ERR_INVALID_ARGUMENT, "inlet in the last cell");
-    if ((flags[i] & kOutlet) && i == 0) return fail(h, FLB_ERR_INVALID_ARGUMENT, "outlet in the first cell");
-  }
+  // one OR over all the bytes (a loop the compiler vectorises: it runs on
+  // every reset), then the two cells an inlet or outlet may not occupy, in
+  // the order a cell-by-cell scan meets them
+  const uint64_t N = h->N;
+  uint8_t any = 0;
+  for (uint64_t i = 0; i < N; i++) any = (uint8_t)(any | flags[i]);
+  h->has_io = (any & (kInlet | kOutlet)) != 0;
+  if (N == 1 && (flags[0] & kInlet)) return fail(h, FLB_ERR_INVALID_ARGUMENT, "inlet in the last cell");
+  if (N > 0 && (flags[0] & kOutlet)) return fail(h, FLB_ERR_INVALID_ARGUMENT, "outlet in the first cell");
+  if (N > 0 && (flags[N - 1] & kInlet)) return fail(h, FLB_ERR_INVALID_ARGUMENT, "inlet in the last cell");
   return FLB_OK;
 }
 
@@ -773,7 +777,10 @@ FLB_API flb_status flb_reset(flb_handle h, const uint8_t* host_flags) {
   DeviceGuard guard(h->device);
   const bool had_io = h->has_io;
   flb_status s = check_io(h, host_flags);
-  if (s != FLB_OK) return s;
+  if (s != FLB_OK) {
+    h->has_io = had_io;  // the handle keeps its state
+    return s;
+  }
   if (h->has_io && !had_io) {
     h->has_io = false;
     return fail(h, FLB_ERR_UNSUPPORTED, "reset adds inlet/outlet cells to a case created without them");

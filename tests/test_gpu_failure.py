@@ -111,3 +111,28 @@ def _allocation_failures(torch, c, kw, monkeypatch):
     s.close()
     assert abs(_free_bytes(torch) - before) <= 2 << 20
     assert "FLB_FAIL_ALLOC_AT" not in os.environ
+
+
+@pytest.mark.parametrize("where,msg", [("last", "inlet in the last cell"), ("first", "outlet in the first cell")])
+def test_inlet_outlet_placement_is_checked(require_gpu, where, msg):
+    """An inlet takes its density from the next cell and an outlet its velocity
+    from the previous one, so an inlet in the last cell or an outlet in the
+    first is refused with FLB_ERR_INVALID_ARGUMENT, at creation and at a
+    reset; a valid reset of the same handle works afterwards."""
+    c = cases.plain_channel(64, 16)
+    bad = c.flags.copy()
+    if where == "last":
+        bad.flat[-1] = cases.INLET | cases.FLUID
+    else:
+        bad.flat[0] = cases.OUTLET | cases.FLUID
+    with pytest.raises(E.FlowLBError) as ei:
+        E.Solver(bad, free_surface=False, precision=32, tau=c.tau, fx=c.fx, device=0)
+    assert ei.value.status == 1  # FLB_ERR_INVALID_ARGUMENT (the reason goes to stderr: no handle exists)
+    s = E.Solver(c.flags, free_surface=False, precision=32, tau=c.tau, fx=c.fx, device=0)
+    with pytest.raises(E.FlowLBError) as ei:
+        s.reset(bad)
+    assert ei.value.status == 1 and msg in str(ei.value)
+    s.reset(c.flags)
+    s.step(4)
+    assert s.check_finite()
+    s.close()
