@@ -72,3 +72,17 @@ def test_algorithmic_bytes_per_pass():
     assert b16["stream_collide"] == 1010 * (86.0 - 36.0) + 10 * 9.0
     assert b16["fs1"] == 1010 * (93.0 - 34.0)
     assert b16["fs234"] == b32["fs234"]
+
+
+def test_pass_shares_and_traffic_cover_the_three_passes():
+    """The launch-list shares that split the measured step among the three
+    free-surface passes name the same passes as the algorithmic bytes, add
+    up to the step (within the rounding of the committed figures), and each
+    pass has a per-launch DRAM traffic figure."""
+    counts = {"fluid": 1, "interface": 0, "gas": 0, "wall": 0}
+    passes = set(bench.algorithmic_bytes(counts))
+    assert set(bench.PASS_SHARE_NCU) == passes
+    assert set(bench.TRAFFIC_NCU) == passes
+    assert abs(sum(bench.PASS_SHARE_NCU.values()) - 1.0) < 0.01
+    assert all(0.0 < v < 1.0 for v in bench.PASS_SHARE_NCU.values())
+    assert all(v > 0 for v in bench.TRAFFIC_NCU.values())
